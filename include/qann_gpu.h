@@ -1,0 +1,144 @@
+/*
+ * qann_gpu — C ABI of the B200 search path for qann's dense indexes.
+ *
+ * Every function returns 0 (QG_OK) or a status code; qg_last_error() gives the
+ * message of the calling thread's last failure. Buffers passed in are HOST
+ * memory owned by the caller unless a name says _dev. Status codes map onto
+ * the exceptions qann's Python layer raises (reference
+ * bindings/python_bindings.cpp): QG_INVALID_ARGUMENT -> ValueError,
+ * QG_LOGIC_ERROR / QG_RUNTIME_ERROR -> RuntimeError.
+ *
+ * Handles are reference-counted views of an index; a RefineIndex keeps its
+ * base alive. Concurrent qg_search calls on one handle are safe (readers
+ * share the index; writers — add, remove, train, setters — are exclusive),
+ * as the reference's bindings lock (reference bindings/python_bindings.cpp:97-131).
+ */
+#ifndef QANN_GPU_H
+#define QANN_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct qg_index qg_index;
+
+enum {
+    QG_OK = 0,
+    QG_INVALID_ARGUMENT = 1,
+    QG_LOGIC_ERROR = 2,
+    QG_RUNTIME_ERROR = 3,
+    QG_CUDA_ERROR = 4,
+    QG_OUT_OF_MEMORY = 5,
+    QG_UNSUPPORTED = 6,
+};
+
+/* Index kinds: the .qann file format's tags (reference src/serialize.hpp:29-38). */
+enum { QG_KIND_FLAT = 1, QG_KIND_IVF = 2, QG_KIND_REFINE = 3 };
+/* Metrics (reference include/vecengine/index.hpp:57-62). */
+enum { QG_METRIC_L2 = 0, QG_METRIC_COSINE = 1, QG_METRIC_INNER_PRODUCT = 2 };
+/* Coarse clustering (reference include/vecengine/ivf_index.hpp:27-30). */
+enum { QG_CLUSTERING_EMEANS = 0, QG_CLUSTERING_LLOYD = 1 };
+
+/* The calling thread's last error message ("" when none). */
+const char* qg_last_error(void);
+
+/* Version string of the library build. */
+const char* qg_version(void);
+
+/* --- construction ------------------------------------------------------------
+ * qg_create_ivf   replaces IVFIndex::IVFIndex(dim, nlist, nprobe, custom_ids, metric)
+ *                 (reference include/vecengine/ivf_index.hpp:62)
+ * qg_enable_pq    replaces IVFIndex::enable_pq(m, K, fast_scan, rotate) (ivf_index.hpp:69-70)
+ * qg_create_flat  replaces FlatIndex::FlatIndex(dim, capacity, custom_ids, metric)
+ *                 (reference include/vecengine/flat_index.hpp:25)
+ * qg_create_refine replaces RefineIndex::RefineIndex(base, k_factor, custom_ids)
+ *                 (reference include/vecengine/refine_index.hpp:37)
+ */
+int qg_create_ivf(size_t dim, size_t nlist, size_t nprobe, int metric, int custom_ids, qg_index** out);
+int qg_enable_pq(qg_index* h, size_t m, size_t centroids_per_subspace, int fast_scan, int rotate);
+int qg_create_flat(size_t dim, int metric, int custom_ids, qg_index** out);
+int qg_create_refine(qg_index* base, size_t k_factor, int custom_ids, qg_index** out);
+/* A new handle to a RefineIndex's base (reference refine_index.hpp:88-89 base()). */
+int qg_refine_base(qg_index* refine, qg_index** out);
+void qg_free(qg_index* h);
+
+/* --- training and adding --------------------------------------------------------
+ * qg_train replaces IVFIndex::train(vectors, n, max_iters, seed, clustering, passes)
+ *          (reference include/vecengine/ivf_index.hpp:143-145); seed < 0 = unseeded.
+ * qg_add   replaces DenseIndex::add_batch(vecs, n, ids) (reference index.hpp:185);
+ *          ids is NULL unless the index has custom ids; out_ids (n) may be NULL.
+ */
+int qg_train(qg_index* h, const float* x, size_t n, size_t max_iters, int64_t seed, int clustering, size_t passes);
+int qg_add(qg_index* h, const float* x, size_t n, const int64_t* ids, int64_t* out_ids);
+/* replaces IndexBase::remove / compact (reference index.hpp:122-128) */
+int qg_remove(qg_index* h, const int64_t* ids, size_t n, size_t* removed);
+int qg_compact(qg_index* h, size_t* reclaimed);
+
+/* --- search ------------------------------------------------------------------------
+ * Replaces DenseIndex::query_batch(queries, nq, k[, allowed]) (reference
+ * include/vecengine/index.hpp:197-209) as the Python batch_query presents it
+ * (reference bindings/python_bindings.cpp:582-648): out_ids / out_dists are
+ * nq * k, padded with -1 / +inf. allowed: NULL for no filter, else n_allowed
+ * ids (unknown / deleted / repeated ids are ignored).
+ * Host buffers; the copies to and from the device are part of the call.
+ */
+int qg_search(qg_index* h, const float* q, size_t nq, size_t k, const int64_t* allowed, size_t n_allowed,
+              int64_t* out_ids, float* out_dists);
+/* The same with the filter as a slot bitmap (bit s of words[s / 64]: slot s
+ * may be returned), the form a host-side where= evaluation produces
+ * (reference src/index.cpp:156-163). nwords must cover the index's slots. */
+int qg_search_bitmap(qg_index* h, const float* q, size_t nq, size_t k, const uint64_t* words, size_t nwords,
+                     int64_t* out_ids, float* out_dists);
+/* Device-resident variant: q_dev, out_ids_dev, out_dists_dev are device
+ * pointers and the work runs on `stream` (a cudaStream_t, NULL = the legacy
+ * default stream); the call returns when the results are written. */
+int qg_search_device(qg_index* h, const float* q_dev, size_t nq, size_t k, int64_t* out_ids_dev, float* out_dists_dev,
+                     void* stream);
+
+/* --- properties ------------------------------------------------------------------
+ * keys: "nprobe", "k_factor", "precomputed_tables", "cosine_inner_product",
+ * "filter_probe_scaling" (settable; reference ivf_index.hpp:83-118,
+ * refine_index.hpp:91-93) and the read-only "dim", "kind", "metric", "nlist",
+ * "size", "slots", "custom_ids", "fast_scan", "pq_m", "pq_k", "trained",
+ * "rotate", "sq_bits", "wrapped".
+ */
+int qg_get(qg_index* h, const char* key, int64_t* value);
+int qg_set(qg_index* h, const char* key, int64_t value);
+
+/* --- files ------------------------------------------------------------------------
+ * .qann format 13, interchangeable with qann (reference src/index_factory.cpp:94-141).
+ * qg_load: *kind receives QG_KIND_*.
+ */
+int qg_save(qg_index* h, const char* path);
+int qg_load(const char* path, qg_index** out, int* kind);
+
+/* --- kernels of the path on device memory (parity tests and tools) ----------------
+ * qg_quantize_lut_dev: n tables of m x 16 floats -> n LUTs of m x 16 bytes plus
+ *   scale / offset each; bit-exact with quantize_lut (reference src/fast_scan.cpp:22-46).
+ * qg_build_quantize_lut_dev: n tables B_i + C_i (+ A_i on row 0) rounded the same
+ *   way (reference src/fast_scan.cpp:243-254 build_quantize_lut).
+ * qg_fast_scan_dev: sums[v] = sum_s lut[lut_of[v / 64]][s][code(v, s)] for n
+ *   vectors with plain codes (n x m bytes, one code per byte) and one LUT index
+ *   per group of 64 vectors; the same values fast_scan_block computes
+ *   (reference src/fast_scan.cpp:256-262). LUTs are nluts x m x 16 bytes,
+ *   16-byte aligned.
+ * qg_exact_scores_dev: out[i * nb + j] = squared L2 (ip = 0) or -(a . b) (ip = 1)
+ *   in the reference's AVX2 accumulation order (reference src/distance.cpp:66-96, :138-151).
+ */
+int qg_quantize_lut_dev(const float* tables_dev, size_t n, size_t m, uint8_t* lut_dev, float* scale_dev,
+                        float* offset_dev, void* stream);
+int qg_build_quantize_lut_dev(const float* B_dev, const float* C_dev, const float* A_dev, size_t n, size_t m,
+                              uint8_t* lut_dev, float* scale_dev, float* offset_dev, void* stream);
+int qg_fast_scan_dev(const uint8_t* lut_dev, size_t nluts, size_t m, const uint8_t* codes_dev,
+                     const uint32_t* lut_of_dev, size_t n, uint16_t* sums_dev, void* stream);
+int qg_exact_scores_dev(const float* a_dev, size_t na, const float* b_dev, size_t nb, size_t dim, int ip,
+                        float* out_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QANN_GPU_H */

@@ -1,0 +1,293 @@
+"""qann_b200 — qann's dense-vector search path on NVIDIA B200.
+
+A drop-in for the part of qann (https://github.com/maxtmiller/qann) that
+searches dense vectors: ``IVFIndex`` with 4-bit PQ fast-scan, ``RefineIndex``
+re-ranking, ``FlatIndex``, their ``train`` / ``add`` / ``batch_query`` /
+``save`` / ``load``, ``nprobe``, ``k_factor`` and ``allowed`` filters, with
+the same signatures, defaults, errors and ``.qann`` files. Behind it, C++ host
+code drives hand-written sm_100a CUDA kernels through the C ABI in
+``include/qann_gpu.h``; results match the reference's CPU build (see
+DESIGN.md for the exact contract).
+
+Differences from qann: ``where=`` metadata filters are evaluated by the
+caller (pass the matching ids as ``allowed``); HNSW, SQ, sparse, hybrid and
+journal indexes are not part of this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import CudaError, check
+
+__all__ = [
+    "Metric", "Clustering", "PQDistance", "DenseIndex", "FlatIndex", "IVFIndex", "RefineIndex", "load",
+    "set_num_threads", "CudaError", "version",
+]
+
+
+class Metric(enum.IntEnum):
+    """How an index compares vectors (reference include/vecengine/index.hpp:57-62)."""
+    L2 = 0
+    Cosine = 1
+    InnerProduct = 2
+
+
+class Clustering(enum.IntEnum):
+    """How IVFIndex.train learns the coarse centroids."""
+    EMeans = 0
+    Lloyd = 1
+
+
+class PQDistance(enum.IntEnum):
+    ADC = 0
+    SDC = 1
+
+
+def version() -> str:
+    return _lib.lib.qg_version().decode()
+
+
+_threads = os.cpu_count() or 1
+
+
+def set_num_threads(n: int) -> None:
+    """Accepted for API compatibility: the search path runs on the GPU, so the
+    host thread count has no effect on it."""
+    global _threads
+    if n < 1:
+        raise ValueError("num_threads must be >= 1")
+    _threads = int(n)
+
+
+def _f32_rows(data, dim: int, what: str = "data") -> np.ndarray:
+    a = np.asarray(data, dtype=np.float32)
+    if a.ndim != 2:
+        raise ValueError(f"{what} must be a 2D array of shape (n, dim)")
+    if a.shape[1] != dim:
+        raise ValueError(f"{what} dimension does not match index dimension")
+    return np.ascontiguousarray(a)
+
+
+def _ids(ids) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(list(ids) if not hasattr(ids, "__len__") else ids, dtype=np.int64).ravel())
+
+
+class DenseIndex:
+    """An index of dense float32 vectors. Not constructed directly."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+        self._parent = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _lib.lib.qg_free(h)
+            self._h = None
+
+    # -- properties -----------------------------------------------------------------
+    def _get(self, key: str) -> int:
+        v = C.c_int64()
+        check(_lib.lib.qg_get(self._h, key.encode(), C.byref(v)))
+        return v.value
+
+    def _set(self, key: str, value) -> None:
+        check(_lib.lib.qg_set(self._h, key.encode(), int(value)))
+
+    def dim(self) -> int:
+        return self._get("dim")
+
+    def size(self) -> int:
+        """Number of live (not deleted) vectors."""
+        return self._get("size")
+
+    @property
+    def metric(self) -> Metric:
+        return Metric(self._get("metric"))
+
+    @property
+    def custom_ids(self) -> bool:
+        return bool(self._get("custom_ids"))
+
+    @property
+    def stores_vectors(self) -> bool:
+        return isinstance(self, (FlatIndex, RefineIndex))
+
+    # -- writes -----------------------------------------------------------------------
+    def add(self, data, ids=None, *, metadata=None):
+        """Adds an (n, dim) array; returns the vectors' int64 ids."""
+        if metadata is not None:
+            raise NotImplementedError("metadata columns are not supported by qann_b200; filter with allowed=")
+        x = _f32_rows(data, self.dim())
+        n = x.shape[0]
+        idarr = None if ids is None else _ids(ids)
+        if idarr is not None and idarr.size != n:
+            raise ValueError("ids must have one id per row")
+        out = np.empty(n, np.int64)
+        check(_lib.lib.qg_add(self._h, x.ctypes.data, n, None if idarr is None else idarr.ctypes.data,
+                              out.ctypes.data))
+        return out
+
+    def remove(self, ids) -> int:
+        a = _ids(ids)
+        r = C.c_size_t()
+        check(_lib.lib.qg_remove(self._h, a.ctypes.data, a.size, C.byref(r)))
+        return r.value
+
+    def compact(self) -> int:
+        r = C.c_size_t()
+        check(_lib.lib.qg_compact(self._h, C.byref(r)))
+        return r.value
+
+    # -- queries ----------------------------------------------------------------------
+    def batch_query(self, query, k, *, allowed=None, where=None):
+        """k nearest neighbours of each row: (ids int64 (nq, k), distances
+        float32 (nq, k)), padded with -1 / inf."""
+        if where is not None:
+            raise NotImplementedError("where= needs metadata evaluation; pass the matching ids as allowed=")
+        q = _f32_rows(query, self.dim(), "query")
+        k = int(k)
+        if k < 0:
+            raise ValueError("k must be >= 0")
+        nq = q.shape[0]
+        ids = np.empty((nq, k), np.int64)
+        d = np.empty((nq, k), np.float32)
+        if allowed is None:
+            check(_lib.lib.qg_search(self._h, q.ctypes.data, nq, k, None, 0, ids.ctypes.data, d.ctypes.data))
+        else:
+            al = _ids(allowed)
+            check(_lib.lib.qg_search(self._h, q.ctypes.data, nq, k, al.ctypes.data, al.size, ids.ctypes.data,
+                                     d.ctypes.data))
+        return ids, d
+
+    def batch_query_bitmap(self, query, k, words):
+        """batch_query with the filter given as a slot bitmap (uint64 words,
+        bit s of words[s // 64] allows slot s), as a where= evaluation yields."""
+        q = _f32_rows(query, self.dim(), "query")
+        w = np.ascontiguousarray(words, dtype=np.uint64)
+        nq = q.shape[0]
+        ids = np.empty((nq, k), np.int64)
+        d = np.empty((nq, k), np.float32)
+        check(_lib.lib.qg_search_bitmap(self._h, q.ctypes.data, nq, k, w.ctypes.data, w.size, ids.ctypes.data,
+                                        d.ctypes.data))
+        return ids, d
+
+    def query(self, query, k, *, allowed=None, where=None):
+        """k nearest neighbours of one (dim,) vector: 1D (ids, distances), one
+        entry per result found."""
+        q = np.asarray(query, dtype=np.float32)
+        if q.ndim != 1:
+            raise ValueError("query must be a 1D array of shape (dim,)")
+        ids, d = self.batch_query(q[None], k, allowed=allowed, where=where)
+        keep = ids[0] >= 0
+        return ids[0][keep], d[0][keep]
+
+    def search_device(self, q_ptr: int, nq: int, k: int, out_ids_ptr: int, out_d_ptr: int, stream: int = 0) -> None:
+        """batch_query on device memory (raw CUDA pointers, e.g. torch
+        ``tensor.data_ptr()``): q (nq, dim) float32 in, ids (nq, k) int64 and
+        distances (nq, k) float32 out, on ``stream``."""
+        check(_lib.lib.qg_search_device(self._h, q_ptr, nq, k, out_ids_ptr, out_d_ptr, stream or None))
+
+    def save(self, path) -> None:
+        check(_lib.lib.qg_save(self._h, os.fspath(path).encode()))
+
+    def __len__(self):
+        return self.size()
+
+
+class FlatIndex(DenseIndex):
+    """Exact search over every stored vector (reference include/vecengine/flat_index.hpp)."""
+
+    def __init__(self, dim, *, custom_ids=False, metric=Metric.L2, _handle=None):
+        if _handle is None:
+            h = C.c_void_p()
+            check(_lib.lib.qg_create_flat(int(dim), int(metric), int(bool(custom_ids)), C.byref(h)))
+            _handle = h.value
+        super().__init__(_handle)
+
+
+class IVFIndex(DenseIndex):
+    """Inverted-file index with residual PQ (4-bit fast-scan on the GPU path)
+    (reference include/vecengine/ivf_index.hpp)."""
+
+    def __init__(self, dim, nlist, nprobe=10, *, custom_ids=False, metric=Metric.L2, _handle=None):
+        if _handle is None:
+            h = C.c_void_p()
+            check(_lib.lib.qg_create_ivf(int(dim), int(nlist), int(nprobe), int(metric), int(bool(custom_ids)),
+                                         C.byref(h)))
+            _handle = h.value
+        super().__init__(_handle)
+
+    def train(self, data, max_iters=10, seed=None, *, clustering=Clustering.EMeans, passes=2):
+        x = _f32_rows(data, self.dim())
+        check(_lib.lib.qg_train(self._h, x.ctypes.data, x.shape[0], int(max_iters), -1 if seed is None else int(seed),
+                                int(clustering), int(passes)))
+
+    def enable_pq(self, num_subspaces, centroids_per_subspace=None, *, fast_scan=False, rotate=False):
+        K = centroids_per_subspace if centroids_per_subspace is not None else (16 if fast_scan else 256)
+        check(_lib.lib.qg_enable_pq(self._h, int(num_subspaces), int(K), int(bool(fast_scan)), int(bool(rotate))))
+
+    nlist = property(lambda self: self._get("nlist"))
+    nprobe = property(lambda self: self._get("nprobe"), lambda self, v: self._set("nprobe", v))
+    precomputed_tables = property(lambda self: bool(self._get("precomputed_tables")),
+                                  lambda self, v: self._set("precomputed_tables", bool(v)))
+    cosine_inner_product = property(lambda self: bool(self._get("cosine_inner_product")),
+                                    lambda self, v: self._set("cosine_inner_product", bool(v)))
+    filter_probe_scaling = property(lambda self: bool(self._get("filter_probe_scaling")),
+                                    lambda self, v: self._set("filter_probe_scaling", bool(v)))
+    pq_distance = property(lambda self: PQDistance(self._get("pq_distance")),
+                           lambda self, v: self._set("pq_distance", int(v)))
+    fast_scan = property(lambda self: bool(self._get("fast_scan")))
+    pq_rotate = property(lambda self: bool(self._get("rotate")))
+    sq_bits = property(lambda self: self._get("sq_bits"))
+    mapped = property(lambda self: False)
+
+
+class RefineIndex(DenseIndex):
+    """Re-ranks an approximate base's k * k_factor candidates with exact
+    distances (reference include/vecengine/refine_index.hpp)."""
+
+    def __init__(self, base=None, k_factor=10, *, custom_ids=False, _handle=None):
+        if _handle is None:
+            if not isinstance(base, DenseIndex):
+                raise TypeError("base must be a qann_b200 index")
+            h = C.c_void_p()
+            check(_lib.lib.qg_create_refine(base._h, int(k_factor), int(bool(custom_ids)), C.byref(h)))
+            _handle = h.value
+        super().__init__(_handle)
+        self._base = base
+
+    k_factor = property(lambda self: self._get("k_factor"), lambda self, v: self._set("k_factor", v))
+    mapped = property(lambda self: False)
+
+    @property
+    def base(self):
+        if self._base is None:
+            h = C.c_void_p()
+            check(_lib.lib.qg_refine_base(self._h, C.byref(h)))
+            kind = self._get("base_kind")
+            self._base = (IVFIndex if kind == 2 else FlatIndex)(0, 0, _handle=h.value) if kind == 2 else \
+                FlatIndex(0, _handle=h.value)
+        return self._base
+
+
+def load(path, *, mmap=False):
+    """Loads an index saved by qann or by this package (.qann format 1..13);
+    returns FlatIndex, IVFIndex or RefineIndex. mmap is accepted for API
+    compatibility: the device holds the whole index either way."""
+    h = C.c_void_p()
+    kind = C.c_int()
+    check(_lib.lib.qg_load(os.fspath(path).encode(), C.byref(h), C.byref(kind)))
+    if kind.value == 1:
+        return FlatIndex(0, _handle=h.value)
+    if kind.value == 2:
+        return IVFIndex(0, 0, _handle=h.value)
+    return RefineIndex(_handle=h.value)
+
+
+Index = DenseIndex

@@ -1,0 +1,447 @@
+// The C ABI (include/qann_gpu.h): handles, status codes, argument checks with
+// the reference's messages, locking, and per-thread streams.
+#include "../../include/qann_gpu.h"
+
+#include "qg_device.cuh"
+#include "qg_ops.h"
+
+#include <limits>
+#include <string>
+
+using namespace qg;
+
+struct qg_index {
+    std::shared_ptr<IndexObj> obj;
+};
+
+namespace {
+
+thread_local std::string t_err;
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return QG_OK;
+    } catch (const Error& e) {
+        t_err = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        t_err = "out of host memory";
+        return QG_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        t_err = e.what();
+        return QG_RUNTIME_ERROR;
+    }
+}
+
+// One non-blocking stream per host thread, so concurrent searches overlap.
+cudaStream_t thread_stream() {
+    thread_local cudaStream_t s = nullptr;
+    if (!s) QG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+}
+
+IndexObj& obj(qg_index* h) {
+    require(h && h->obj, "null index handle");
+    return *h->obj;
+}
+
+IVFObj& ivf_of(qg_index* h) {
+    IndexObj& o = obj(h);
+    if (o.kind == Kind::IVF) return static_cast<IVFObj&>(o);
+    if (o.kind == Kind::Refine) {
+        auto& r = static_cast<RefineObj&>(o);
+        if (r.base->kind == Kind::IVF) return static_cast<IVFObj&>(*r.base);
+    }
+    throw Error(kInvalidArgument, "not an IVFIndex");
+}
+
+qg_index* wrap(std::shared_ptr<IndexObj> o) {
+    auto* h = new qg_index;
+    h->obj = std::move(o);
+    return h;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* qg_last_error(void) { return t_err.c_str(); }
+
+const char* qg_version(void) { return "qann-b200 0.1.0 (sm_100a)"; }
+
+int qg_create_ivf(size_t dim, size_t nlist, size_t nprobe, int metric, int custom_ids, qg_index** out) {
+    return guarded([&] {
+        require(nlist >= 100 && nlist <= 65535, "nlist must be in [100, 65535]");
+        require(dim >= 1, "dim must be >= 1");
+        require(nprobe >= 1 && nprobe <= nlist, "nprobe must be in [1, nlist]");
+        require(metric >= 0 && metric <= 2, "unknown metric");
+        auto o = std::make_shared<IVFObj>();
+        o->model.dim = dim;
+        o->model.nlist = nlist;
+        o->model.nprobe = nprobe;
+        o->model.metric = static_cast<Metric>(metric);
+        o->model.idmap = IdMap(custom_ids != 0);
+        o->model.list_ids.resize(nlist);
+        o->model.list_codes.resize(nlist);
+        o->model.list_vecs.resize(nlist);
+        *out = wrap(o);
+    });
+}
+
+int qg_enable_pq(qg_index* h, size_t m, size_t K, int fast_scan, int rotate) {
+    return guarded([&] {
+        IVFObj& o = ivf_of(h);
+        std::unique_lock<std::shared_mutex> lk(o.mu);
+        IVFModel& M = o.model;
+        if (M.idmap.slots() > 0 || M.trained)
+            throw Error(kLogicError, "enable_pq must be called before train()/add()");
+        if (M.sq_bits) throw Error(kLogicError, "enable_pq cannot be combined with enable_sq");
+        if (fast_scan && (K != 16 || m % 2 != 0 || m > kFsMaxSubspaces))
+            throw Error(kInvalidArgument, "fast_scan needs 16 centroids per subspace and an even num_subspaces <= 1024");
+        if (fast_scan && M.pq_distance == 1) throw Error(kInvalidArgument, "cannot use SDC with fast-scan");
+        require(M.dim >= 1 && m >= 1, "dim and num_subspaces must be >= 1");
+        require(M.dim % m == 0, "dim must be divisible by num_subspaces");
+        require(K >= 1 && K <= 256, "centroids_per_subspace must be in [1, 256]");
+        M.has_pq = true;
+        M.fast_scan = fast_scan != 0;
+        M.rotate = rotate != 0;
+        M.pq = PQCodebook{};
+        M.pq.dim = M.dim;
+        M.pq.m = m;
+        M.pq.K = K;
+        M.pq.sub_dim = M.dim / m;
+        M.pq.centroids.assign(m * K * M.pq.sub_dim, 0.0f);
+        o.dev_dirty = true;
+    });
+}
+
+int qg_create_flat(size_t dim, int metric, int custom_ids, qg_index** out) {
+    return guarded([&] {
+        require(dim >= 1, "dim must be >= 1");
+        require(metric >= 0 && metric <= 2, "unknown metric");
+        auto o = std::make_shared<FlatObj>();
+        o->model.dim = dim;
+        o->model.metric = static_cast<Metric>(metric);
+        o->model.idmap = IdMap(custom_ids != 0);
+        *out = wrap(o);
+    });
+}
+
+int qg_create_refine(qg_index* base, size_t k_factor, int custom_ids, qg_index** out) {
+    return guarded([&] {
+        IndexObj& b = obj(base);
+        std::unique_lock<std::shared_mutex> lk(b.mu);
+        if (b.kind == Kind::Refine)
+            throw Error(kInvalidArgument,
+                        "a RefineIndex's base must not be a RefineIndex; wrap the approximate index directly");
+        if (b.idmap().slots() != 0) throw Error(kInvalidArgument, "base index must be empty");
+        if (k_factor == 0) throw Error(kInvalidArgument, "k_factor must be >= 1");
+        if (!b.idmap().ids_are_slots())
+            throw Error(kInvalidArgument, "base index must not use custom ids or have been compacted");
+        if (b.wrapped) throw Error(kInvalidArgument, "base index is already wrapped by another index");
+        auto o = std::make_shared<RefineObj>();
+        o->base = base->obj;
+        o->k_factor = k_factor;
+        o->map = IdMap(custom_ids != 0);
+        b.wrapped = true;
+        *out = wrap(o);
+    });
+}
+
+int qg_refine_base(qg_index* refine, qg_index** out) {
+    return guarded([&] {
+        IndexObj& o = obj(refine);
+        require(o.kind == Kind::Refine, "not a RefineIndex");
+        *out = wrap(static_cast<RefineObj&>(o).base);
+    });
+}
+
+void qg_free(qg_index* h) { delete h; }
+
+int qg_train(qg_index* h, const float* x, size_t n, size_t max_iters, int64_t seed, int clustering, size_t passes) {
+    return guarded([&] {
+        IndexObj& o0 = obj(h);
+        require(o0.kind == Kind::IVF, "train() is an IVFIndex method");
+        auto& o = static_cast<IVFObj&>(o0);
+        std::unique_lock<std::shared_mutex> lk(o.mu);
+        train(o, x, n, max_iters, seed, clustering, passes, thread_stream());
+    });
+}
+
+int qg_add(qg_index* h, const float* x, size_t n, const int64_t* ids, int64_t* out_ids) {
+    return guarded([&] {
+        IndexObj& o = obj(h);
+        std::unique_lock<std::shared_mutex> lk(o.mu);
+        if (o.wrapped)
+            throw Error(kInvalidArgument, "cannot add on an index wrapped by a RefineIndex or HybridIndex; add through "
+                                          "the wrapper instead");
+        std::unique_lock<std::shared_mutex> lb;
+        if (o.kind == Kind::Refine) lb = std::unique_lock<std::shared_mutex>(static_cast<RefineObj&>(o).base->mu);
+        validate_add(o, n, ids);
+        if (n == 0) return;
+        add(o, x, n, ids, out_ids, thread_stream());
+    });
+}
+
+int qg_remove(qg_index* h, const int64_t* ids, size_t n, size_t* removed) {
+    return guarded([&] {
+        IndexObj& o = obj(h);
+        std::unique_lock<std::shared_mutex> lk(o.mu);
+        if (o.wrapped)
+            throw Error(kInvalidArgument, "cannot remove on an index wrapped by a RefineIndex or HybridIndex; remove "
+                                          "through the wrapper instead");
+        std::vector<uint32_t> slots;
+        *removed = o.idmap().remove({ids, n}, &slots);
+        o.dev_dirty = true;
+        if (o.kind == Kind::Refine) {
+            auto& r = static_cast<RefineObj&>(o);
+            std::unique_lock<std::shared_mutex> lb(r.base->mu);
+            std::vector<int64_t> base_ids(slots.begin(), slots.end());
+            r.base->idmap().remove(base_ids);
+            r.base->dev_dirty = true;
+        }
+    });
+}
+
+int qg_compact(qg_index* h, size_t* reclaimed) {
+    return guarded([&] {
+        IndexObj& o = obj(h);
+        std::unique_lock<std::shared_mutex> lk(o.mu);
+        compact(o, reclaimed);
+    });
+}
+
+static int search_common(qg_index* h, const float* q, size_t nq, size_t k, const SlotBits* filter, int64_t* out_ids,
+                         float* out_d, IoSpace io, cudaStream_t st) {
+    IndexObj& o = obj(h);
+    std::shared_lock<std::shared_mutex> lk(o.mu);
+    std::shared_lock<std::shared_mutex> lb;
+    if (o.kind == Kind::Refine) lb = std::shared_lock<std::shared_mutex>(static_cast<RefineObj&>(o).base->mu);
+    SearchRequest r;
+    r.q = q;
+    r.nq = nq;
+    r.k = k;
+    r.filter = filter;
+    r.out_ids = out_ids;
+    r.out_d = out_d;
+    r.io = io;
+    search(o, r, st);
+    return QG_OK;
+}
+
+int qg_search(qg_index* h, const float* q, size_t nq, size_t k, const int64_t* allowed, size_t n_allowed,
+              int64_t* out_ids, float* out_dists) {
+    return guarded([&] {
+        IndexObj& o = obj(h);
+        SlotBits f;
+        if (allowed) {
+            std::shared_lock<std::shared_mutex> lk(o.mu);
+            f = o.idmap().filter({allowed, n_allowed});
+        }
+        search_common(h, q, nq, k, allowed ? &f : nullptr, out_ids, out_dists, IoSpace::Host, thread_stream());
+    });
+}
+
+int qg_search_bitmap(qg_index* h, const float* q, size_t nq, size_t k, const uint64_t* words, size_t nwords,
+                     int64_t* out_ids, float* out_dists) {
+    return guarded([&] {
+        IndexObj& o = obj(h);
+        SlotBits f;
+        {
+            std::shared_lock<std::shared_mutex> lk(o.mu);
+            require(nwords * 64 >= o.idmap().slots(), "the bitmap must cover every slot of the index");
+            f = o.idmap().live(std::vector<uint64_t>(words, words + nwords));
+        }
+        search_common(h, q, nq, k, &f, out_ids, out_dists, IoSpace::Host, thread_stream());
+    });
+}
+
+int qg_search_device(qg_index* h, const float* q_dev, size_t nq, size_t k, int64_t* out_ids_dev, float* out_dists_dev,
+                     void* stream) {
+    return guarded([&] {
+        search_common(h, q_dev, nq, k, nullptr, out_ids_dev, out_dists_dev, IoSpace::Device,
+                      static_cast<cudaStream_t>(stream));
+    });
+}
+
+int qg_get(qg_index* h, const char* key, int64_t* value) {
+    return guarded([&] {
+        IndexObj& o = obj(h);
+        std::shared_lock<std::shared_mutex> lk(o.mu);
+        const std::string k(key);
+        if (k == "dim") *value = static_cast<int64_t>(o.dim());
+        else if (k == "kind") *value = static_cast<int64_t>(o.kind);
+        else if (k == "metric") *value = static_cast<int64_t>(o.metric());
+        else if (k == "size") *value = static_cast<int64_t>(o.idmap().live_count());
+        else if (k == "slots") *value = static_cast<int64_t>(o.idmap().slots());
+        else if (k == "custom_ids") *value = o.idmap().custom();
+        else if (k == "wrapped") *value = o.wrapped;
+        else if (k == "k_factor") {
+            require(o.kind == Kind::Refine, "not a RefineIndex");
+            *value = static_cast<int64_t>(static_cast<RefineObj&>(o).k_factor);
+        } else if (k == "base_kind") {
+            require(o.kind == Kind::Refine, "not a RefineIndex");
+            *value = static_cast<int64_t>(static_cast<RefineObj&>(o).base->kind);
+        } else {
+            require(o.kind == Kind::IVF, "unknown property '" + k + "' for this index");
+            const IVFObj& v = static_cast<IVFObj&>(o);
+            const IVFModel& M = v.model;
+            if (k == "nprobe") *value = static_cast<int64_t>(M.nprobe);
+            else if (k == "nlist") *value = static_cast<int64_t>(M.nlist);
+            else if (k == "precomputed_tables") *value = v.precomputed_available();
+            else if (k == "cosine_inner_product") *value = M.cosine_ip;
+            else if (k == "filter_probe_scaling") *value = M.filter_probe_scaling;
+            else if (k == "fast_scan") *value = M.fast_scan;
+            else if (k == "pq_m") *value = static_cast<int64_t>(M.has_pq ? M.pq.m : 0);
+            else if (k == "pq_k") *value = static_cast<int64_t>(M.has_pq ? M.pq.K : 0);
+            else if (k == "trained") *value = M.trained;
+            else if (k == "rotate") *value = M.rotate;
+            else if (k == "sq_bits") *value = M.sq_bits;
+            else if (k == "pq_distance") *value = M.pq_distance;
+            else throw Error(kInvalidArgument, "unknown property '" + k + "'");
+        }
+    });
+}
+
+int qg_set(qg_index* h, const char* key, int64_t value) {
+    return guarded([&] {
+        IndexObj& o = obj(h);
+        std::unique_lock<std::shared_mutex> lk(o.mu);
+        const std::string k(key);
+        if (k == "k_factor") {
+            require(o.kind == Kind::Refine, "not a RefineIndex");
+            require(value >= 1, "k_factor must be >= 1");
+            static_cast<RefineObj&>(o).k_factor = static_cast<uint64_t>(value);
+            return;
+        }
+        require(o.kind == Kind::IVF, "unknown property '" + k + "' for this index");
+        IVFObj& v = static_cast<IVFObj&>(o);
+        IVFModel& M = v.model;
+        if (k == "nprobe") {
+            require(value >= 1 && static_cast<uint64_t>(value) <= M.nlist, "nprobe must be in [1, nlist]");
+            M.nprobe = static_cast<uint64_t>(value);
+        } else if (k == "precomputed_tables") {
+            M.use_precomputed = value != 0;
+            v.dev_dirty = true;
+        } else if (k == "cosine_inner_product") {
+            M.cosine_ip = value != 0;
+            v.dev_dirty = true;
+        } else if (k == "filter_probe_scaling") {
+            M.filter_probe_scaling = value != 0;
+        } else if (k == "pq_distance") {
+            if (M.fast_scan && value == 1) throw Error(kInvalidArgument, "cannot use SDC with fast-scan");
+            if (M.metric == Metric::InnerProduct && value == 1)
+                throw Error(kInvalidArgument, "cannot use SDC with Metric::InnerProduct");
+            require(value == 0 || value == 1, "pq_distance must be ADC (0) or SDC (1)");
+            M.pq_distance = static_cast<uint8_t>(value);
+        } else {
+            throw Error(kInvalidArgument, "unknown or read-only property '" + k + "'");
+        }
+    });
+}
+
+int qg_save(qg_index* h, const char* path) {
+    return guarded([&] {
+        IndexObj& o = obj(h);
+        std::shared_lock<std::shared_mutex> lk(o.mu);
+        Writer w;
+        if (o.kind == Kind::IVF) {
+            write_header(w, Kind::IVF);
+            static_cast<IVFObj&>(o).model.save_body(w);
+        } else if (o.kind == Kind::Flat) {
+            write_header(w, Kind::Flat);
+            static_cast<FlatObj&>(o).model.save_body(w);
+        } else {
+            auto& r = static_cast<RefineObj&>(o);
+            std::shared_lock<std::shared_mutex> lb(r.base->mu);
+            write_header(w, Kind::Refine);
+            w.pod<uint64_t>(r.k_factor);
+            w.pod<uint64_t>(r.map.slots());
+            if (r.base->kind == Kind::IVF) {
+                write_header(w, Kind::IVF);
+                static_cast<IVFObj&>(*r.base).model.save_body(w);
+            } else {
+                write_header(w, Kind::Flat);
+                static_cast<FlatObj&>(*r.base).model.save_body(w);
+            }
+            w.pod<uint64_t>(r.map.slots() * r.dim());
+            w.pad(64 * 1024);
+            w.bytes(r.data.data(), r.data.size() * sizeof(float));
+            r.map.save(w);
+            r.meta.write(w);
+        }
+        write_file_atomic(path, w.buf);
+    });
+}
+
+int qg_load(const char* path, qg_index** out, int* kind) {
+    return guarded([&] {
+        const std::vector<char> bytes = read_file(path);
+        Reader r{bytes.data(), bytes.size()};
+        uint32_t version = 0;
+        const Kind k = read_header(r, &version);
+        std::shared_ptr<IndexObj> o;
+        if (k == Kind::IVF) {
+            auto v = std::make_shared<IVFObj>();
+            v->model = std::move(*IVFModel::load_body(r, version));
+            o = v;
+        } else if (k == Kind::Flat) {
+            auto f = std::make_shared<FlatObj>();
+            f->model = std::move(*FlatModel::load_body(r, version));
+            o = f;
+        } else {
+            auto m = RefineModel::load_body(r, version);
+            auto ro = std::make_shared<RefineObj>();
+            if (m->base_kind == Kind::IVF) {
+                auto v = std::make_shared<IVFObj>();
+                v->model = std::move(*m->ivf);
+                ro->base = v;
+            } else {
+                auto f = std::make_shared<FlatObj>();
+                f->model = std::move(*m->flat);
+                ro->base = f;
+            }
+            ro->base->wrapped = true;
+            ro->k_factor = m->k_factor;
+            ro->data = std::move(m->data);
+            ro->map = std::move(m->idmap);
+            ro->meta = std::move(m->meta);
+            o = ro;
+        }
+        if (r.pos != r.size) throw Error(kRuntimeError, "corrupt file: unexpected data after the index");
+        *kind = static_cast<int>(k);
+        *out = wrap(o);
+    });
+}
+
+// ---- kernels on device memory ----------------------------------------------------
+
+int qg_quantize_lut_dev(const float* tables_dev, size_t n, size_t m, uint8_t* lut_dev, float* scale_dev,
+                        float* offset_dev, void* stream) {
+    return guarded([&] { quantize_luts(tables_dev, nullptr, nullptr, n, m, lut_dev, scale_dev, offset_dev,
+                                        static_cast<cudaStream_t>(stream)); });
+}
+
+int qg_build_quantize_lut_dev(const float* B_dev, const float* C_dev, const float* A_dev, size_t n, size_t m,
+                              uint8_t* lut_dev, float* scale_dev, float* offset_dev, void* stream) {
+    return guarded([&] { quantize_luts(B_dev, C_dev, A_dev, n, m, lut_dev, scale_dev, offset_dev,
+                                        static_cast<cudaStream_t>(stream)); });
+}
+
+int qg_fast_scan_dev(const uint8_t* lut_dev, size_t nluts, size_t m, const uint8_t* codes_dev,
+                     const uint32_t* lut_of_dev, size_t n, uint16_t* sums_dev, void* stream) {
+    return guarded([&] { fast_scan_sums(lut_dev, nluts, m, codes_dev, lut_of_dev, n, sums_dev,
+                                         static_cast<cudaStream_t>(stream)); });
+}
+
+int qg_exact_scores_dev(const float* a_dev, size_t na, const float* b_dev, size_t nb, size_t dim, int ip,
+                        float* out_dev, void* stream) {
+    return guarded([&] {
+        pair_scores(a_dev, static_cast<int>(na), b_dev, static_cast<int>(nb), static_cast<int>(dim), ip != 0, out_dev,
+                    nb, static_cast<cudaStream_t>(stream));
+    });
+}
+
+} // extern "C"

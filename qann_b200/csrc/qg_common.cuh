@@ -1,0 +1,212 @@
+// Shared device/host helpers for the qann B200 search path.
+//
+// Numerics contract: every float operation whose result must match the
+// reference CPU build bit for bit is written with explicit round-to-nearest
+// intrinsics (__fadd_rn, __fmul_rn, __fdiv_rn, __fmaf_rn) and the library is
+// compiled with -fmad=false, so nvcc never fuses a multiply into an add that
+// the reference (built as ISO C++20, where GCC does not contract) rounds twice.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "qg_error.h"
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+namespace qg {
+
+[[noreturn]] inline void throw_cuda(cudaError_t e, const char* what, const char* file, int line) {
+    std::string msg = std::string("CUDA error in ") + what + " (" + file + ":" + std::to_string(line) +
+                      "): " + cudaGetErrorString(e);
+    throw Error(e == cudaErrorMemoryAllocation ? kOutOfMemory : kCudaError, msg);
+}
+
+#define QG_CUDA(call)                                                        \
+    do {                                                                     \
+        cudaError_t qg_e_ = (call);                                          \
+        if (qg_e_ != cudaSuccess) ::qg::throw_cuda(qg_e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define QG_LAUNCH_CHECK() QG_CUDA(cudaGetLastError())
+
+// ---------------------------------------------------------------------------
+// Ordered float keys (reference src/topk.hpp:82-91): a float maps to a uint32
+// that sorts the same way (negative floats flipped, positives with the sign
+// bit set). -0.0f sorts just below +0.0f, as in the reference's TopK.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint32_t float_key(float f) {
+#ifdef __CUDA_ARCH__
+    const uint32_t b = __float_as_uint(f);
+#else
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+#endif
+    return b ^ (static_cast<uint32_t>(static_cast<int32_t>(b) >> 31) | 0x80000000u);
+}
+
+__host__ __device__ __forceinline__ float key_float(uint32_t k) {
+    const uint32_t b = (k & 0x80000000u) ? (k ^ 0x80000000u) : ~k;
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(b);
+#else
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+#endif
+}
+
+// Key for comparisons the reference does on float values with operator<
+// (std::sort / nth_element over (float, slot) pairs, e.g. RefineIndex::rerank):
+// there -0.0f == +0.0f, so both map to +0's key.
+__host__ __device__ __forceinline__ uint32_t float_key_eq0(float f) {
+    return float_key(f == 0.0f ? 0.0f : f);
+}
+
+// ---------------------------------------------------------------------------
+// Exact distances in the reference's AVX2+FMA accumulation order
+// (reference src/distance.cpp:66-96 l2_distance_avx2, :138-151
+// inner_product_avx2). Four 8-lane accumulators over 32-float steps, an
+// 8-float step into accumulator 0, the lane sum
+// ((a0+a1)+(a2+a3)) per lane, then the hsum256 tree
+// ((l0+l4)+(l1+l5)) + ((l2+l6)+(l3+l7)), then the n % 8 tail as the
+// reference's release build (GCC -O3 -mavx2 -mfma) computes `result += d * d`:
+// with 4 or more elements left, four products rounded and added in order
+// (its vectorised epilogue), then one FMA per remaining element.
+//
+// chain(j, L): the FMA chain of accumulator j, lane L.
+// ---------------------------------------------------------------------------
+template <bool kL2>
+__device__ __forceinline__ float exact_tail(const float* __restrict__ a, const float* __restrict__ b, int i, int n,
+                                            float r) {
+    if (n - i >= 4) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            float p;
+            if (kL2) {
+                const float d = __fsub_rn(a[i + e], b[i + e]);
+                p = __fmul_rn(d, d);
+            } else {
+                p = __fmul_rn(a[i + e], b[i + e]);
+            }
+            r = __fadd_rn(r, p);
+        }
+        i += 4;
+    }
+    for (; i < n; ++i) {
+        if (kL2) {
+            const float d = __fsub_rn(a[i], b[i]);
+            r = __fmaf_rn(d, d, r);
+        } else {
+            r = __fmaf_rn(a[i], b[i], r);
+        }
+    }
+    return r;
+}
+
+template <bool kL2>
+__device__ __forceinline__ float exact_avx2(const float* __restrict__ a, const float* __restrict__ b, int n) {
+    const int n32 = n & ~31;
+    const int n8 = n & ~7;     // end of the 8-float steps
+    float t[4];
+#pragma unroll
+    for (int L = 0; L < 4; ++L) {
+        float s[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int lane = L + 4 * h;
+            float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
+            int i = 0;
+            for (; i < n32; i += 32) {
+                if (kL2) {
+                    const float d0 = __fsub_rn(a[i + lane], b[i + lane]);
+                    const float d1 = __fsub_rn(a[i + 8 + lane], b[i + 8 + lane]);
+                    const float d2 = __fsub_rn(a[i + 16 + lane], b[i + 16 + lane]);
+                    const float d3 = __fsub_rn(a[i + 24 + lane], b[i + 24 + lane]);
+                    acc0 = __fmaf_rn(d0, d0, acc0);
+                    acc1 = __fmaf_rn(d1, d1, acc1);
+                    acc2 = __fmaf_rn(d2, d2, acc2);
+                    acc3 = __fmaf_rn(d3, d3, acc3);
+                } else {
+                    acc0 = __fmaf_rn(a[i + lane], b[i + lane], acc0);
+                    acc1 = __fmaf_rn(a[i + 8 + lane], b[i + 8 + lane], acc1);
+                    acc2 = __fmaf_rn(a[i + 16 + lane], b[i + 16 + lane], acc2);
+                    acc3 = __fmaf_rn(a[i + 24 + lane], b[i + 24 + lane], acc3);
+                }
+            }
+            for (; i < n8; i += 8) {
+                if (kL2) {
+                    const float d = __fsub_rn(a[i + lane], b[i + lane]);
+                    acc0 = __fmaf_rn(d, d, acc0);
+                } else {
+                    acc0 = __fmaf_rn(a[i + lane], b[i + lane], acc0);
+                }
+            }
+            s[h] = __fadd_rn(__fadd_rn(acc0, acc1), __fadd_rn(acc2, acc3));
+        }
+        t[L] = __fadd_rn(s[0], s[1]);
+    }
+    float r = __fadd_rn(__fadd_rn(t[0], t[1]), __fadd_rn(t[2], t[3]));
+    return exact_tail<kL2>(a, b, n8, n, r);
+}
+
+// The score the reference's DenseIndex ranks by (reference
+// include/vecengine/index.hpp:269-271): squared L2, or -(a . b) for inner product.
+__device__ __forceinline__ float exact_score(const float* a, const float* b, int n, bool ip) {
+    return ip ? -exact_avx2<false>(a, b, n) : exact_avx2<true>(a, b, n);
+}
+
+// ---------------------------------------------------------------------------
+// Small host utilities
+// ---------------------------------------------------------------------------
+inline size_t ceil_div(size_t a, size_t b) { return (a + b - 1) / b; }
+
+// Number of SMs of the current device (cached per device by the caller).
+inline int sm_count() {
+    int dev = 0, n = 0;
+    QG_CUDA(cudaGetDevice(&dev));
+    QG_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    return n;
+}
+
+// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync on one stream).
+template <class T>
+struct DevBuf {
+    T* ptr = nullptr;
+    size_t count = 0;
+    cudaStream_t stream = nullptr;
+
+    DevBuf() = default;
+    DevBuf(size_t n, cudaStream_t s) { alloc(n, s); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), count(o.count), stream(o.stream) { o.ptr = nullptr; o.count = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            ptr = o.ptr; count = o.count; stream = o.stream;
+            o.ptr = nullptr; o.count = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+
+    void alloc(size_t n, cudaStream_t s) {
+        release();
+        stream = s;
+        count = n;
+        if (n) QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), s));
+    }
+    void release() noexcept {
+        if (ptr) cudaFreeAsync(ptr, stream);
+        ptr = nullptr;
+        count = 0;
+    }
+    T* get() const { return ptr; }
+    size_t bytes() const { return count * sizeof(T); }
+};
+
+} // namespace qg

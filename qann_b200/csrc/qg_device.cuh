@@ -1,0 +1,235 @@
+// Device building blocks of the search path: block-wide bitonic sort, the
+// bit-exact uint8 LUT quantisation, the reference's PQ table terms, and the
+// register-resident 4-bit lookup of the code scan.
+#pragma once
+
+#include "qg_common.cuh"
+
+namespace qg {
+
+inline constexpr int kLutMax = 63;   // reference src/fast_scan.hpp:36-39
+
+// ---------------------------------------------------------------------------
+// Block-wide bitonic sort of n (a power of two) (key, val) pairs in shared
+// memory, ascending by (key, val). Every thread of the block must call it.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool pair_less(uint64_t ka, int64_t va, uint64_t kb, int64_t vb) {
+    return ka < kb || (ka == kb && va < vb);
+}
+
+__device__ __noinline__ static void bitonic_sort(uint64_t* key, int64_t* val, int n) {
+    for (int size = 2; size <= n; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            __syncthreads();
+            for (int t = threadIdx.x; t < (n >> 1); t += blockDim.x) {
+                const int lo = 2 * t - (t & (stride - 1));
+                const int hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const uint64_t k0 = key[lo], k1 = key[hi];
+                const int64_t v0 = val[lo], v1 = val[hi];
+                const bool swap = up ? pair_less(k1, v1, k0, v0) : pair_less(k0, v0, k1, v1);
+                if (swap) {
+                    key[lo] = k1; key[hi] = k0;
+                    val[lo] = v1; val[hi] = v0;
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+__host__ __device__ __forceinline__ int next_pow2(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// Block reductions
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float warp_max(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// Rounding an m x 16 float table to uint8 entries, bit-exact with the
+// reference's quantize_lut (reference src/fast_scan.cpp:18-46 scalar,
+// :164-192 AVX2; both give the same bytes):
+//   row minimum / maximum over its 16 entries (exact in any order),
+//   widest = max over rows of (max - min),
+//   scale  = 63 / widest (IEEE division), or 1 when every row is constant,
+//   offset = (p0 + p1) + (p2 + p3), p[i % 4] summing the row minimums in row order,
+//   lut    = round-half-even((x - min) * scale), subtract and multiply rounded apart.
+// Implemented for one warp working on a table in shared memory; the LUT rows
+// are written as four 32-bit words (entries 0-3, 4-7, 8-11, 12-15).
+// row_min: m floats of warp-private shared scratch.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
+    return static_cast<uint32_t>(a) | (static_cast<uint32_t>(b) << 8) | (static_cast<uint32_t>(c) << 16) |
+           (static_cast<uint32_t>(d) << 24);
+}
+
+// The table row r is produced on demand by row(r, v) (16 floats), which lets
+// callers fuse the table sum (B + C + A) into the rounding as the reference's
+// build_quantize_lut does. Returns scale / offset to every lane.
+template <class RowFn>
+__device__ void warp_quantize_lut(RowFn row, int m, int m_pad, float* row_min, uint4* lut_out, float& scale_out,
+                                  float& offset_out) {
+    const int lane = threadIdx.x & 31;
+    float widest = 0.0f;
+    for (int r = lane; r < m; r += 32) {
+        float v[16];
+        row(r, v);
+        float lo = v[0], hi = v[0];
+#pragma unroll
+        for (int j = 1; j < 16; ++j) {
+            lo = fminf(lo, v[j]);
+            hi = fmaxf(hi, v[j]);
+        }
+        row_min[r] = lo;
+        const float w = __fsub_rn(hi, lo);
+        widest = widest < w ? w : widest;   // std::max(widest, w)
+    }
+    widest = warp_max(widest);
+    __syncwarp();
+    float part = 0.0f;
+    if (lane < 4)
+        for (int r = lane; r < m; r += 4) part = __fadd_rn(part, row_min[r]);
+    const float p0 = __shfl_sync(0xffffffffu, part, 0), p1 = __shfl_sync(0xffffffffu, part, 1);
+    const float p2 = __shfl_sync(0xffffffffu, part, 2), p3 = __shfl_sync(0xffffffffu, part, 3);
+    const float offset = __fadd_rn(__fadd_rn(p0, p1), __fadd_rn(p2, p3));
+    const float scale = widest > 0.0f ? __fdiv_rn(static_cast<float>(kLutMax), widest) : 1.0f;
+    for (int r = lane; r < m_pad; r += 32) {
+        if (r >= m) {
+            lut_out[r] = make_uint4(0, 0, 0, 0);
+            continue;
+        }
+        float v[16];
+        row(r, v);
+        const float mn = row_min[r];
+        int q[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) q[j] = __float2int_rn(__fmul_rn(__fsub_rn(v[j], mn), scale));
+        lut_out[r] = make_uint4(pack4(q[0], q[1], q[2], q[3]), pack4(q[4], q[5], q[6], q[7]),
+                                pack4(q[8], q[9], q[10], q[11]), pack4(q[12], q[13], q[14], q[15]));
+    }
+    scale_out = scale;
+    offset_out = offset;
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// PQ table terms, bit-exact with the reference (reference src/pq.cpp):
+//   inner (C): out[s][k] = sum_j ((-2 * q[s*sd+j]) * y[s][j][k])   (:186-204)
+//   list  (B): out[s][k] = sum_j y * (y + 2 * c[s*sd+j])            (:206-223)
+//   adc      : out[s][k] = sum_j (q - y)^2                          (:165-184)
+// y is the transposed codebook, m * sd * K floats. The reference's release
+// build (GCC, C++, -mfma; CMakeLists.txt:63-68) fuses each `out += a * b`
+// into one FMA (GCC's default -ffp-contract=fast in C++ modes), so these do too.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float inner_term(const float* q, const float* yt, int s, int sd, int K, int k) {
+    float out = 0.0f;
+    for (int j = 0; j < sd; ++j) {
+        out = __fmaf_rn(__fmul_rn(-2.0f, q[s * sd + j]), yt[(s * sd + j) * K + k], out);
+    }
+    return out;
+}
+
+__device__ __forceinline__ float list_term(const float* c, const float* yt, int s, int sd, int K, int k) {
+    float out = 0.0f;
+    for (int j = 0; j < sd; ++j) {
+        const float y = yt[(s * sd + j) * K + k];
+        out = __fmaf_rn(y, __fadd_rn(y, __fmul_rn(2.0f, c[s * sd + j])), out);
+    }
+    return out;
+}
+
+__device__ __forceinline__ float adc_term(const float* r, const float* yt, int s, int sd, int K, int k) {
+    float out = 0.0f;
+    for (int j = 0; j < sd; ++j) {
+        const float diff = __fsub_rn(r[s * sd + j], yt[(s * sd + j) * K + k]);
+        out = __fmaf_rn(diff, diff, out);
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// 4-bit lookups from registers. prmt.b32 picks four bytes out of eight by
+// four 4-bit selectors; a selector with its top bit set yields the sign of the
+// picked byte (0x00 for LUT entries, which are <= 63). So with the 16-entry
+// row as words L0..L3:
+//   prmt(L0, L1, codes)          = entry c for codes c < 8, 0 otherwise
+//   prmt(L2, L3, codes ^ 0x8888) = entry c for codes c >= 8, 0 otherwise
+// and their sum is the lookup of four codes at once, one byte each.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+    uint32_t d;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+    return d;
+}
+
+// Device code layout (built from the file format's blocks, see qg_lists.cu):
+// a list is stored in superblocks of 64 vectors. Octet lane r (0..7) owns
+// vectors 8r..8r+7; its word for subspace s holds their codes, vector 8r+i
+// in nibble i. Words are interleaved so each 16-byte load of the 8 lanes is
+// one 128-byte line: uint4 index (s/4)*8 + r holds subspaces s..s+3.
+inline constexpr int kSuperBlock = 64;
+
+// Sums of the 8 vectors of one octet lane over m_pad subspaces (m_pad % 4 == 0).
+// lut: m_pad rows as uint4 (shared memory). Sums are exact uint16 values
+// (m_pad * 63 <= 64512).
+__device__ __forceinline__ void octet_sums(const uint4* __restrict__ sb, const uint4* __restrict__ lut, int m_pad,
+                                           int r, uint32_t sums[8]) {
+    uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+    const int nq = m_pad >> 2;
+    for (int q = 0; q < nq; ++q) {
+        const uint4 w = __ldg(sb + q * 8 + r);
+        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+        uint32_t g0 = 0, g1 = 0;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const uint4 L = lut[4 * q + t];
+            const uint32_t c = ws[t];
+            const uint32_t cx = c ^ 0x88888888u;
+            g0 += prmt(L.x, L.y, c) + prmt(L.z, L.w, cx);
+            g1 += prmt(L.x, L.y, c >> 16) + prmt(L.z, L.w, cx >> 16);
+        }
+        a0 += g0 & 0x00FF00FFu;
+        b0 += (g0 >> 8) & 0x00FF00FFu;
+        a1 += g1 & 0x00FF00FFu;
+        b1 += (g1 >> 8) & 0x00FF00FFu;
+    }
+    sums[0] = a0 & 0xFFFFu;
+    sums[1] = b0 & 0xFFFFu;
+    sums[2] = a0 >> 16;
+    sums[3] = b0 >> 16;
+    sums[4] = a1 & 0xFFFFu;
+    sums[5] = b1 & 0xFFFFu;
+    sums[6] = a1 >> 16;
+    sums[7] = b1 >> 16;
+}
+
+// Fast-scan distance of an integer sum: sums / scale + offset, an IEEE
+// division then an add (reference src/ivf_index.cpp:496).
+__device__ __forceinline__ float fs_dist(uint32_t sum, float scale, float offset) {
+    return __fadd_rn(__fdiv_rn(static_cast<float>(sum), scale), offset);
+}
+
+// Largest integer sum whose distance has key <= thr_key, or -1 when none;
+// 65535 when every sum passes. Distances grow monotonically with the sum, so
+// the exact float test `key(dist(S)) <= thr_key` becomes `S <= result`.
+__device__ __forceinline__ int sum_limit(uint32_t thr_key, float scale, float offset) {
+    if (thr_key == 0xFFFFFFFFu) return 65535;
+    // binary search of the monotone predicate over [-1, 65535]: 17 steps
+    int lo = -1, hi = 65535;   // invariant: pred(lo) true (or lo == -1), pred(hi + 1) false
+    if (float_key(fs_dist(65535u, scale, offset)) <= thr_key) return 65535;
+    while (lo < hi - 1) {
+        const int mid = (lo + hi) >> 1;
+        if (float_key(fs_dist(static_cast<uint32_t>(mid), scale, offset)) <= thr_key) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+} // namespace qg

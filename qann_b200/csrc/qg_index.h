@@ -1,0 +1,99 @@
+// Index objects behind the C ABI: the host model (canonical, what save()
+// writes) plus its device copy, rebuilt lazily after writes.
+#pragma once
+
+#include "qg_common.cuh"
+#include "qg_host.h"
+#include "qg_search.h"
+
+#include <memory>
+#include <mutex>
+#include <shared_mutex>
+
+namespace qg {
+
+// Device copy of an IVF fast-scan index.
+struct DeviceIVF {
+    IvfView view;
+    DevBuf<float> centroids, resid, sqnorm, pq_t, B;
+    DevBuf<uint32_t> sb_off, list_size, ids;
+    DevBuf<uint4> codes;
+    DevBuf<uint64_t> deleted;
+    DevBuf<int64_t> labels;   // slot -> id when the ids are not the slots
+    size_t total_sb = 0;
+};
+
+// Device rows of a FlatIndex or of a RefineIndex's raw vectors.
+struct DeviceRows {
+    DevBuf<float> rows;
+    DevBuf<int64_t> labels;
+    DevBuf<uint64_t> deleted;
+};
+
+struct IndexObj {
+    Kind kind;
+    mutable std::shared_mutex mu;     // shared for queries, exclusive for writes
+    std::mutex dev_mu;                // guards (re)building the device copy
+    bool dev_dirty = true;
+    bool wrapped = false;             // a RefineIndex wraps this index
+    int device = 0;
+    explicit IndexObj(Kind k) : kind(k) {}
+    virtual ~IndexObj() = default;
+    virtual size_t dim() const = 0;
+    virtual Metric metric() const = 0;
+    virtual IdMap& idmap() = 0;
+    virtual const IdMap& idmap() const = 0;
+};
+
+struct IVFObj : IndexObj {
+    IVFModel model;
+    DeviceIVF dev;
+    IVFObj() : IndexObj(Kind::IVF) {}
+    size_t dim() const override { return model.dim; }
+    Metric metric() const override { return model.metric; }
+    IdMap& idmap() override { return model.idmap; }
+    const IdMap& idmap() const override { return model.idmap; }
+    bool precomputed_available() const;
+    int scan_mode() const;
+};
+
+struct FlatObj : IndexObj {
+    FlatModel model;
+    DeviceRows dev;
+    FlatObj() : IndexObj(Kind::Flat) {}
+    size_t dim() const override { return model.dim; }
+    Metric metric() const override { return model.metric; }
+    IdMap& idmap() override { return model.idmap; }
+    const IdMap& idmap() const override { return model.idmap; }
+};
+
+struct RefineObj : IndexObj {
+    std::shared_ptr<IndexObj> base;
+    uint64_t k_factor = 10;
+    std::vector<float> data;   // slots * dim raw rows
+    IdMap map;
+    MetaBlob meta;
+    DeviceRows dev;
+    RefineObj() : IndexObj(Kind::Refine) {}
+    ~RefineObj() override {
+        if (base) base->wrapped = false;
+    }
+    size_t dim() const override { return base->dim(); }
+    Metric metric() const override { return base->metric(); }
+    IdMap& idmap() override { return map; }
+    const IdMap& idmap() const override { return map; }
+};
+
+// Builds / refreshes the device copy (callers hold the object's lock).
+void ensure_device(IVFObj& o, cudaStream_t st);
+void ensure_device(FlatObj& o, cudaStream_t st);
+void ensure_device(RefineObj& o, cudaStream_t st);
+
+// Packs plain codes (n x m bytes, lists concatenated in order) into the
+// device superblock layout. sb_list: the list of each superblock; voff: the
+// first vector of each list in `codes`; sb_off: first superblock of each list.
+void pack_superblocks(const uint8_t* codes_dev, const uint32_t* ids_dev, const uint32_t* voff_dev,
+                      const uint32_t* sb_off_dev, const uint32_t* list_size_dev, const uint32_t* sb_list_dev,
+                      size_t total_sb, int m, int m_pad, uint4* out_codes, uint32_t* out_ids, cudaStream_t st);
+
+} // namespace qg

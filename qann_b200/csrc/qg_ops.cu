@@ -1,0 +1,296 @@
+// Search dispatch over the index kinds, flat exact search, and the pieces of
+// add (nearest-centroid assignment, PQ encoding) that run on the GPU.
+#include "qg_device.cuh"
+#include "qg_ops.h"
+
+#include <algorithm>
+#include <numeric>
+
+namespace qg {
+
+// ---------------------------------------------------------------------------
+// Flat exact search: tiles of rows scored for a block of queries, each tile's
+// k best per query (by (score, slot), -0 == +0 as the reference's heap of
+// (float, slot) pairs compares; reference src/flat_index.cpp:33-64) merged
+// into the running k best.
+// ---------------------------------------------------------------------------
+__global__ void k_cols_to_keys(const uint32_t* __restrict__ col, const float* __restrict__ score, size_t n, int P,
+                               int k, size_t col_base, uint64_t* __restrict__ key, uint32_t* __restrict__ slot) {
+    const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n * k) return;
+    const size_t row = t / k;
+    const int j = static_cast<int>(t % k);
+    if (j < P && col[row * P + j] != 0xFFFFFFFFu) {
+        const uint64_t s = col_base + col[row * P + j];
+        key[t] = (static_cast<uint64_t>(float_key_eq0(score[row * P + j])) << 32) | s;
+        slot[t] = static_cast<uint32_t>(s);
+    } else {
+        key[t] = ~0ull;
+        slot[t] = 0xFFFFFFFFu;
+    }
+}
+
+// merges running (a) and tile (b) lists of k into a, per query
+__global__ void __launch_bounds__(256) k_merge2(uint64_t* __restrict__ akey, uint32_t* __restrict__ aslot,
+                                                const uint64_t* __restrict__ bkey, const uint32_t* __restrict__ bslot,
+                                                int k) {
+    extern __shared__ uint8_t sm_raw[];
+    const int n = next_pow2(2 * k);
+    uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);
+    int64_t* val = reinterpret_cast<int64_t*>(key + n);
+    const size_t base = static_cast<size_t>(blockIdx.x) * k;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        if (i < k) {
+            key[i] = akey[base + i];
+            val[i] = aslot[base + i];
+        } else if (i < 2 * k) {
+            key[i] = bkey[base + i - k];
+            val[i] = bslot[base + i - k];
+        } else {
+            key[i] = ~0ull;
+            val[i] = INT64_MAX;
+        }
+    }
+    bitonic_sort(key, val, n);
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        akey[base + i] = key[i];
+        aslot[base + i] = key[i] == ~0ull ? 0xFFFFFFFFu : static_cast<uint32_t>(val[i]);
+    }
+}
+
+void flat_candidates(const float* q_dev, size_t nq, const float* rows_dev, size_t n, int dim, bool ip, size_t k,
+                     const uint64_t* allow_dev, const uint64_t* deny_dev, uint64_t* out_key, uint32_t* out_slot,
+                     cudaStream_t st) {
+    if (nq == 0 || k == 0) return;
+    require(k <= 4096, "k above 4096 is not supported by the GPU flat search", kUnsupported);
+    QG_CUDA(cudaMemsetAsync(out_key, 0xFF, nq * k * sizeof(uint64_t), st));
+    QG_CUDA(cudaMemsetAsync(out_slot, 0xFF, nq * k * sizeof(uint32_t), st));
+    if (n == 0) return;
+    const size_t QB = std::min<size_t>(nq, 4096);
+    const size_t T = std::min<size_t>(n, std::max<size_t>(k, (size_t{256} << 20) / (QB * sizeof(float))));
+    DevBuf<float> scores(QB * T, st);
+    DevBuf<uint32_t> col(QB * std::min(k, T), st);
+    DevBuf<float> sc(QB * std::min(k, T), st);
+    DevBuf<uint64_t> tkey(QB * k, st);
+    DevBuf<uint32_t> tslot(QB * k, st);
+    const int msm_n = next_pow2(static_cast<int>(2 * k));
+    const size_t msm = static_cast<size_t>(msm_n) * 16;
+    if (msm > 48 * 1024)
+        QG_CUDA(cudaFuncSetAttribute(k_merge2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm)));
+    for (size_t q0 = 0; q0 < nq; q0 += QB) {
+        const size_t nb = std::min(QB, nq - q0);
+        for (size_t r0 = 0; r0 < n; r0 += T) {
+            const size_t nr = std::min(T, n - r0);
+            const int P = static_cast<int>(std::min(k, nr));
+            pair_scores(q_dev + q0 * dim, static_cast<int>(nb), rows_dev + r0 * dim, static_cast<int>(nr), dim, ip,
+                        scores.get(), nr, st);
+            select_rows(scores.get(), nr, static_cast<int>(nb), static_cast<int>(nr), P, col.get(), sc.get(), st,
+                        allow_dev, deny_dev, r0, true);
+            k_cols_to_keys<<<static_cast<unsigned>(ceil_div(nb * k, 256)), 256, 0, st>>>(col.get(), sc.get(), nb, P,
+                                                                                        static_cast<int>(k), r0,
+                                                                                        tkey.get(), tslot.get());
+            QG_LAUNCH_CHECK();
+            k_merge2<<<static_cast<unsigned>(nb), 256, msm, st>>>(out_key + q0 * k, out_slot + q0 * k, tkey.get(),
+                                                                   tslot.get(), static_cast<int>(k));
+            QG_LAUNCH_CHECK();
+        }
+    }
+}
+
+// Flat results in (score, slot) order with ids and the exact score.
+__global__ void k_finalize_flat(const float* __restrict__ q, int dim, const float* __restrict__ rows,
+                                const uint32_t* __restrict__ slot, int k, bool ip, const int64_t* __restrict__ labels,
+                                bool cosine, int64_t* __restrict__ out_ids, float* __restrict__ out_d, size_t nq) {
+    const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= nq * k) return;
+    const size_t qi = t / k;
+    const uint32_t s = slot[t];
+    if (s == 0xFFFFFFFFu) {
+        out_ids[t] = -1;
+        out_d[t] = __int_as_float(0x7f800000);
+        return;
+    }
+    const float d = exact_score(rows + static_cast<size_t>(s) * dim, q + qi * dim, dim, ip);
+    out_ids[t] = labels ? labels[s] : static_cast<int64_t>(s);
+    out_d[t] = cosine ? __fmul_rn(d, 0.5f) : d;
+}
+
+// ---------------------------------------------------------------------------
+// Search dispatch
+// ---------------------------------------------------------------------------
+static int sm_count_cached() {
+    static int n = 0;
+    if (!n) n = sm_count();
+    return n;
+}
+
+namespace {
+struct Prepared {
+    DevBuf<float> q;     // prepared queries (normalised for cosine)
+    DevBuf<uint64_t> filter;
+    DevBuf<int> err;
+};
+} // namespace
+
+static void prepare(IndexObj& idx, const SearchRequest& r, Prepared& p, cudaStream_t st) {
+    const size_t dim = idx.dim();
+    const size_t n = r.nq * dim;
+    p.err.alloc(2, st);
+    QG_CUDA(cudaMemsetAsync(p.err.get(), 0, 2 * sizeof(int), st));
+    DevBuf<float> raw;
+    const float* src = r.q;
+    if (r.io == IoSpace::Host) {
+        raw.alloc(n, st);
+        QG_CUDA(cudaMemcpyAsync(raw.get(), r.q, n * sizeof(float), cudaMemcpyHostToDevice, st));
+        src = raw.get();
+    }
+    p.q.alloc(n, st);
+    if (idx.metric() == Metric::Cosine) {
+        normalize_rows(src, p.q.get(), static_cast<int>(r.nq), static_cast<int>(dim), p.err.get() + 1, st);
+    } else {
+        QG_CUDA(cudaMemcpyAsync(p.q.get(), src, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    }
+    if (r.filter) {
+        p.filter.alloc(r.filter->words.size(), st);
+        QG_CUDA(cudaMemcpyAsync(p.filter.get(), r.filter->words.data(), r.filter->words.size() * 8,
+                                cudaMemcpyHostToDevice, st));
+    }
+}
+
+static void fill_empty(const SearchRequest& r, cudaStream_t st) {
+    const size_t n = r.nq * r.k;
+    if (!n) return;
+    std::vector<int64_t> ids(n, -1);
+    std::vector<float> d(n, std::numeric_limits<float>::infinity());
+    if (r.io == IoSpace::Host) {
+        std::copy(ids.begin(), ids.end(), r.out_ids);
+        std::copy(d.begin(), d.end(), r.out_d);
+    } else {
+        QG_CUDA(cudaMemcpyAsync(r.out_ids, ids.data(), n * 8, cudaMemcpyHostToDevice, st));
+        QG_CUDA(cudaMemcpyAsync(r.out_d, d.data(), n * 4, cudaMemcpyHostToDevice, st));
+        QG_CUDA(cudaStreamSynchronize(st));
+    }
+}
+
+static void check_err(const DevBuf<int>& err, cudaStream_t st) {
+    int h[2] = {0, 0};
+    QG_CUDA(cudaMemcpyAsync(h, err.get(), sizeof(h), cudaMemcpyDeviceToHost, st));
+    QG_CUDA(cudaStreamSynchronize(st));
+    if (h[1]) throw Error(kInvalidArgument, "cosine metric needs non-zero vectors");
+    if (h[0]) throw Error(kRuntimeError, "fast-scan candidate buffer overflowed (internal error)");
+}
+
+void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
+    if (r.nq == 0) return;
+    const bool empty_filter = r.filter && r.filter->count == 0;
+    if (r.k == 0) return;
+    const int dim = static_cast<int>(idx.dim());
+    const bool cosine = idx.metric() == Metric::Cosine;
+    const bool ip = idx.metric() == Metric::InnerProduct;
+    // output staging
+    DevBuf<int64_t> o_ids;
+    DevBuf<float> o_d;
+    int64_t* out_ids = r.out_ids;
+    float* out_d = r.out_d;
+    if (r.io == IoSpace::Host) {
+        o_ids.alloc(r.nq * r.k, st);
+        o_d.alloc(r.nq * r.k, st);
+        out_ids = o_ids.get();
+        out_d = o_d.get();
+    }
+    auto finish = [&](const Prepared& p) {
+        if (r.io == IoSpace::Host) {
+            QG_CUDA(cudaMemcpyAsync(r.out_ids, out_ids, r.nq * r.k * 8, cudaMemcpyDeviceToHost, st));
+            QG_CUDA(cudaMemcpyAsync(r.out_d, out_d, r.nq * r.k * 4, cudaMemcpyDeviceToHost, st));
+        }
+        check_err(p.err, st);
+    };
+
+    if (idx.kind == Kind::IVF) {
+        auto& o = static_cast<IVFObj&>(idx);
+        if (empty_filter || o.model.idmap.live_count() == 0) {
+            fill_empty(r, st);
+            return;
+        }
+        require(r.filter == nullptr, "filtered queries on a bare IVFIndex are not on the GPU path yet", kUnsupported);
+        ensure_device(o, st);
+        Prepared p;
+        prepare(idx, r, p, st);
+        const int kp = static_cast<int>(r.k);
+        require(kp <= 3072, "k above 3072 is not supported by the GPU fast-scan", kUnsupported);
+        DevBuf<uint64_t> ck(r.nq * kp, st);
+        DevBuf<uint32_t> cs(r.nq * kp, st);
+        IvfSearchArgs a;
+        a.q = p.q.get();
+        a.nq = static_cast<int>(r.nq);
+        a.k = static_cast<int>(r.k);
+        a.kp = kp;
+        a.nprobe = static_cast<int>(o.model.nprobe);
+        a.filter = nullptr;
+        a.sm_count = sm_count_cached();
+        a.d_err = p.err.get();
+        ivf_candidates(o.dev.view, a, ck.get(), cs.get(), st);
+        finalize_ivf(ck.get(), cs.get(), a.nq, kp, a.k, o.dev.labels.get(), cosine, out_ids, out_d, st);
+        finish(p);
+        return;
+    }
+
+    if (idx.kind == Kind::Flat) {
+        auto& o = static_cast<FlatObj&>(idx);
+        if (empty_filter || o.model.idmap.live_count() == 0) {
+            fill_empty(r, st);
+            return;
+        }
+        ensure_device(o, st);
+        Prepared p;
+        prepare(idx, r, p, st);
+        DevBuf<uint64_t> ck(r.nq * r.k, st);
+        DevBuf<uint32_t> cs(r.nq * r.k, st);
+        flat_candidates(p.q.get(), r.nq, o.dev.rows.get(), o.model.idmap.slots(), dim, ip, r.k, p.filter.get(),
+                        r.filter ? nullptr : o.dev.deleted.get(), ck.get(), cs.get(), st);
+        k_finalize_flat<<<static_cast<unsigned>(ceil_div(r.nq * r.k, 256)), 256, 0, st>>>(
+            p.q.get(), dim, o.dev.rows.get(), cs.get(), static_cast<int>(r.k), ip, o.dev.labels.get(), cosine, out_ids,
+            out_d, r.nq);
+        QG_LAUNCH_CHECK();
+        finish(p);
+        return;
+    }
+
+    // RefineIndex
+    auto& o = static_cast<RefineObj&>(idx);
+    const size_t live = r.filter ? r.filter->count : o.map.live_count();
+    if (empty_filter || o.map.live_count() == 0) {
+        fill_empty(r, st);
+        return;
+    }
+    ensure_device(o, st);
+    Prepared p;
+    prepare(idx, r, p, st);
+    const size_t kp = std::min(r.k * o.k_factor, live);
+    require(kp <= 3072, "k * k_factor above 3072 is not supported by the GPU path", kUnsupported);
+    DevBuf<uint64_t> ck(r.nq * kp, st);
+    DevBuf<uint32_t> cs(r.nq * kp, st);
+    if (o.base->kind == Kind::IVF) {
+        auto& b = static_cast<IVFObj&>(*o.base);
+        require(r.filter == nullptr, "filtered queries through an IVF base are not on the GPU path yet", kUnsupported);
+        IvfSearchArgs a;
+        a.q = p.q.get();
+        a.nq = static_cast<int>(r.nq);
+        a.k = static_cast<int>(r.k);
+        a.kp = static_cast<int>(kp);
+        a.nprobe = static_cast<int>(b.model.nprobe);
+        a.filter = p.filter.get();
+        a.sm_count = sm_count_cached();
+        a.d_err = p.err.get();
+        ivf_candidates(b.dev.view, a, ck.get(), cs.get(), st);
+    } else {
+        auto& b = static_cast<FlatObj&>(*o.base);
+        flat_candidates(p.q.get(), r.nq, b.dev.rows.get(), b.model.idmap.slots(), dim, ip, kp, p.filter.get(),
+                        r.filter ? nullptr : b.dev.deleted.get(), ck.get(), cs.get(), st);
+    }
+    refine_candidates(p.q.get(), static_cast<int>(r.nq), dim, o.dev.rows.get(), ck.get(), cs.get(), static_cast<int>(kp),
+                      static_cast<int>(r.k), ip, o.dev.labels.get(), cosine, out_ids, out_d, st);
+    finish(p);
+}
+
+} // namespace qg

@@ -1,0 +1,56 @@
+// Operations on index objects: search, add, train. Callers hold the object's
+// lock (shared for search, exclusive for the rest).
+#pragma once
+
+#include "qg_index.h"
+
+namespace qg {
+
+// Where the query and result buffers live.
+enum class IoSpace { Host, Device };
+
+struct SearchRequest {
+    const float* q = nullptr;        // nq * dim
+    size_t nq = 0, k = 0;
+    const SlotBits* filter = nullptr;   // host bitmap of allowed slots, or null
+    int64_t* out_ids = nullptr;      // nq * k
+    float* out_d = nullptr;
+    IoSpace io = IoSpace::Host;
+};
+
+// Runs a batch query on `st` and, for host I/O, waits for it.
+void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st);
+
+// add()'s argument checks alone, so they fail before any CUDA work.
+void validate_add(const IndexObj& idx, size_t n, const int64_t* ids);
+
+// Adds n vectors (host rows); returns their ids in out_ids (may be null).
+void add(IndexObj& idx, const float* x, size_t n, const int64_t* ids, int64_t* out_ids, cudaStream_t st);
+
+// IVFIndex::train on the GPU.
+void train(IVFObj& o, const float* x, size_t n, size_t max_iters, int64_t seed, int clustering, size_t passes,
+           cudaStream_t st);
+
+// Flat exact search over device rows: the k smallest by (score, slot) per
+// query, as (key64 = key_eq0(score) << 32 | slot) sorted lists of length k.
+void flat_candidates(const float* q_dev, size_t nq, const float* rows_dev, size_t n, int dim, bool ip, size_t k,
+                     const uint64_t* allow_dev, const uint64_t* deny_dev, uint64_t* out_key, uint32_t* out_slot,
+                     cudaStream_t st);
+
+// Nearest centroid (squared L2, first index on ties) of each row, as the
+// reference's assign_nearest without BLAS (reference src/kmeans.cpp:34-115).
+void assign_nearest(const float* x_dev, size_t n, const float* c_dev, size_t k, int dim, uint32_t* out_dev,
+                    cudaStream_t st);
+
+// Drops deleted slots (IndexBase::compact); *reclaimed = slots freed.
+void compact(IndexObj& idx, size_t* reclaimed);
+
+// Kernel-level entry points (qg_tools.cu): n tables rounded to uint8 LUTs
+// (C == null: the tables are B; else B + C, plus A on row 0 when A != null),
+// and fast-scan sums of plain codes with one LUT per 64 vectors.
+void quantize_luts(const float* B, const float* C, const float* A, size_t n, size_t m, uint8_t* lut, float* scale,
+                   float* offset, cudaStream_t st);
+void fast_scan_sums(const uint8_t* lut, size_t nluts, size_t m, const uint8_t* codes, const uint32_t* lut_of, size_t n,
+                    uint16_t* sums, cudaStream_t st);
+
+} // namespace qg

@@ -1,0 +1,807 @@
+// The IVF fast-scan + refine query path on the GPU.
+//
+// One search call runs, on one stream:
+//   k_normalize       cosine queries to unit length (reference src/index.cpp:193-218)
+//   coarse            every (query, centroid) exact score in the reference's
+//                     AVX2 order, then the nprobe smallest by (score, list)
+//                     (reference src/ivf_index.cpp:305-356)
+//   k_probe_terms     per-probe distance terms A / base (reference :526-529, :577-579)
+//   k_query_tables    per-query C table, or the per-query uint8 LUT for inner
+//                     product scoring (reference :436-456)
+//   k_scan            per (query, probe chunk): LUT build in shared memory,
+//                     4-bit lookups from registers, fused top-k' selection
+//                     (reference :421-641 and src/topk.hpp)
+//   k_merge           per query: the k' best of its chunks
+//   k_finalize_ivf /  the k results, sorted by (distance, id) (reference
+//   k_refine          src/topk.hpp:53-77), or re-ranked with exact distances
+//                     from the raw rows (reference src/refine_index.cpp:112-140)
+#include "qg_device.cuh"
+#include "qg_search.h"
+
+#include <algorithm>
+#include <vector>
+
+namespace qg {
+
+// ---------------------------------------------------------------------------
+// Cosine normalisation: one thread per row, the row's sum of squares in
+// double in index order (each `sum += x * x` one double FMA, as the
+// reference's GCC build contracts it), scale = float(1 / sqrt(sum)), x * scale.
+// ---------------------------------------------------------------------------
+__global__ void k_normalize(const float* __restrict__ x, float* __restrict__ y, int n, int d, int* zero_row) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* r = x + static_cast<size_t>(i) * d;
+    double s = 0.0;
+    for (int j = 0; j < d; ++j) {
+        const double v = static_cast<double>(r[j]);
+        s = __fma_rn(v, v, s);
+    }
+    const double len = __dsqrt_rn(s);
+    float* o = y + static_cast<size_t>(i) * d;
+    if (len == 0.0) {
+        atomicExch(zero_row, 1);
+        for (int j = 0; j < d; ++j) o[j] = 0.0f;
+        return;
+    }
+    const float scale = __double2float_rn(__ddiv_rn(1.0, len));
+    for (int j = 0; j < d; ++j) o[j] = __fmul_rn(r[j], scale);
+}
+
+// ---------------------------------------------------------------------------
+// All-pairs exact scores, out[i * nb + j] = score(a_i, b_j), in the AVX2
+// chain order of exact_avx2 (qg_common.cuh). Tiles of 16 rows of a x 32 rows
+// of b; each thread keeps the 32 chain accumulators of two pairs while the
+// 32-float chunks of the rows stream through shared memory.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kTA = 16, kTB = 32;
+}
+
+template <bool kIP>
+__global__ void __launch_bounds__(256) k_pair_scores(const float* __restrict__ A, int na, const float* __restrict__ Bm,
+                                                     int nb, int d, float* __restrict__ out, size_t ld_out) {
+    __shared__ float sa[kTA][33];
+    __shared__ float sb[kTB][33];
+    const int ta = threadIdx.x >> 4;          // 0..15: row of a
+    const int tb = threadIdx.x & 15;          // pairs (tb) and (tb + 16) of b
+    const int a0 = blockIdx.y * kTA, b0 = blockIdx.x * kTB;
+    float acc[2][4][8];
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int L = 0; L < 8; ++L) acc[p][j][L] = 0.0f;
+
+    const int n32 = d & ~31;
+    auto stage = [&](int base, int len) {
+        for (int e = threadIdx.x; e < kTA * 32; e += 256) {
+            const int r = e >> 5, c = e & 31;
+            const int gi = a0 + r;
+            sa[r][c] = (gi < na && c < len) ? A[static_cast<size_t>(gi) * d + base + c] : 0.0f;
+        }
+        for (int e = threadIdx.x; e < kTB * 32; e += 256) {
+            const int r = e >> 5, c = e & 31;
+            const int gj = b0 + r;
+            sb[r][c] = (gj < nb && c < len) ? Bm[static_cast<size_t>(gj) * d + base + c] : 0.0f;
+        }
+    };
+    for (int base = 0; base < n32; base += 32) {
+        stage(base, 32);
+        __syncthreads();
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const float* qa = sa[ta];
+            const float* qb = sb[tb + 16 * p];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int L = 0; L < 8; ++L) {
+                    const int e = 8 * j + L;
+                    if (kIP) {
+                        acc[p][j][L] = __fmaf_rn(qa[e], qb[e], acc[p][j][L]);
+                    } else {
+                        const float df = __fsub_rn(qa[e], qb[e]);
+                        acc[p][j][L] = __fmaf_rn(df, df, acc[p][j][L]);
+                    }
+                }
+        }
+        __syncthreads();
+    }
+    const int rem = d - n32;
+    if (rem > 0) {
+        stage(n32, rem);
+        __syncthreads();
+    }
+    const int rem8 = rem & ~7;
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+        const float* qa = sa[ta];
+        const float* qb = sb[tb + 16 * p];
+        for (int u = 0; u < rem8; u += 8)
+#pragma unroll
+            for (int L = 0; L < 8; ++L) {
+                if (kIP) {
+                    acc[p][0][L] = __fmaf_rn(qa[u + L], qb[u + L], acc[p][0][L]);
+                } else {
+                    const float df = __fsub_rn(qa[u + L], qb[u + L]);
+                    acc[p][0][L] = __fmaf_rn(df, df, acc[p][0][L]);
+                }
+            }
+        float s[8];
+#pragma unroll
+        for (int L = 0; L < 8; ++L)
+            s[L] = __fadd_rn(__fadd_rn(acc[p][0][L], acc[p][1][L]), __fadd_rn(acc[p][2][L], acc[p][3][L]));
+        float r = __fadd_rn(__fadd_rn(__fadd_rn(s[0], s[4]), __fadd_rn(s[1], s[5])),
+                            __fadd_rn(__fadd_rn(s[2], s[6]), __fadd_rn(s[3], s[7])));
+        r = exact_tail<!kIP>(qa, qb, rem8, rem, r);   // the n % 8 tail as the reference build computes it
+        const int gi = a0 + ta, gj = b0 + tb + 16 * p;
+        if (gi < na && gj < nb) out[static_cast<size_t>(gi) * ld_out + gj] = kIP ? -r : r;
+    }
+}
+
+void pair_scores(const float* A, int na, const float* B, int nb, int d, bool ip, float* out, size_t ld_out,
+                 cudaStream_t st) {
+    if (na == 0 || nb == 0) return;
+    dim3 grid(static_cast<unsigned>(ceil_div(nb, kTB)), static_cast<unsigned>(ceil_div(na, kTA)));
+    if (ip) k_pair_scores<true><<<grid, 256, 0, st>>>(A, na, B, nb, d, out, ld_out);
+    else k_pair_scores<false><<<grid, 256, 0, st>>>(A, na, B, nb, d, out, ld_out);
+    QG_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// The P smallest of each row by (key(score), column), sorted. One block per
+// row: a 4-pass radix select finds the P-th key T, an ordered compaction takes
+// every key < T and the first ties at T in column order, then a bitonic sort.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool col_allowed(const uint64_t* allow, const uint64_t* deny, size_t c) {
+    return (!allow || ((allow[c >> 6] >> (c & 63)) & 1ull)) && (!deny || !((deny[c >> 6] >> (c & 63)) & 1ull));
+}
+
+// Columns refused by allow / deny (bitmaps over col_base + column, either may
+// be null) rank last and come out as column 0xFFFFFFFF with score +inf.
+__global__ void __launch_bounds__(256) k_select_rows(const float* __restrict__ scores, size_t ld, int ncols, int P,
+                                                     const uint64_t* __restrict__ allow, const uint64_t* __restrict__ deny,
+                                                     size_t col_base, bool eq0, uint32_t* __restrict__ out_col,
+                                                     float* __restrict__ out_score) {
+    extern __shared__ uint8_t sm_raw[];
+    const int Pp = next_pow2(P);
+    uint64_t* skey = reinterpret_cast<uint64_t*>(sm_raw);
+    int64_t* sval = reinterpret_cast<int64_t*>(skey + Pp);
+    __shared__ uint32_t hist[256];
+    __shared__ uint32_t s_prefix, s_mask, s_remaining;
+    __shared__ uint32_t warp_cnt[2][8];
+    __shared__ uint32_t s_lt, s_eq;
+    const float* row = scores + static_cast<size_t>(blockIdx.x) * ld;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_prefix = 0;
+        s_mask = 0;
+        s_remaining = static_cast<uint32_t>(P);
+    }
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int b = tid; b < 256; b += blockDim.x) hist[b] = 0;
+        __syncthreads();
+        const uint32_t prefix = s_prefix, mask = s_mask;
+        for (int c = tid; c < ncols; c += blockDim.x) {
+            const uint32_t k = col_allowed(allow, deny, col_base + c) ? (eq0 ? float_key_eq0(row[c]) : float_key(row[c]))
+                                                                       : 0xFFFFFFFFu;
+            if ((k & mask) == prefix) atomicAdd(&hist[(k >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t rem = s_remaining, b = 0;
+            for (; b < 256; ++b) {
+                if (hist[b] >= rem) break;
+                rem -= hist[b];
+            }
+            s_remaining = rem;
+            s_prefix = prefix | (b << shift);
+            s_mask = mask | (255u << shift);
+        }
+        __syncthreads();
+    }
+    const uint32_t T = s_prefix;
+    const uint32_t need_eq = s_remaining;   // ties at T to take, in column order
+    if (tid == 0) {
+        s_lt = 0;
+        s_eq = 0;
+    }
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int base = 0; base < ncols; base += blockDim.x) {
+        const int c = base + tid;
+        const uint32_t k = c < ncols && col_allowed(allow, deny, col_base + c)
+                               ? (eq0 ? float_key_eq0(row[c]) : float_key(row[c]))
+                               : 0xFFFFFFFFu;
+        const bool lt = c < ncols && k < T;
+        const bool eq = c < ncols && k == T;
+        const uint32_t blt = __ballot_sync(0xffffffffu, lt), beq = __ballot_sync(0xffffffffu, eq);
+        if (lane == 0) {
+            warp_cnt[0][warp] = __popc(blt);
+            warp_cnt[1][warp] = __popc(beq);
+        }
+        __syncthreads();
+        uint32_t off_lt = s_lt, off_eq = s_eq;
+        for (int w = 0; w < warp; ++w) {
+            off_lt += warp_cnt[0][w];
+            off_eq += warp_cnt[1][w];
+        }
+        const uint32_t below = (1u << lane) - 1u;
+        if (lt) {
+            const uint32_t pos = off_lt + __popc(blt & below);
+            skey[pos] = static_cast<uint64_t>(k);
+            sval[pos] = c;
+        }
+        if (eq) {
+            const uint32_t r = off_eq + __popc(beq & below);
+            if (r < need_eq) {
+                const uint32_t pos = (static_cast<uint32_t>(P) - need_eq) + r;
+                skey[pos] = static_cast<uint64_t>(k);
+                sval[pos] = c;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t tl = 0, te = 0;
+            for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+                tl += warp_cnt[0][w];
+                te += warp_cnt[1][w];
+            }
+            s_lt += tl;
+            s_eq += te;
+        }
+        __syncthreads();
+    }
+    for (int i = P + tid; i < Pp; i += blockDim.x) {
+        skey[i] = ~0ull;
+        sval[i] = INT64_MAX;
+    }
+    bitonic_sort(skey, sval, Pp);
+    for (int i = tid; i < P; i += blockDim.x) {
+        const uint32_t col = static_cast<uint32_t>(sval[i]);
+        const bool ok = col_allowed(allow, deny, col_base + col);
+        out_col[static_cast<size_t>(blockIdx.x) * P + i] = ok ? col : 0xFFFFFFFFu;
+        out_score[static_cast<size_t>(blockIdx.x) * P + i] =
+            ok ? row[col] : __int_as_float(0x7f800000);
+    }
+}
+
+void select_rows(const float* scores, size_t ld, int nrows, int ncols, int P, uint32_t* out_col, float* out_score,
+                 cudaStream_t st, const uint64_t* allow, const uint64_t* deny, size_t col_base, bool eq0) {
+    if (nrows == 0) return;
+    const size_t smem = static_cast<size_t>(next_pow2(P)) * 16;
+    if (smem > 48 * 1024)
+        QG_CUDA(cudaFuncSetAttribute(k_select_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    k_select_rows<<<nrows, 256, smem, st>>>(scores, ld, ncols, P, allow, deny, col_base, eq0, out_col, out_score);
+    QG_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Per-probe distance terms.
+//   mode L2 / L2-ADC : A (the probe's exact coarse distance, or the exact
+//                      distance to the list's residual center when the index has them)
+//   mode IP          : offset term = A = -(q . c)
+//   mode cosine-IP   : base = (A + 1) - |e|^2 (reference src/ivf_index.cpp:577-579)
+// ---------------------------------------------------------------------------
+__global__ void k_probe_terms(IvfView v, const float* __restrict__ q, int nq, int P, const uint32_t* __restrict__ probe,
+                              const float* __restrict__ pdist, float* __restrict__ term) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= static_cast<size_t>(nq) * P) return;
+    const int qi = static_cast<int>(i / P);
+    const uint32_t list = probe[i];
+    float A = pdist[i];
+    if (v.has_resid) A = exact_avx2<true>(q + static_cast<size_t>(qi) * v.dim, v.resid + static_cast<size_t>(list) * v.dim, v.dim);
+    if (v.mode == kModeCosIP) A = __fsub_rn(__fadd_rn(A, 1.0f), v.sqnorm[list]);
+    term[i] = A;
+}
+
+// ---------------------------------------------------------------------------
+// Per-query tables: C (mode L2, reference src/pq.cpp:186-204), or the inner
+// table rounded to the query's uint8 LUT (modes IP / cosine-IP; IP halves the
+// table first, reference src/ivf_index.cpp:448-456). One block per query.
+// ---------------------------------------------------------------------------
+__global__ void k_query_tables(IvfView v, const float* __restrict__ q, float* __restrict__ qC, uint4* __restrict__ qlut,
+                               float* __restrict__ qscale, float* __restrict__ qoffset) {
+    extern __shared__ float tab[];   // m * 16 floats, then m floats of row minimums
+    const int qi = blockIdx.x;
+    const float* qv = q + static_cast<size_t>(qi) * v.dim;
+    const int T = v.m * 16;
+    for (int t = threadIdx.x; t < T; t += blockDim.x) {
+        float c = inner_term(qv, v.pq_t, t >> 4, v.sd, 16, t & 15);
+        if (v.mode == kModeIP) c = __fmul_rn(c, 0.5f);
+        tab[t] = c;
+        if (v.mode == kModeL2) qC[static_cast<size_t>(qi) * T + t] = c;
+    }
+    if (v.mode == kModeL2 || v.mode == kModeL2Adc) return;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        float s, o;
+        warp_quantize_lut(
+            [&](int r, float* out) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) out[j] = tab[r * 16 + j];
+            },
+            v.m, v.m_pad, tab + T, qlut + static_cast<size_t>(qi) * v.m_pad, s, o);
+        if (threadIdx.x == 0) {
+            qscale[qi] = s;
+            qoffset[qi] = o;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The code scan with fused top-k'.
+//
+// A block handles one query and a chunk of its probes, in probe order. Per
+// probe it builds the list's uint8 LUT in shared memory (mode L2: B + C + A
+// rounded, as build_quantize_lut; mode L2-ADC: the residual's ADC table
+// rounded; modes IP / cosine-IP: the query's one LUT). Octets of 8 threads
+// then take superblocks (64 vectors) of the chunk's lists in turn.
+//
+// Selection keeps the k' smallest candidates by key64 = key(dist) << 32 |
+// push index, the push index being the vector's position in the query's
+// sequence of probed lists: exactly the set the reference's TopK keeps
+// (distance first, first pushed among ties; reference src/topk.hpp:20-25,
+// :94-131). Candidates go to a shared buffer when key64 beats the current
+// k'-th key; the buffer is sorted and cut back to k' when it fills, which
+// lowers the threshold. Deleted (or filtered-out) vectors are skipped before
+// they can enter, as the reference's push() does. The integer pre-test
+// sum <= S* is exact: S* is the largest sum whose distance is <= the
+// threshold distance (sum_limit).
+// ---------------------------------------------------------------------------
+struct ScanSmem {
+    int count;
+    int overflow;
+    uint64_t thr;
+};
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_scan(ScanArgs a) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    constexpr int NW = NT / 32, NOCT = NT / 8;
+    const IvfView& v = a.v;
+    const int qi = blockIdx.x / a.nchunks;
+    const int chunk = blockIdx.x - qi * a.nchunks;
+    const int p0 = chunk * a.pch;
+    const int np = min(a.P, p0 + a.pch) - p0;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
+    const int nlut = shared_lut ? 1 : a.pch;
+
+    // shared memory carve-up (see scan_smem_bytes)
+    uint64_t* ckey = reinterpret_cast<uint64_t*>(sm);
+    int64_t* cval = reinterpret_cast<int64_t*>(ckey + a.cap);
+    uint4* lut = reinterpret_cast<uint4*>(cval + a.cap);
+    float* scratch = reinterpret_cast<float*>(lut + static_cast<size_t>(nlut) * v.m_pad);   // per warp: row minimums
+    const int scr_per_warp = v.m_pad;
+    float* qtab = scratch + NW * scr_per_warp;     // mode L2: C (m*16 floats); mode L2-ADC: the query (dim)
+    const int qtab_len = v.mode == kModeL2 ? v.m * 16 : (v.mode == kModeL2Adc ? v.dim : 0);
+    float* p_scale = qtab + qtab_len;
+    float* p_offset = p_scale + a.pch;
+    int* p_smax = reinterpret_cast<int*>(p_offset + a.pch);
+    uint32_t* p_list = reinterpret_cast<uint32_t*>(p_smax + a.pch);
+    uint32_t* p_size = p_list + a.pch;
+    uint32_t* p_push = p_size + a.pch;
+    uint32_t* p_sbpre = p_push + a.pch;   // pch + 1
+    __shared__ ScanSmem st;
+    __shared__ uint32_t red[NW];
+
+    const size_t qp = static_cast<size_t>(qi) * a.P;
+    if (tid == 0) {
+        st.count = 0;
+        st.overflow = 0;
+        st.thr = ~0ull;
+    }
+    // vectors in probes before this chunk: the push index base
+    uint32_t before = 0;
+    for (int p = tid; p < p0; p += NT) before += v.list_size[a.probe[qp + p]];
+    for (int o = 16; o > 0; o >>= 1) before += __shfl_xor_sync(0xffffffffu, before, o);
+    if (lane == 0) red[warp] = before;
+    for (int p = tid; p < np; p += NT) {
+        const uint32_t l = a.probe[qp + p0 + p];
+        p_list[p] = l;
+        p_size[p] = v.list_size[l];
+    }
+    if (v.mode == kModeL2)
+        for (int t = tid; t < v.m * 16; t += NT) qtab[t] = a.qC[static_cast<size_t>(qi) * v.m * 16 + t];
+    if (v.mode == kModeL2Adc)
+        for (int t = tid; t < v.dim; t += NT) qtab[t] = a.q[static_cast<size_t>(qi) * v.dim + t];
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t base = 0;
+        for (int w = 0; w < NW; ++w) base += red[w];
+        uint32_t sb = 0;
+        for (int p = 0; p < np; ++p) {
+            p_push[p] = base;
+            base += p_size[p];
+            p_sbpre[p] = sb;
+            sb += (p_size[p] + kSuperBlock - 1) / kSuperBlock;
+        }
+        p_sbpre[np] = sb;
+    }
+
+    // ---- LUTs, scales and offsets -------------------------------------------
+    if (shared_lut) {
+        for (int r = tid; r < v.m_pad; r += NT) lut[r] = a.qlut[static_cast<size_t>(qi) * v.m_pad + r];
+        for (int p = tid; p < np; p += NT) {
+            p_scale[p] = a.qscale[qi];
+            p_offset[p] = __fadd_rn(a.qoffset[qi], a.pterm[qp + p0 + p]);
+        }
+    } else {
+        float* rmin = scratch + warp * scr_per_warp;
+        for (int p = warp; p < np; p += NW) {
+            const uint32_t l = a.probe[qp + p0 + p];
+            float s, o;
+            if (v.mode == kModeL2) {
+                const float A = a.pterm[qp + p0 + p];
+                const float* B = v.B + static_cast<size_t>(l) * v.m * 16;
+                warp_quantize_lut(
+                    [&](int r, float* out) {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            float t = __fadd_rn(B[r * 16 + j], qtab[r * 16 + j]);
+                            if (r == 0) t = __fadd_rn(t, A);
+                            out[j] = t;
+                        }
+                    },
+                    v.m, v.m_pad, rmin, lut + static_cast<size_t>(p) * v.m_pad, s, o);
+            } else {
+                // the residual (q - center) is formed per element inside the table
+                // loop, as compute_adc_table reads it (reference src/ivf_index.cpp:594-610)
+                const float* ctr = v.resid + static_cast<size_t>(l) * v.dim;
+                warp_quantize_lut(
+                    [&](int r, float* out) {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            float acc = 0.0f;
+                            for (int u = 0; u < v.sd; ++u) {
+                                const int e = r * v.sd + u;
+                                const float diff = __fsub_rn(__fsub_rn(qtab[e], ctr[e]), v.pq_t[e * 16 + j]);
+                                acc = __fmaf_rn(diff, diff, acc);
+                            }
+                            out[j] = acc;
+                        }
+                    },
+                    v.m, v.m_pad, rmin, lut + static_cast<size_t>(p) * v.m_pad, s, o);
+            }
+            if (lane == 0) {
+                p_scale[p] = s;
+                p_offset[p] = o;
+            }
+        }
+    }
+    __syncthreads();
+    for (int p = tid; p < np; p += NT) p_smax[p] = 65535;
+    __syncthreads();
+
+    // ---- rounds over superblocks --------------------------------------------
+    const int total = static_cast<int>(p_sbpre[np]);
+    const int oct = tid >> 3, r = tid & 7;
+    for (int base = 0; base < total; base += NOCT) {
+        const int item = base + oct;
+        if (item < total) {
+            int pl = 0;
+            while (pl + 1 < np && static_cast<int>(p_sbpre[pl + 1]) <= item) ++pl;
+            const int sbl = item - static_cast<int>(p_sbpre[pl]);
+            const uint32_t l = p_list[pl];
+            const size_t sbg = static_cast<size_t>(v.sb_off[l]) + sbl;
+            const uint4* sbp = v.codes + sbg * static_cast<size_t>(2 * v.m_pad);
+            const uint4* L = lut + static_cast<size_t>(shared_lut ? 0 : pl) * v.m_pad;
+            uint32_t sums[8];
+            octet_sums(sbp, L, v.m_pad, r, sums);
+            const int smax = p_smax[pl];
+            const uint32_t size = p_size[pl];
+            const float scale = p_scale[pl], offset = p_offset[pl];
+            const uint64_t thr = st.thr;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const uint32_t pos = static_cast<uint32_t>(sbl) * kSuperBlock + 8 * r + i;
+                if (pos < size && static_cast<int>(sums[i]) <= smax) {
+                    const float dist = fs_dist(sums[i], scale, offset);
+                    const uint64_t key = (static_cast<uint64_t>(float_key(dist)) << 32) | (p_push[pl] + pos);
+                    if (key < thr) {
+                        const uint32_t slot = v.ids[sbg * kSuperBlock + 8 * r + i];
+                        const bool ok = a.filter ? ((a.filter[slot >> 6] >> (slot & 63)) & 1ull)
+                                                 : !(v.deleted && ((v.deleted[slot >> 6] >> (slot & 63)) & 1ull));
+                        if (ok) {
+                            const int idx = atomicAdd(&st.count, 1);
+                            if (idx < a.cap) {
+                                ckey[idx] = key;
+                                cval[idx] = slot;
+                            } else {
+                                st.overflow = 1;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        const bool last = base + NOCT >= total;
+        if (st.count > a.cap - NOCT * kSuperBlock || (last && st.count > 0)) {
+            const int n = min(st.count, a.cap);
+            const int npow = max(2, next_pow2(n));
+            for (int i = n + tid; i < npow; i += NT) {
+                ckey[i] = ~0ull;
+                cval[i] = INT64_MAX;
+            }
+            bitonic_sort(ckey, cval, npow);
+            if (tid == 0) {
+                if (n >= a.kp) st.thr = ckey[a.kp - 1];
+                st.count = min(n, a.kp);
+            }
+            __syncthreads();
+            const uint32_t tk = static_cast<uint32_t>(st.thr >> 32);
+            for (int p = tid; p < np; p += NT) p_smax[p] = sum_limit(st.thr == ~0ull ? 0xFFFFFFFFu : tk, p_scale[p], p_offset[p]);
+            __syncthreads();
+        }
+    }
+    // ---- output: this chunk's k' best, sorted by key64 ----------------------------
+    const int n = st.count;
+    const size_t ob = static_cast<size_t>(blockIdx.x) * a.kp;
+    for (int i = tid; i < a.kp; i += NT) {
+        a.out_key[ob + i] = i < n ? ckey[i] : ~0ull;
+        a.out_slot[ob + i] = i < n ? static_cast<uint32_t>(cval[i]) : 0xFFFFFFFFu;
+    }
+    if (tid == 0 && st.overflow) atomicExch(a.err, 1);
+}
+
+size_t scan_smem_bytes(const IvfView& v, int pch, int cap, int nt) {
+    const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
+    const int nlut = shared_lut ? 1 : pch;
+    const int nw = nt / 32;
+    const int scr = v.m_pad;
+    const int qtab = v.mode == kModeL2 ? v.m * 16 : (v.mode == kModeL2Adc ? v.dim : 0);
+    size_t b = static_cast<size_t>(cap) * 16;
+    b += static_cast<size_t>(nlut) * v.m_pad * 16;
+    b += static_cast<size_t>(nw) * scr * 4;
+    b += static_cast<size_t>(qtab) * 4;
+    b += static_cast<size_t>(pch) * 4 * 7 + 4 + 16;   // per-probe arrays: 7 of pch words, plus p_sbpre's last
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// Merge: the k' smallest key64 of a query's chunk outputs, sorted. The buffer
+// holds the current best k' and the next batch of entries.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_merge(const uint64_t* __restrict__ in_key, const uint32_t* __restrict__ in_slot,
+                                               int nchunks, int kp, int capm, uint64_t* __restrict__ out_key,
+                                               uint32_t* __restrict__ out_slot) {
+    extern __shared__ uint8_t sm_raw[];
+    uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);
+    int64_t* val = reinterpret_cast<int64_t*>(key + capm);
+    const int qi = blockIdx.x;
+    const size_t total = static_cast<size_t>(nchunks) * kp;
+    const uint64_t* ik = in_key + static_cast<size_t>(qi) * total;
+    const uint32_t* is = in_slot + static_cast<size_t>(qi) * total;
+    for (int i = threadIdx.x; i < kp; i += blockDim.x) {
+        key[i] = ~0ull;
+        val[i] = INT64_MAX;
+    }
+    const int batch = capm - kp;
+    for (size_t b0 = 0; b0 < total; b0 += batch) {
+        for (int i = threadIdx.x; i < batch; i += blockDim.x) {
+            const size_t e = b0 + i;
+            const bool ok = e < total && ik[e] != ~0ull;
+            key[kp + i] = ok ? ik[e] : ~0ull;
+            val[kp + i] = ok ? static_cast<int64_t>(is[e]) : INT64_MAX;
+        }
+        bitonic_sort(key, val, capm);
+    }
+    for (int i = threadIdx.x; i < kp; i += blockDim.x) {
+        out_key[static_cast<size_t>(qi) * kp + i] = key[i];
+        out_slot[static_cast<size_t>(qi) * kp + i] = key[i] == ~0ull ? 0xFFFFFFFFu : static_cast<uint32_t>(val[i]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// IVF results: the first k of the k' list, sorted by (distance key, id) as
+// take_sorted does (reference src/topk.hpp:53-77), ids mapped through labels.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_finalize_ivf(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ slot_in,
+                                                      int kp, int k, const int64_t* __restrict__ labels, bool cosine,
+                                                      int64_t* __restrict__ out_ids, float* __restrict__ out_d) {
+    extern __shared__ uint8_t sm_raw[];
+    const int kpow = max(2, next_pow2(k));
+    uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);
+    int64_t* val = reinterpret_cast<int64_t*>(key + kpow);
+    const int qi = blockIdx.x;
+    for (int i = threadIdx.x; i < kpow; i += blockDim.x) {
+        const uint64_t k64 = i < k && i < kp ? key_in[static_cast<size_t>(qi) * kp + i] : ~0ull;
+        if (k64 == ~0ull) {
+            key[i] = ~0ull;
+            val[i] = INT64_MAX;
+        } else {
+            const uint32_t slot = slot_in[static_cast<size_t>(qi) * kp + i];
+            key[i] = k64 >> 32;
+            val[i] = labels ? labels[slot] : static_cast<int64_t>(slot);
+        }
+    }
+    bitonic_sort(key, val, kpow);
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const size_t o = static_cast<size_t>(qi) * k + i;
+        if (key[i] == ~0ull) {
+            out_ids[o] = -1;
+            out_d[o] = __int_as_float(0x7f800000);
+        } else {
+            const float d = key_float(static_cast<uint32_t>(key[i]));
+            out_ids[o] = val[i];
+            out_d[o] = cosine ? __fmul_rn(d, 0.5f) : d;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Re-rank (reference src/refine_index.cpp:112-140): the exact score of every
+// candidate from the raw rows, then the k smallest by (score, slot), compared
+// as floats (so -0 == +0), ids mapped through the refine index's labels.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_refine(const float* __restrict__ q, int dim, const float* __restrict__ rows,
+                                                const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ slot_in,
+                                                int kp, int k, bool ip, const int64_t* __restrict__ labels, bool cosine,
+                                                int64_t* __restrict__ out_ids, float* __restrict__ out_d) {
+    extern __shared__ uint8_t sm_raw[];
+    const int kpow = max(2, next_pow2(kp));
+    uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);
+    int64_t* val = reinterpret_cast<int64_t*>(key + kpow);
+    float* qv = reinterpret_cast<float*>(val + kpow);
+    const int qi = blockIdx.x;
+    for (int t = threadIdx.x; t < dim; t += blockDim.x) qv[t] = q[static_cast<size_t>(qi) * dim + t];
+    __syncthreads();
+    for (int i = threadIdx.x; i < kpow; i += blockDim.x) {
+        const bool ok = i < kp && key_in[static_cast<size_t>(qi) * kp + i] != ~0ull;
+        if (!ok) {
+            key[i] = ~0ull;
+            val[i] = INT64_MAX;
+            continue;
+        }
+        const uint32_t slot = slot_in[static_cast<size_t>(qi) * kp + i];
+        const float d = exact_score(qv, rows + static_cast<size_t>(slot) * dim, dim, ip);
+        key[i] = float_key_eq0(d);
+        val[i] = slot;
+    }
+    bitonic_sort(key, val, kpow);
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const size_t o = static_cast<size_t>(qi) * k + i;
+        if (key[i] == ~0ull) {
+            out_ids[o] = -1;
+            out_d[o] = __int_as_float(0x7f800000);
+        } else {
+            const uint32_t slot = static_cast<uint32_t>(val[i]);
+            // recompute: float_key_eq0 folded -0 into +0, and the reference returns the value itself
+            const float d = exact_score(qv, rows + static_cast<size_t>(slot) * dim, dim, ip);
+            out_ids[o] = labels ? labels[slot] : static_cast<int64_t>(slot);
+            out_d[o] = cosine ? __fmul_rn(d, 0.5f) : d;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host orchestration
+// ---------------------------------------------------------------------------
+void normalize_rows(const float* x, float* y, int n, int d, int* d_zero, cudaStream_t st) {
+    if (n == 0) return;
+    k_normalize<<<static_cast<unsigned>(ceil_div(n, 128)), 128, 0, st>>>(x, y, n, d, d_zero);
+    QG_LAUNCH_CHECK();
+}
+
+int scan_cap(int kp) {
+    // room for k' kept entries plus one full round of candidates (16 octets of a
+    // 128-thread block, 64 vectors each)
+    return next_pow2(kp + 16 * kSuperBlock);
+}
+
+void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st) {
+    const int nq = s.nq, P = s.nprobe, kp = s.kp;
+    if (nq == 0) return;
+    constexpr int NT = 128;
+    // coarse: all pair scores, then the P nearest lists per query
+    DevBuf<float> scores(static_cast<size_t>(nq) * v.nlist, st);
+    pair_scores(s.q, nq, v.centroids, v.nlist, v.dim, v.ip_metric, scores.get(), v.nlist, st);
+    DevBuf<uint32_t> probe(static_cast<size_t>(nq) * P, st);
+    DevBuf<float> pdist(static_cast<size_t>(nq) * P, st);
+    // (score, list) compared as the reference's heap of (float, uint16_t) pairs does: -0 == +0
+    select_rows(scores.get(), v.nlist, nq, v.nlist, P, probe.get(), pdist.get(), st, nullptr, nullptr, 0, true);
+    scores.release();
+
+    DevBuf<float> pterm(static_cast<size_t>(nq) * P, st);
+    {
+        const size_t n = static_cast<size_t>(nq) * P;
+        k_probe_terms<<<static_cast<unsigned>(ceil_div(n, 256)), 256, 0, st>>>(v, s.q, nq, P, probe.get(), pdist.get(),
+                                                                                pterm.get());
+        QG_LAUNCH_CHECK();
+    }
+    DevBuf<float> qC, qscale, qoffset;
+    DevBuf<uint4> qlut;
+    if (v.mode == kModeL2) qC.alloc(static_cast<size_t>(nq) * v.m * 16, st);
+    if (v.mode == kModeIP || v.mode == kModeCosIP) {
+        qlut.alloc(static_cast<size_t>(nq) * v.m_pad, st);
+        qscale.alloc(nq, st);
+        qoffset.alloc(nq, st);
+    }
+    if (v.mode != kModeL2Adc) {
+        const size_t smem = static_cast<size_t>(v.m) * 17 * 4;
+        if (smem > 48 * 1024)
+            QG_CUDA(cudaFuncSetAttribute(k_query_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        k_query_tables<<<nq, 128, smem, st>>>(v, s.q, qC.get(), qlut.get(), qscale.get(), qoffset.get());
+        QG_LAUNCH_CHECK();
+    }
+
+    // chunking: enough blocks to fill the GPU several times over
+    const int sms = s.sm_count > 0 ? s.sm_count : 148;
+    int nchunks = std::clamp(static_cast<int>(ceil_div(static_cast<size_t>(4 * sms), nq)), 1, P);
+    int pch = static_cast<int>(ceil_div(P, nchunks));
+    const int cap = scan_cap(kp);
+    // the per-probe LUTs of a chunk must fit in shared memory
+    while (pch > 1 && scan_smem_bytes(v, pch, cap, NT) > 200 * 1024) pch = (pch + 1) / 2;
+    nchunks = static_cast<int>(ceil_div(P, pch));
+    const size_t smem = scan_smem_bytes(v, pch, cap, NT);
+    require(smem <= 227 * 1024, "fast-scan shared memory exceeds the B200 limit for this m / k * k_factor",
+            kUnsupported);
+
+    const bool direct = nchunks == 1;
+    const size_t nout = static_cast<size_t>(nq) * nchunks * kp;
+    DevBuf<uint64_t> ckey;
+    DevBuf<uint32_t> cslot;
+    if (!direct) {
+        ckey.alloc(nout, st);
+        cslot.alloc(nout, st);
+    }
+    ScanArgs a{};
+    a.v = v;
+    a.q = s.q;
+    a.probe = probe.get();
+    a.pterm = pterm.get();
+    a.qC = qC.get();
+    a.qlut = qlut.get();
+    a.qscale = qscale.get();
+    a.qoffset = qoffset.get();
+    a.filter = s.filter;
+    a.P = P;
+    a.pch = pch;
+    a.nchunks = nchunks;
+    a.kp = kp;
+    a.cap = cap;
+    a.out_key = direct ? out_key : ckey.get();
+    a.out_slot = direct ? out_slot : cslot.get();
+    a.err = s.d_err;
+    QG_CUDA(cudaFuncSetAttribute(k_scan<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    k_scan<NT><<<static_cast<unsigned>(nq * nchunks), NT, smem, st>>>(a);
+    QG_LAUNCH_CHECK();
+    if (!direct) merge_candidates(ckey.get(), cslot.get(), nq, nchunks, kp, out_key, out_slot, st);
+}
+
+void merge_candidates(const uint64_t* in_key, const uint32_t* in_slot, int nq, int nchunks, int kp, uint64_t* out_key,
+                      uint32_t* out_slot, cudaStream_t st) {
+    if (nq == 0) return;
+    const int capm = next_pow2(2 * kp);
+    const size_t msm = static_cast<size_t>(capm) * 16;
+    if (msm > 48 * 1024)
+        QG_CUDA(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm)));
+    k_merge<<<nq, 256, msm, st>>>(in_key, in_slot, nchunks, kp, capm, out_key, out_slot);
+    QG_LAUNCH_CHECK();
+}
+
+void finalize_ivf(const uint64_t* key, const uint32_t* slot, int nq, int kp, int k, const int64_t* labels, bool cosine,
+                  int64_t* out_ids, float* out_d, cudaStream_t st) {
+    if (nq == 0 || k == 0) return;
+    const int kpow = std::max(2, next_pow2(k));
+    k_finalize_ivf<<<nq, 128, static_cast<size_t>(kpow) * 16, st>>>(key, slot, kp, k, labels, cosine, out_ids, out_d);
+    QG_LAUNCH_CHECK();
+}
+
+void refine_candidates(const float* q, int nq, int dim, const float* rows, const uint64_t* key, const uint32_t* slot,
+                       int kp, int k, bool ip, const int64_t* labels, bool cosine, int64_t* out_ids, float* out_d,
+                       cudaStream_t st) {
+    if (nq == 0 || k == 0) return;
+    const int kpow = std::max(2, next_pow2(kp));
+    const size_t rsm = static_cast<size_t>(kpow) * 16 + static_cast<size_t>(dim) * 4;
+    if (rsm > 48 * 1024)
+        QG_CUDA(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(rsm)));
+    k_refine<<<nq, 128, rsm, st>>>(q, dim, rows, key, slot, kp, k, ip, labels, cosine, out_ids, out_d);
+    QG_LAUNCH_CHECK();
+}
+
+} // namespace qg

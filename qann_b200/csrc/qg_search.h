@@ -1,0 +1,85 @@
+// Device views of an index and the launchers of the search kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace qg {
+
+// How an IVF fast-scan index scores codes (reference src/ivf_index.cpp:436-456):
+enum ScanMode : int {
+    kModeL2 = 0,      // per-list LUT from the precomputed tables: B[list] + C[query] + A on row 0
+    kModeL2Adc = 1,   // per-list LUT from the ADC table of (query - list center), no precomputed tables
+    kModeIP = 2,      // one LUT per query from half the inner table; the list adds -(q . c)
+    kModeCosIP = 3,   // cosine scored by inner product: one LUT per query; the list adds (A + 1) - |e|^2
+};
+
+// Device arrays of an IVF fast-scan index (all owned by the index object).
+struct IvfView {
+    int dim = 0, nlist = 0, m = 0, m_pad = 0, sd = 0;
+    int mode = kModeL2;
+    bool ip_metric = false;   // coarse ranks by -(q . c)
+    bool has_resid = false;   // cosine: A is measured against each list's residual center
+    const float* centroids = nullptr;   // nlist * dim
+    const float* resid = nullptr;       // nlist * dim: residual centers, or the centroids
+    const float* sqnorm = nullptr;      // nlist: |resid center|^2 (cosine-IP base)
+    const float* pq_t = nullptr;        // m * sd * 16, transposed codebook
+    const float* B = nullptr;           // nlist * m * 16 precomputed list terms (mode L2)
+    const uint32_t* sb_off = nullptr;   // nlist + 1 superblock offsets
+    const uint32_t* list_size = nullptr;
+    const uint4* codes = nullptr;       // superblocks, 2 * m_pad uint4 each
+    const uint32_t* ids = nullptr;      // 64 slots per superblock, kRemoved for padding
+    const uint64_t* deleted = nullptr;  // slot bitmap of deleted vectors, or null
+};
+
+struct ScanArgs {
+    IvfView v;
+    const float* q;          // nq * dim prepared queries
+    const uint32_t* probe;   // nq * P lists, nearest first
+    const float* pterm;      // nq * P per-probe terms
+    const float* qC;         // mode L2: nq * m * 16
+    const uint4* qlut;       // modes IP / cosine-IP: nq * m_pad rows
+    const float* qscale;
+    const float* qoffset;
+    const uint64_t* filter;  // allowed-slot bitmap, or null
+    int P, pch, nchunks, kp, cap;
+    uint64_t* out_key;       // (nq * nchunks) * kp
+    uint32_t* out_slot;
+    int* err;
+};
+
+struct IvfSearchArgs {
+    const float* q = nullptr;   // nq * dim, prepared (normalised for cosine)
+    int nq = 0, k = 0, kp = 0, nprobe = 0;
+    const uint64_t* filter = nullptr;
+    int sm_count = 0;
+    int* d_err = nullptr;
+};
+
+void normalize_rows(const float* x, float* y, int n, int d, int* d_zero, cudaStream_t st);
+void pair_scores(const float* A, int na, const float* B, int nb, int d, bool ip, float* out, size_t ld_out,
+                 cudaStream_t st);
+// The P smallest scores of each row by (key, column), sorted; refused columns
+// (allow / deny bitmaps over col_base + column) come out as 0xFFFFFFFF / +inf.
+// eq0 compares -0 and +0 as equal (float operator< semantics).
+void select_rows(const float* scores, size_t ld, int nrows, int ncols, int P, uint32_t* out_col, float* out_score,
+                 cudaStream_t st, const uint64_t* allow = nullptr, const uint64_t* deny = nullptr, size_t col_base = 0,
+                 bool eq0 = false);
+// The k' = s.kp best candidates of each query, as sorted (key64, slot) lists
+// (key64 = key(dist) << 32 | push index; 0xFFFF... marks an empty entry).
+void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st);
+// The kp smallest key64 over nchunks sorted lists per query.
+void merge_candidates(const uint64_t* in_key, const uint32_t* in_slot, int nq, int nchunks, int kp, uint64_t* out_key,
+                      uint32_t* out_slot, cudaStream_t st);
+// IVF results from candidates: the first k, sorted by (distance, id).
+void finalize_ivf(const uint64_t* key, const uint32_t* slot, int nq, int kp, int k, const int64_t* labels, bool cosine,
+                  int64_t* out_ids, float* out_d, cudaStream_t st);
+// Exact re-rank of candidates from raw rows: the k best by (score, slot).
+void refine_candidates(const float* q, int nq, int dim, const float* rows, const uint64_t* key, const uint32_t* slot,
+                       int kp, int k, bool ip, const int64_t* labels, bool cosine, int64_t* out_ids, float* out_d,
+                       cudaStream_t st);
+int scan_cap(int kp);
+
+} // namespace qg

@@ -1,0 +1,109 @@
+"""CPU checks of the boundary: the C-ABI library loads and exports every entry
+point include/qann_gpu.h declares, argument errors match the reference's
+exception classes, and `.qann` files round-trip byte for byte with qann."""
+import filecmp
+import pathlib
+import re
+
+import numpy as np
+import pytest
+
+import qann_b200 as qb
+from qann_b200 import _lib
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+
+
+def test_library_exports_every_declared_symbol():
+    header = (ROOT / "include" / "qann_gpu.h").read_text()
+    declared = set(re.findall(r"\b(qg_[a-z_0-9]+)\s*\(", header))
+    assert declared, "no declarations found"
+    for name in declared:
+        assert hasattr(_lib.lib, name), name
+    assert declared == set(_lib.EXPORTS)
+
+
+def test_version():
+    assert "sm_100a" in qb.version()
+
+
+def test_constructor_errors_match_reference():
+    with pytest.raises(ValueError, match="nlist"):
+        qb.IVFIndex(16, 50)
+    with pytest.raises(ValueError, match="nprobe"):
+        qb.IVFIndex(16, 100, 101)
+    with pytest.raises(ValueError, match="dim"):
+        qb.FlatIndex(0)
+    ivf = qb.IVFIndex(32, 100)
+    with pytest.raises(ValueError):
+        ivf.enable_pq(16, 256, fast_scan=True)
+    with pytest.raises(ValueError):
+        ivf.enable_pq(15, fast_scan=True)
+    ivf.enable_pq(16, fast_scan=True)
+    with pytest.raises(ValueError):
+        ivf.pq_distance = qb.PQDistance.SDC
+    with pytest.raises(RuntimeError, match="train"):
+        ivf.add(np.zeros((3, 32), np.float32))
+
+
+def test_refine_base_rules():
+    base = qb.IVFIndex(16, 100)
+    base.enable_pq(8, fast_scan=True)
+    with pytest.raises(ValueError, match="k_factor"):
+        qb.RefineIndex(base, 0)
+    r = qb.RefineIndex(base, 4)
+    with pytest.raises(ValueError, match="wrapped"):
+        qb.RefineIndex(base, 4)
+    with pytest.raises(ValueError, match="RefineIndex"):
+        qb.RefineIndex(r, 2)
+    custom = qb.FlatIndex(16, custom_ids=True)
+    with pytest.raises(ValueError, match="custom ids"):
+        qb.RefineIndex(custom)
+
+
+def test_setters_validate():
+    ivf = qb.IVFIndex(16, 100, 10)
+    ivf.nprobe = 100
+    assert ivf.nprobe == 100
+    with pytest.raises(ValueError):
+        ivf.nprobe = 0
+
+
+@pytest.mark.parametrize("name", ["gen/refine_l2.qann", "gen/ivf_cos_ip.qann", "gen/ivf_l2_custom_del.qann",
+                                  "gen/refine_l2_custom_del.qann", "gen/refine_cos_l2.qann"])
+def test_resave_is_byte_identical(golden, tmp_path, name):
+    src = golden / name
+    idx = qb.load(src)
+    out = tmp_path / "x.qann"
+    idx.save(out)
+    assert filecmp.cmp(src, out, shallow=False)
+
+
+@pytest.mark.parametrize("name", ["v4_ivf_fs", "v11_ivf_cos_fs", "v12_ivf_cos_l2", "v1_flat", "v2_refine"])
+def test_old_versions_load(golden, name):
+    idx = qb.load(golden / "ref" / f"{name}.qann")
+    assert idx.size() > 0
+
+
+def test_corrupt_files_raise(tmp_path, golden):
+    b = (golden / "gen" / "ivf_l2.qann").read_bytes()
+    p = tmp_path / "bad.qann"
+    p.write_bytes(b"XXXX" + b[4:])
+    with pytest.raises(RuntimeError, match="not a qann index file"):
+        qb.load(p)
+    p.write_bytes(b[: len(b) // 2])
+    with pytest.raises(RuntimeError, match="truncated|corrupt"):
+        qb.load(p)
+    p.write_bytes(b + b"\0")
+    with pytest.raises(RuntimeError, match="unexpected data"):
+        qb.load(p)
+
+
+def test_reference_reads_our_files(ref, golden, tmp_path):
+    idx = qb.load(golden / "gen" / "refine_cos_ip.qann")
+    out = tmp_path / "ours.qann"
+    idx.save(out)
+    r = ref.load(out)
+    q = np.load(golden / "gen" / "queries.npy")
+    ids, _ = r.batch_query(q, 10)
+    np.testing.assert_array_equal(ids, np.load(golden / "gen" / "refine_cos_ip_ids.npy"))

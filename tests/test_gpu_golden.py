@@ -1,0 +1,52 @@
+"""The CUDA path against the golden fixtures: the reference's own
+cross-version files (tests/golden/ref) and indexes the reference library
+built on seeded data with its query results (tests/golden/gen).
+
+Bar: ids identical; distances within rtol 1e-5 of the reference's (most are
+bit-identical; the saved results of older qann releases came from other CPUs).
+"""
+import numpy as np
+import pytest
+
+import qann_b200 as qb
+
+pytestmark = pytest.mark.gpu
+
+REF_FS = [
+    ("v4_ivf_fs", "v4_queries"),
+    ("v11_ivf_cos_fs", "v11_cos_queries"),
+    ("v12_ivf_cos_l2", "v12_cos_queries"),
+]
+REF_FLAT = [("v1_flat", "v1_queries"), ("v2_flat", "v2_queries"), ("v3_flat", "v3_queries"),
+            ("v4_flat", "v4_queries"), ("v5_flat", "v5_queries"), ("v9_ip_flat", "v9_ip_queries")]
+GEN = ["l2", "l2_adc", "ip", "cos_ip", "cos_l2", "l2_custom_del"]
+
+
+@pytest.mark.parametrize("name,qn", REF_FS)
+def test_reference_fast_scan_files(golden, name, qn):
+    idx = qb.load(golden / "ref" / f"{name}.qann")
+    q = np.load(golden / "ref" / f"{qn}.npy")
+    ids, d = idx.batch_query(q, 10)
+    np.testing.assert_array_equal(ids, np.load(golden / "ref" / f"{name}_ids.npy"))
+    np.testing.assert_allclose(d, np.load(golden / "ref" / f"{name}_dists.npy"), rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("name,qn", REF_FLAT)
+def test_reference_flat_files(golden, name, qn):
+    idx = qb.load(golden / "ref" / f"{name}.qann")
+    q = np.load(golden / "ref" / f"{qn}.npy")
+    ids, d = idx.batch_query(q, 10)
+    exp = np.load(golden / "ref" / f"{name}_ids.npy")
+    # the oldest files were saved by releases on other CPUs: near-ties may swap (reference tests: >= 0.99)
+    assert np.mean(ids == exp) >= 0.99
+    np.testing.assert_allclose(d, np.load(golden / "ref" / f"{name}_dists.npy"), rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.parametrize("kind", ["ivf", "refine"])
+@pytest.mark.parametrize("name", GEN)
+def test_generated_indexes(golden, kind, name):
+    idx = qb.load(golden / "gen" / f"{kind}_{name}.qann")
+    q = np.load(golden / "gen" / "queries.npy")
+    ids, d = idx.batch_query(q, 10)
+    np.testing.assert_array_equal(ids, np.load(golden / "gen" / f"{kind}_{name}_ids.npy"))
+    np.testing.assert_array_equal(d, np.load(golden / "gen" / f"{kind}_{name}_dists.npy"))

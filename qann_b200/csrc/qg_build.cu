@@ -6,6 +6,7 @@
 // src/pq.cpp:88-116).
 #include "qg_device.cuh"
 #include "qg_ops.h"
+#include "qg_train.h"
 
 #include <algorithm>
 #include <numeric>
@@ -83,6 +84,13 @@ __global__ void k_encode16(const float* __restrict__ x, size_t n, int dim, const
     for (int k = 15; k >= 0; --k)
         if (acc[k] == mn) best = k;
     codes[t] = static_cast<uint8_t>(best);
+}
+
+void encode16(const float* x, size_t n, int dim, const float* centers, const uint32_t* assign, const float* yt, int m,
+              int sd, uint8_t* codes, cudaStream_t st) {
+    if (n == 0) return;
+    k_encode16<<<static_cast<unsigned>(ceil_div(n * m, 256)), 256, 0, st>>>(x, n, dim, centers, assign, yt, m, sd, codes);
+    QG_LAUNCH_CHECK();
 }
 
 // Rows prepared for the metric: cosine rows scaled to unit length on the GPU

@@ -3,35 +3,18 @@
 // Numerics contract: every float operation whose result must match the
 // reference CPU build bit for bit is written with explicit round-to-nearest
 // intrinsics (__fadd_rn, __fmul_rn, __fdiv_rn, __fmaf_rn) and the library is
-// compiled with -fmad=false, so nvcc never fuses a multiply into an add that
-// the reference (built as ISO C++20, where GCC does not contract) rounds twice.
+// compiled with -fmad=false, so a multiply and an add are fused exactly where
+// the reference's release build (GCC, C++, -mavx2 -mfma, whose default
+// -ffp-contract=fast fuses `x += a * b`) fuses them, and nowhere else.
 #pragma once
 
-#include <cuda_runtime.h>
-
-#include "qg_error.h"
+#include "qg_cuda.h"
 
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
-#include <stdexcept>
-#include <string>
 
 namespace qg {
-
-[[noreturn]] inline void throw_cuda(cudaError_t e, const char* what, const char* file, int line) {
-    std::string msg = std::string("CUDA error in ") + what + " (" + file + ":" + std::to_string(line) +
-                      "): " + cudaGetErrorString(e);
-    throw Error(e == cudaErrorMemoryAllocation ? kOutOfMemory : kCudaError, msg);
-}
-
-#define QG_CUDA(call)                                                        \
-    do {                                                                     \
-        cudaError_t qg_e_ = (call);                                          \
-        if (qg_e_ != cudaSuccess) ::qg::throw_cuda(qg_e_, #call, __FILE__, __LINE__); \
-    } while (0)
-
-#define QG_LAUNCH_CHECK() QG_CUDA(cudaGetLastError())
 
 // ---------------------------------------------------------------------------
 // Ordered float keys (reference src/topk.hpp:82-91): a float maps to a uint32
@@ -158,55 +141,5 @@ __device__ __forceinline__ float exact_avx2(const float* __restrict__ a, const f
 __device__ __forceinline__ float exact_score(const float* a, const float* b, int n, bool ip) {
     return ip ? -exact_avx2<false>(a, b, n) : exact_avx2<true>(a, b, n);
 }
-
-// ---------------------------------------------------------------------------
-// Small host utilities
-// ---------------------------------------------------------------------------
-inline size_t ceil_div(size_t a, size_t b) { return (a + b - 1) / b; }
-
-// Number of SMs of the current device (cached per device by the caller).
-inline int sm_count() {
-    int dev = 0, n = 0;
-    QG_CUDA(cudaGetDevice(&dev));
-    QG_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
-    return n;
-}
-
-// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync on one stream).
-template <class T>
-struct DevBuf {
-    T* ptr = nullptr;
-    size_t count = 0;
-    cudaStream_t stream = nullptr;
-
-    DevBuf() = default;
-    DevBuf(size_t n, cudaStream_t s) { alloc(n, s); }
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), count(o.count), stream(o.stream) { o.ptr = nullptr; o.count = 0; }
-    DevBuf& operator=(DevBuf&& o) noexcept {
-        if (this != &o) {
-            release();
-            ptr = o.ptr; count = o.count; stream = o.stream;
-            o.ptr = nullptr; o.count = 0;
-        }
-        return *this;
-    }
-    ~DevBuf() { release(); }
-
-    void alloc(size_t n, cudaStream_t s) {
-        release();
-        stream = s;
-        count = n;
-        if (n) QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), s));
-    }
-    void release() noexcept {
-        if (ptr) cudaFreeAsync(ptr, stream);
-        ptr = nullptr;
-        count = 0;
-    }
-    T* get() const { return ptr; }
-    size_t bytes() const { return count * sizeof(T); }
-};
 
 } // namespace qg

@@ -2,7 +2,7 @@
 // writes) plus its device copy, rebuilt lazily after writes.
 #pragma once
 
-#include "qg_common.cuh"
+#include "qg_cuda.h"
 #include "qg_host.h"
 #include "qg_search.h"
 

@@ -1,0 +1,58 @@
+// GPU kernels of training (k-means / e-means / PQ codebooks) and the host
+// entry points that drive them.
+#pragma once
+
+#include "qg_cuda.h"
+
+#include <cstdint>
+#include <optional>
+#include <vector>
+
+namespace qg {
+
+// ---- device steps (qg_train.cu); P independent problems of n points x d dims
+// and k centroids each, packed problem-major. -----------------------------------
+
+// assign[p][i] = nearest centroid (squared L2 in the reference's AVX2 order,
+// first index on ties), for small k (PQ codebooks).
+void assign_small(const float* x, size_t n, int d, const float* c, int k, int P, uint32_t* assign, cudaStream_t st);
+
+// out[p][c][l] = x[order[off[c]]][l] + x[order[off[c] + 1]][l] + ... summed in
+// float from 0 in the order given (the reference adds members in point order).
+// order / off are per problem: order P x n, off P x (k + 1).
+void member_sums(const float* x, size_t n, int d, const uint32_t* order, const uint32_t* off, int k, int P, float* out,
+                 cudaStream_t st);
+
+// dist[p][i] = squared L2 (AVX2 order) of point i to centroid assign[p][i].
+void own_dist(const float* x, size_t n, int d, const float* c, int k, const uint32_t* assign, int P, float* dist,
+              cudaStream_t st);
+
+// rows[i] = src[idx[i]] (n rows of d floats).
+void gather_rows(const float* src, const uint32_t* idx, size_t n, int d, float* out, cudaStream_t st);
+// out[i] = x[i] - centers[assign[i]]
+void residuals(const float* x, size_t n, int d, const float* centers, const uint32_t* assign, float* out,
+               cudaStream_t st);
+// out[p][i][0..d) = x[i][p*d .. (p+1)*d): the subspace columns, problem-major
+void split_columns(const float* x, size_t n, int dim, int d, int P, float* out, cudaStream_t st);
+
+// ---- host algorithms (qg_train_host.cpp) ----------------------------------------
+
+struct KMeansOut {
+    std::vector<float> centroids;   // P * k * d
+    std::vector<uint32_t> assign;   // P * n
+};
+
+// Lloyd's k-means (reference src/kmeans.cpp:174-252) for P problems at once
+// (x_dev: P x n x d); problem p starts from seeds[p], or a random seed.
+KMeansOut kmeans_lloyd(const float* x_dev, size_t n, int d, int k, size_t iters,
+                       const std::vector<std::optional<uint32_t>>& seeds, bool spherical, int P, cudaStream_t st);
+
+// e-means (reference src/kmeans.cpp:280-414), one problem.
+KMeansOut emeans(const float* x_dev, size_t n, int d, int k, size_t passes, std::optional<uint32_t> seed,
+                 bool spherical, cudaStream_t st);
+
+// PQ codes (K = 16) of x - centers[assign] (qg_build.cu).
+void encode16(const float* x, size_t n, int dim, const float* centers, const uint32_t* assign, const float* yt, int m,
+              int sd, uint8_t* codes, cudaStream_t st);
+
+} // namespace qg

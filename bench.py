@@ -1,0 +1,437 @@
+#!/usr/bin/env python
+"""Headline benchmark: the angular IVF-PQ fast-scan + RefineIndex workload.
+
+Workload (synthetic stand-in for a GloVe-100-angular-shaped set; the real set
+is not available offline): 2,000 centres ~ N(0, I_100), cluster c drawn with
+p ~ (c + 1)^-1.1, row = centre + 0.3 * N(0, I), L2-normalised; 1,200,000 base
+rows (seed 0) and 10,000 queries (seed 1) from the same mixture; cosine;
+IVFIndex(nlist 4096) + PQ 50 x 4-bit fast-scan trained with e-means (seed 1),
+RefineIndex(k_factor 10), k = 10. nprobe is the smallest of 8..256 whose
+recall@10 (against exact brute force) reaches 0.95; the metric is queries per
+second at that nprobe.
+
+One step = one batch_query of the 10,000 queries. `value` is measured with
+the queries already in HBM (device-resident search, CUDA events on the
+launching stream, L2 flushed between steps); `e2e` is the same metric through
+the public Python API with host arrays (copies in and out inside the timed
+region). `cpu_baseline` times the reference's own C++ build (oracle/_ref) on
+the host cores on a bounded sample of the same queries.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl qann_b200|reference]
+
+For N > 1 every rank holds a replica of the index and serves its own 10,000
+queries (seed 1 + rank): weak scaling with no collective on the data path;
+the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+os.environ.setdefault("QANN_DISABLE_AVX512", "1")
+
+# nprobe is swept over 8..256 as the workload names it, and on to 1024 when
+# recall@10 has not reached 0.95 by 256
+FULL = dict(n=1_200_000, d=100, centres=2000, zipf=1.1, sigma=0.3, nq=10_000, nlist=4096, m=50, k=10, kf=10,
+            train_seed=1, nprobes=[8, 16, 32, 64, 128, 256, 384, 512, 768, 1024], target=0.95)
+SMALL = dict(FULL, n=120_000, nq=2_000, nlist=512)   # --small: a quick functional check, not a bench line
+CACHE = pathlib.Path(os.environ.get("QANN_B200_BENCH_CACHE", "/tmp/qann_b200_bench"))
+L2_FLUSH_BYTES = 256 << 20   # twice the B200's 126 MB L2
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---- data --------------------------------------------------------------------------------
+
+def mixture(cfg, seed_rows, nrows):
+    c_rng = np.random.default_rng(12345)
+    centres = c_rng.standard_normal((cfg["centres"], cfg["d"]), dtype=np.float32)
+    p = (np.arange(cfg["centres"]) + 1.0) ** -cfg["zipf"]
+    p /= p.sum()
+    rng = np.random.default_rng(seed_rows)
+    lab = rng.choice(cfg["centres"], size=nrows, p=p)
+    x = centres[lab] + np.float32(cfg["sigma"]) * rng.standard_normal((nrows, cfg["d"]), dtype=np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    return np.ascontiguousarray(x, dtype=np.float32)
+
+
+def tag(cfg):
+    return f"angular_{cfg['n']}x{cfg['d']}_nl{cfg['nlist']}_m{cfg['m']}_kf{cfg['kf']}"
+
+
+def build_or_load(cfg, base, rank, world, barrier):
+    import qann_b200 as qb
+    CACHE.mkdir(parents=True, exist_ok=True)
+    path = CACHE / f"{tag(cfg)}.qann"
+    if rank == 0 and not path.exists():
+        t = time.time()
+        ivf = qb.IVFIndex(cfg["d"], cfg["nlist"], 16, metric=qb.Metric.Cosine)
+        ivf.enable_pq(cfg["m"], fast_scan=True)
+        ivf.train(base, seed=cfg["train_seed"])
+        t_train = time.time() - t
+        r = qb.RefineIndex(ivf, cfg["kf"])
+        r.add(base)
+        t_add = time.time() - t - t_train
+        r.save(str(path) + ".part")
+        os.replace(str(path) + ".part", path)
+        log(f"built index on the GPU: train {t_train:.1f}s add {t_add:.1f}s "
+            f"(cosine_inner_product={ivf.cosine_inner_product})")
+    barrier()
+    return qb.load(path), path
+
+
+def ground_truth(cfg, base, queries, dev):
+    """Exact top-k by cosine: fp32 similarities on the GPU to pick 64 candidates,
+    rescored in fp64 (measurement only)."""
+    import torch
+    digest = hashlib.sha1(queries[:16].tobytes()).hexdigest()[:12]
+    path = CACHE / f"{tag(cfg)}_gt_{queries.shape[0]}_{digest}.npy"
+    if path.exists():
+        return np.load(path)
+    torch.backends.cuda.matmul.allow_tf32 = False
+    b = torch.from_numpy(base).to(dev)
+    out = np.empty((queries.shape[0], cfg["k"]), np.int64)
+    for s in range(0, queries.shape[0], 1000):
+        q = torch.from_numpy(queries[s:s + 1000]).to(dev)
+        cand = torch.topk(q @ b.T, 64, dim=1).indices
+        exact = torch.einsum("qd,qcd->qc", q.double(), b[cand].double())
+        order = torch.argsort(-exact, dim=1, stable=True)[:, :cfg["k"]]
+        out[s:s + 1000] = torch.gather(cand, 1, order).cpu().numpy()
+    del b
+    np.save(path, out)
+    return out
+
+
+def recall(ids, gt):
+    k = gt.shape[1]
+    return float(np.mean([len(set(a[:k]) & set(b)) / k for a, b in zip(ids, gt)]))
+
+
+def choose_nprobe(cfg, index, queries, gt):
+    ivf = index.base
+    path = CACHE / f"{tag(cfg)}_sweep.json"
+    if path.exists():
+        return json.loads(path.read_text())
+    sweep = {}
+    chosen = None
+    for npb in cfg["nprobes"]:
+        ivf.nprobe = npb
+        ids, _ = index.batch_query(queries, cfg["k"])
+        sweep[str(npb)] = round(recall(ids, gt), 4)
+        log(f"nprobe {npb}: recall@10 {sweep[str(npb)]}")
+        if chosen is None and sweep[str(npb)] >= cfg["target"]:
+            chosen = npb
+            break
+    res = {"sweep": sweep, "nprobe": chosen or cfg["nprobes"][-1]}
+    path.write_text(json.dumps(res))
+    return res
+
+
+# ---- measurement helpers ---------------------------------------------------------------------
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "50", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        time.sleep(0.1)
+        return self
+
+    def __exit__(self, *exc):
+        time.sleep(0.1)
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out, _ = self.p.communicate()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak(key, fallback):
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())[key]), "measured"
+    except Exception:
+        return fallback, "fallback"
+
+
+def scan_traffic():
+    """dram bytes per scan launch from the committed ncu summary, when present."""
+    p = ROOT / "profiles" / "scan_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("bytes_per_launch="):
+            return float(line.split("=", 1)[1])
+    return None
+
+
+def algorithmic_scan_bytes(cfg, index, queries, nprobe, dev):
+    """Code bytes the scan must read per launch: for every (query, probed
+    list), the list's vectors x m/2 bytes (4-bit codes)."""
+    import torch
+    ivf = index.base
+    sizes = torch.from_numpy(ivf.list_sizes().astype(np.int64)).to(dev)
+    cent = torch.from_numpy(ivf.centroids()).to(dev)
+    total = 0
+    for s in range(0, queries.shape[0], 2000):
+        q = torch.from_numpy(queries[s:s + 2000]).to(dev)
+        d2 = (q * q).sum(1, keepdim=True) - 2 * q @ cent.T + (cent * cent).sum(1)[None]
+        probes = torch.topk(d2, nprobe, dim=1, largest=False).indices
+        total += int(sizes[probes].sum())
+    return total * cfg["m"] // 2
+
+
+# ---- the reference arm -------------------------------------------------------------------------
+
+def reference_arm(args, cfg):
+    from oracle import ref
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libqann_ref.so was not built"}))
+        return 0
+    import torch
+    dev = torch.device("cuda:0")
+    base = mixture(cfg, 0, cfg["n"])
+    queries = mixture(cfg, 1, cfg["nq"])
+    index, path = build_or_load(cfg, base, 0, 1, lambda: None)
+    gt = ground_truth(cfg, base, queries, dev)
+    sel = choose_nprobe(cfg, index, queries, gt)
+    del index
+    r = ref.load(path)
+    r.base.nprobe = sel["nprobe"]
+    cores = os.cpu_count() or 1
+    ref.set_num_threads(cores)
+    # size each step to ~2 s of CPU work from a short probe
+    t = time.time()
+    r.batch_query(queries[:200], cfg["k"])
+    per_q = max((time.time() - t) / 200, 1e-6)
+    sample = int(min(cfg["nq"], max(200, 2.0 / per_q)))
+    for w in range(args.warmup):
+        r.batch_query(queries[:sample], cfg["k"])
+    times = []
+    for s in range(args.steps):
+        off = (s * sample) % max(1, cfg["nq"] - sample + 1)
+        t = time.perf_counter()
+        ids, _ = r.batch_query(queries[off:off + sample], cfg["k"])
+        times.append(time.perf_counter() - t)
+    qps = sample * len(times) / sum(times)
+    rec = recall(r.batch_query(queries[:2000], cfg["k"])[0], gt[:2000])
+    line = {
+        "impl": "reference", "metric": "QPS@recall10>=0.95 (angular 1.2Mx100, IVF4096-PQ50x4fs + refine kf10)",
+        "value": round(qps, 1), "unit": "queries/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": tag(cfg), "nprobe": sel["nprobe"], "k": cfg["k"], "k_factor": cfg["kf"],
+                   "queries_per_step": sample, "recall@10": round(rec, 4), "threads": cores,
+                   "index": "built by qann_b200 on the GPU, byte-identical to the reference's own train+add "
+                            "(tests/test_gpu_build.py); loaded and queried by the reference library"},
+        "cpu_baseline": {"value": round(qps, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
+                         "sample": f"{sample} queries per step"},
+        "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---- our arm -------------------------------------------------------------------------------------
+
+def cpu_baseline(cfg, path, queries, nprobe):
+    from oracle import ref
+    if not ref.available():
+        return None
+    r = ref.load(path)
+    r.base.nprobe = nprobe
+    cores = os.cpu_count() or 1
+    ref.set_num_threads(cores)
+    t = time.time()
+    r.batch_query(queries[:200], cfg["k"])
+    per_q = max((time.time() - t) / 200, 1e-6)
+    sample = int(min(queries.shape[0], max(200, 10.0 / per_q)))
+    t = time.perf_counter()
+    r.batch_query(queries[:sample], cfg["k"])
+    dt = time.perf_counter() - t
+    return {"value": round(sample / dt, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
+            "sample": f"{sample} of the {queries.shape[0]} queries, one batch_query on {cores} threads"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="qann_b200", choices=["qann_b200", "reference"])
+    ap.add_argument("--small", action="store_true", help="a quick functional run on a 10x smaller set")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = SMALL if args.small else FULL
+    if args.impl == "reference":
+        return reference_arm(args, cfg)
+
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    import qann_b200 as qb
+    from qann_b200 import profiling
+
+    base = mixture(cfg, 0, cfg["n"])
+    queries = mixture(cfg, 1 + rank, cfg["nq"])
+    index, path = build_or_load(cfg, base, rank, world, barrier)
+    gt = ground_truth(cfg, base, queries, dev) if rank == 0 else None
+    if rank == 0:
+        sel = choose_nprobe(cfg, index, queries, gt)
+    barrier()
+    if rank != 0:
+        sel = json.loads((CACHE / f"{tag(cfg)}_sweep.json").read_text())
+    nprobe = sel["nprobe"]
+    index.base.nprobe = nprobe
+    nq, k = cfg["nq"], cfg["k"]
+
+    # ---- device-resident steps ----
+    q_dev = torch.from_numpy(queries).to(dev)
+    out_ids = torch.empty((nq, k), dtype=torch.int64, device=dev)
+    out_d = torch.empty((nq, k), dtype=torch.float32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        index.search_device(q_dev.data_ptr(), nq, k, out_ids.data_ptr(), out_d.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    profiling.enable(True)
+    profiling.reset()
+    launches0 = profiling.launch_count()
+    step_ms = []
+    barrier()
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            index.search_device(q_dev.data_ptr(), nq, k, out_ids.data_ptr(), out_d.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    barrier()
+    launches = profiling.launch_count() - launches0
+    profiling.enable(False)
+    scan_ms, scan_n = profiling.get("scan")
+    kernel_ms = {kname: profiling.get(kname) for kname in profiling.KERNELS}
+    total_ms = float(sum(step_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = nq * args.steps * world / (total_ms / 1e3)
+    got = out_ids.cpu().numpy()
+
+    # ---- end to end through the public API, host arrays ----
+    e2e_times = []
+    for _ in range(max(3, args.steps // 5)):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ids_h, _ = index.batch_query(queries, k)
+        e2e_times.append(time.perf_counter() - t)
+    e2e_qps = nq * len(e2e_times) / sum(e2e_times)
+    if dist is not None:
+        t = torch.tensor([sum(e2e_times)], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_qps = nq * len(e2e_times) * world / float(t.item())
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    rec = recall(got, gt)
+    assert np.array_equal(got, ids_h), "device-resident and host-API results differ"
+    alg_bytes = algorithmic_scan_bytes(cfg, index, queries, nprobe, dev)
+    per_launch_ms = scan_ms / max(1, scan_n)
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    peak, peak_src = measured_peak("hbm_gbs", 6650.0)
+    traffic = scan_traffic()
+    cpu = None if (args.no_cpu_baseline or world > 1) else cpu_baseline(cfg, path, queries, nprobe)
+    srt = sorted(step_ms)
+    line = {
+        "metric": "QPS@recall10>=0.95 (angular 1.2Mx100, IVF4096-PQ50x4fs + refine kf10)",
+        "value": round(value, 1), "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": tag(cfg), "nq": nq, "k": k, "k_factor": cfg["kf"], "nprobe": nprobe,
+                   "recall@10": round(rec, 4), "sweep": sel["sweep"], "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"replicas x{world}", "batch_latency_ms": {
+                       "p50": round(srt[len(srt) // 2], 4), "p99": round(srt[min(len(srt) - 1, int(0.99 * len(srt)))], 4)},
+                   "kernel_ms_total": {kk: round(v[0], 3) for kk, v in kernel_ms.items() if v[1]}},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
+                     "kernel": "k_scan", "algorithmic_bytes_per_launch": alg_bytes,
+                     "launch_ms": round(per_launch_ms, 4)},
+        "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": nq * cfg["d"] * 4,
+                "d2h_bytes_per_step": nq * k * 12, "timing": "host wall clock around the blocking batch_query"},
+        "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -107,6 +107,11 @@ int qg_search_device(qg_index* h, const float* q_dev, size_t nq, size_t k, int64
  */
 int qg_get(qg_index* h, const char* key, int64_t* value);
 int qg_set(qg_index* h, const char* key, int64_t value);
+/* IVF inspection (for sizing and accounting; the reference keeps these
+ * private, reference include/vecengine/ivf_index.hpp:251-283): the vector
+ * count of each of the nlist lists, and the nlist x dim coarse centroids. */
+int qg_ivf_list_sizes(qg_index* h, uint32_t* out_sizes);
+int qg_ivf_centroids(qg_index* h, float* out_centroids);
 
 /* --- files ------------------------------------------------------------------------
  * .qann format 13, interchangeable with qann (reference src/index_factory.cpp:94-141).
@@ -114,6 +119,18 @@ int qg_set(qg_index* h, const char* key, int64_t value);
  */
 int qg_save(qg_index* h, const char* path);
 int qg_load(const char* path, qg_index** out, int* kind);
+
+/* --- profiling (no counterpart in the reference, which times sections with
+ * compile-time timers, reference src/profile.hpp) --------------------------------
+ * qg_profile_enable(1) brackets each launch of the named kernels ("scan",
+ * "pair_scores", "select_rows", "query_tables", "merge", "refine") with CUDA
+ * events on its stream; qg_profile_get folds finished timings in and returns
+ * the total milliseconds and launch count for one name; qg_launch_count is
+ * the number of this library's kernel launches since the library loaded. */
+int qg_profile_enable(int on);
+int qg_profile_reset(void);
+int qg_profile_get(const char* kernel, double* total_ms, int64_t* launches);
+int64_t qg_launch_count(void);
 
 /* --- kernels of the path on device memory (parity tests and tools) ----------------
  * qg_quantize_lut_dev: n tables of m x 16 floats -> n LUTs of m x 16 bytes plus

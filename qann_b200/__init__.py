@@ -242,6 +242,18 @@ class IVFIndex(DenseIndex):
                                     lambda self, v: self._set("filter_probe_scaling", bool(v)))
     pq_distance = property(lambda self: PQDistance(self._get("pq_distance")),
                            lambda self, v: self._set("pq_distance", int(v)))
+    def list_sizes(self) -> np.ndarray:
+        """Vectors per inverted list (nlist,), uint32."""
+        out = np.empty(self.nlist, np.uint32)
+        check(_lib.lib.qg_ivf_list_sizes(self._h, out.ctypes.data))
+        return out
+
+    def centroids(self) -> np.ndarray:
+        """The (nlist, dim) coarse centroids."""
+        out = np.empty((self.nlist, self.dim()), np.float32)
+        check(_lib.lib.qg_ivf_centroids(self._h, out.ctypes.data))
+        return out
+
     fast_scan = property(lambda self: bool(self._get("fast_scan")))
     pq_rotate = property(lambda self: bool(self._get("rotate")))
     sq_bits = property(lambda self: self._get("sq_bits"))

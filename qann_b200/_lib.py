@@ -38,8 +38,14 @@ _SIGS = {
     "qg_search_device": (C.c_int, [_vp, _vp, _sz, _sz, _vp, _vp, _vp]),
     "qg_get": (C.c_int, [_vp, C.c_char_p, C.POINTER(_i64)]),
     "qg_set": (C.c_int, [_vp, C.c_char_p, _i64]),
+    "qg_ivf_list_sizes": (C.c_int, [_vp, _vp]),
+    "qg_ivf_centroids": (C.c_int, [_vp, _vp]),
     "qg_save": (C.c_int, [_vp, C.c_char_p]),
     "qg_load": (C.c_int, [C.c_char_p, _H, C.POINTER(C.c_int)]),
+    "qg_profile_enable": (C.c_int, [C.c_int]),
+    "qg_profile_reset": (C.c_int, []),
+    "qg_profile_get": (C.c_int, [C.c_char_p, C.POINTER(C.c_double), C.POINTER(_i64)]),
+    "qg_launch_count": (_i64, []),
     "qg_quantize_lut_dev": (C.c_int, [_vp, _sz, _sz, _vp, _vp, _vp, _vp]),
     "qg_build_quantize_lut_dev": (C.c_int, [_vp, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _vp]),
     "qg_fast_scan_dev": (C.c_int, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),

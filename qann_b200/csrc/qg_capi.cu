@@ -35,10 +35,26 @@ int guarded(F&& f) {
     }
 }
 
+// The stream-ordered allocator's default pool hands memory back to the driver
+// at every synchronisation (release threshold 0), so each search would pay for
+// fresh allocations; keep freed blocks cached in the pool instead.
+void keep_pool_memory() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return;
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    });
+}
+
 // One non-blocking stream per host thread, so concurrent searches overlap.
 cudaStream_t thread_stream() {
     thread_local cudaStream_t s = nullptr;
     if (!s) QG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    keep_pool_memory();
     return s;
 }
 
@@ -261,6 +277,7 @@ int qg_search_bitmap(qg_index* h, const float* q, size_t nq, size_t k, const uin
 int qg_search_device(qg_index* h, const float* q_dev, size_t nq, size_t k, int64_t* out_ids_dev, float* out_dists_dev,
                      void* stream) {
     return guarded([&] {
+        keep_pool_memory();
         search_common(h, q_dev, nq, k, nullptr, out_ids_dev, out_dists_dev, IoSpace::Device,
                       static_cast<cudaStream_t>(stream));
     });
@@ -342,6 +359,23 @@ int qg_set(qg_index* h, const char* key, int64_t value) {
     });
 }
 
+int qg_ivf_list_sizes(qg_index* h, uint32_t* out_sizes) {
+    return guarded([&] {
+        IVFObj& o = ivf_of(h);
+        std::shared_lock<std::shared_mutex> lk(o.mu);
+        for (size_t l = 0; l < o.model.nlist; ++l) out_sizes[l] = static_cast<uint32_t>(o.model.list_ids[l].size());
+    });
+}
+
+int qg_ivf_centroids(qg_index* h, float* out_centroids) {
+    return guarded([&] {
+        IVFObj& o = ivf_of(h);
+        std::shared_lock<std::shared_mutex> lk(o.mu);
+        require(o.model.trained, "train() has not be run yet", kLogicError);
+        std::copy(o.model.centroids.begin(), o.model.centroids.end(), out_centroids);
+    });
+}
+
 int qg_save(qg_index* h, const char* path) {
     return guarded([&] {
         IndexObj& o = obj(h);
@@ -415,6 +449,33 @@ int qg_load(const char* path, qg_index** out, int* kind) {
         *out = wrap(o);
     });
 }
+
+// ---- profiling ------------------------------------------------------------------
+
+int qg_profile_enable(int on) {
+    profiler().on.store(on != 0);
+    return QG_OK;
+}
+
+int qg_profile_reset(void) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> g(profiler().mu);
+        profiler().settle();
+        profiler().totals.clear();
+    });
+}
+
+int qg_profile_get(const char* kernel, double* total_ms, int64_t* launches) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> g(profiler().mu);
+        profiler().settle();
+        auto it = profiler().totals.find(kernel);
+        *total_ms = it == profiler().totals.end() ? 0.0 : it->second.first;
+        *launches = it == profiler().totals.end() ? 0 : it->second.second;
+    });
+}
+
+int64_t qg_launch_count(void) { return profiler().launches.load(); }
 
 // ---- kernels on device memory ----------------------------------------------------
 

@@ -7,9 +7,14 @@
 
 #include "qg_error.h"
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 namespace qg {
 
@@ -25,7 +30,72 @@ namespace qg {
         if (qg_e_ != cudaSuccess) ::qg::throw_cuda(qg_e_, #call, __FILE__, __LINE__); \
     } while (0)
 
-#define QG_LAUNCH_CHECK() QG_CUDA(cudaGetLastError())
+// ---------------------------------------------------------------------------
+// Profiling: a count of this library's kernel launches, and (when enabled)
+// CUDA-event timings of named kernels recorded on the stream they run on.
+// ---------------------------------------------------------------------------
+struct Profiler {
+    std::atomic<bool> on{false};
+    std::atomic<int64_t> launches{0};
+    std::mutex mu;
+    struct Pending {
+        std::string name;
+        cudaEvent_t start, stop;
+    };
+    std::vector<Pending> pending;
+    std::map<std::string, std::pair<double, int64_t>> totals;   // name -> (ms, launches)
+
+    void settle() {   // folds finished event pairs into the totals (caller holds mu)
+        for (auto& p : pending) {
+            float ms = 0.0f;
+            if (cudaEventSynchronize(p.stop) == cudaSuccess && cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
+                auto& t = totals[p.name];
+                t.first += ms;
+                t.second += 1;
+            }
+            cudaEventDestroy(p.start);
+            cudaEventDestroy(p.stop);
+        }
+        pending.clear();
+    }
+};
+
+inline Profiler& profiler() {
+    static Profiler p;
+    return p;
+}
+
+// Brackets one kernel launch with events on its stream when profiling is on.
+class KernelTimer {
+public:
+    KernelTimer(const char* name, cudaStream_t st) : st_(st) {
+        if (!profiler().on.load(std::memory_order_relaxed)) return;
+        name_ = name;
+        if (cudaEventCreate(&a_) != cudaSuccess || cudaEventCreate(&b_) != cudaSuccess) return;
+        cudaEventRecord(a_, st_);
+        armed_ = true;
+    }
+    ~KernelTimer() {
+        if (!armed_) return;
+        cudaEventRecord(b_, st_);
+        std::lock_guard<std::mutex> g(profiler().mu);
+        profiler().pending.push_back({name_, a_, b_});
+    }
+    KernelTimer(const KernelTimer&) = delete;
+    KernelTimer& operator=(const KernelTimer&) = delete;
+
+private:
+    cudaStream_t st_;
+    std::string name_;
+    cudaEvent_t a_{}, b_{};
+    bool armed_ = false;
+};
+
+#define QG_LAUNCH_CHECK()                                                       \
+    do {                                                                        \
+        ::qg::profiler().launches.fetch_add(1, std::memory_order_relaxed);      \
+        QG_CUDA(cudaGetLastError());                                            \
+    } while (0)
 
 // ---------------------------------------------------------------------------
 inline size_t ceil_div(size_t a, size_t b) { return (a + b - 1) / b; }

@@ -145,6 +145,7 @@ void pair_scores(const float* A, int na, const float* B, int nb, int d, bool ip,
                  cudaStream_t st) {
     if (na == 0 || nb == 0) return;
     dim3 grid(static_cast<unsigned>(ceil_div(nb, kTB)), static_cast<unsigned>(ceil_div(na, kTA)));
+    KernelTimer kt("pair_scores", st);
     if (ip) k_pair_scores<true><<<grid, 256, 0, st>>>(A, na, B, nb, d, out, ld_out);
     else k_pair_scores<false><<<grid, 256, 0, st>>>(A, na, B, nb, d, out, ld_out);
     QG_LAUNCH_CHECK();
@@ -274,6 +275,7 @@ void select_rows(const float* scores, size_t ld, int nrows, int ncols, int P, ui
     const size_t smem = static_cast<size_t>(next_pow2(P)) * 16;
     if (smem > 48 * 1024)
         QG_CUDA(cudaFuncSetAttribute(k_select_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    KernelTimer kt("select_rows", st);
     k_select_rows<<<nrows, 256, smem, st>>>(scores, ld, ncols, P, allow, deny, col_base, eq0, out_col, out_score);
     QG_LAUNCH_CHECK();
 }
@@ -725,6 +727,7 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
         const size_t smem = static_cast<size_t>(v.m) * 17 * 4;
         if (smem > 48 * 1024)
             QG_CUDA(cudaFuncSetAttribute(k_query_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        KernelTimer kt("query_tables", st);
         k_query_tables<<<nq, 128, smem, st>>>(v, s.q, qC.get(), qlut.get(), qscale.get(), qoffset.get());
         QG_LAUNCH_CHECK();
     }
@@ -768,7 +771,10 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     a.out_slot = direct ? out_slot : cslot.get();
     a.err = s.d_err;
     QG_CUDA(cudaFuncSetAttribute(k_scan<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    k_scan<NT><<<static_cast<unsigned>(nq * nchunks), NT, smem, st>>>(a);
+    {
+        KernelTimer kt("scan", st);
+        k_scan<NT><<<static_cast<unsigned>(nq * nchunks), NT, smem, st>>>(a);
+    }
     QG_LAUNCH_CHECK();
     if (!direct) merge_candidates(ckey.get(), cslot.get(), nq, nchunks, kp, out_key, out_slot, st);
 }
@@ -780,6 +786,7 @@ void merge_candidates(const uint64_t* in_key, const uint32_t* in_slot, int nq, i
     const size_t msm = static_cast<size_t>(capm) * 16;
     if (msm > 48 * 1024)
         QG_CUDA(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm)));
+    KernelTimer kt("merge", st);
     k_merge<<<nq, 256, msm, st>>>(in_key, in_slot, nchunks, kp, capm, out_key, out_slot);
     QG_LAUNCH_CHECK();
 }
@@ -800,6 +807,7 @@ void refine_candidates(const float* q, int nq, int dim, const float* rows, const
     const size_t rsm = static_cast<size_t>(kpow) * 16 + static_cast<size_t>(dim) * 4;
     if (rsm > 48 * 1024)
         QG_CUDA(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(rsm)));
+    KernelTimer kt("refine", st);
     k_refine<<<nq, 128, rsm, st>>>(q, dim, rows, key, slot, kp, k, ip, labels, cosine, out_ids, out_d);
     QG_LAUNCH_CHECK();
 }

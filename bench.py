@@ -126,7 +126,7 @@ def choose_nprobe(cfg, index, queries, gt):
         return json.loads(path.read_text())
     sweep = {}
     chosen = None
-    for npb in cfg["nprobes"]:
+    for npb in [p for p in cfg["nprobes"] if p <= cfg["nlist"]]:
         ivf.nprobe = npb
         ids, _ = index.batch_query(queries, cfg["k"])
         sweep[str(npb)] = round(recall(ids, gt), 4)
@@ -308,6 +308,7 @@ def main():
     ap.add_argument("--impl", default="qann_b200", choices=["qann_b200", "reference"])
     ap.add_argument("--small", action="store_true", help="a quick functional run on a 10x smaller set")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nprobe", type=int, default=0, help="use this nprobe instead of the recall sweep (profiling)")
     args = ap.parse_args()
     cfg = SMALL if args.small else FULL
     if args.impl == "reference":
@@ -336,10 +337,12 @@ def main():
     queries = mixture(cfg, 1 + rank, cfg["nq"])
     index, path = build_or_load(cfg, base, rank, world, barrier)
     gt = ground_truth(cfg, base, queries, dev) if rank == 0 else None
-    if rank == 0:
+    if args.nprobe:
+        sel = {"sweep": {}, "nprobe": args.nprobe}
+    elif rank == 0:
         sel = choose_nprobe(cfg, index, queries, gt)
     barrier()
-    if rank != 0:
+    if rank != 0 and not args.nprobe:
         sel = json.loads((CACHE / f"{tag(cfg)}_sweep.json").read_text())
     nprobe = sel["nprobe"]
     index.base.nprobe = nprobe

@@ -38,6 +38,26 @@ __device__ __noinline__ static void bitonic_sort(uint64_t* key, int64_t* val, in
     __syncthreads();
 }
 
+// Keys only (unique keys need no tie-break).
+__device__ __noinline__ static void bitonic_sort_keys(uint64_t* key, int n) {
+    for (int size = 2; size <= n; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            __syncthreads();
+            for (int t = threadIdx.x; t < (n >> 1); t += blockDim.x) {
+                const int lo = 2 * t - (t & (stride - 1));
+                const int hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const uint64_t k0 = key[lo], k1 = key[hi];
+                if (up ? (k1 < k0) : (k0 < k1)) {
+                    key[lo] = k1;
+                    key[hi] = k0;
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
 __host__ __device__ __forceinline__ int next_pow2(int n) {
     int p = 1;
     while (p < n) p <<= 1;

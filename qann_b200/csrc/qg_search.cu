@@ -334,237 +334,6 @@ __global__ void k_query_tables(IvfView v, const float* __restrict__ q, float* __
 }
 
 // ---------------------------------------------------------------------------
-// The code scan with fused top-k'.
-//
-// A block handles one query and a chunk of its probes, in probe order. Per
-// probe it builds the list's uint8 LUT in shared memory (mode L2: B + C + A
-// rounded, as build_quantize_lut; mode L2-ADC: the residual's ADC table
-// rounded; modes IP / cosine-IP: the query's one LUT). Octets of 8 threads
-// then take superblocks (64 vectors) of the chunk's lists in turn.
-//
-// Selection keeps the k' smallest candidates by key64 = key(dist) << 32 |
-// push index, the push index being the vector's position in the query's
-// sequence of probed lists: exactly the set the reference's TopK keeps
-// (distance first, first pushed among ties; reference src/topk.hpp:20-25,
-// :94-131). Candidates go to a shared buffer when key64 beats the current
-// k'-th key; the buffer is sorted and cut back to k' when it fills, which
-// lowers the threshold. Deleted (or filtered-out) vectors are skipped before
-// they can enter, as the reference's push() does. The integer pre-test
-// sum <= S* is exact: S* is the largest sum whose distance is <= the
-// threshold distance (sum_limit).
-// ---------------------------------------------------------------------------
-struct ScanSmem {
-    int count;
-    int overflow;
-    uint64_t thr;
-};
-
-template <int NT>
-__global__ void __launch_bounds__(NT) k_scan(ScanArgs a) {
-    extern __shared__ __align__(16) uint8_t sm[];
-    constexpr int NW = NT / 32, NOCT = NT / 8;
-    const IvfView& v = a.v;
-    const int qi = blockIdx.x / a.nchunks;
-    const int chunk = blockIdx.x - qi * a.nchunks;
-    const int p0 = chunk * a.pch;
-    const int np = min(a.P, p0 + a.pch) - p0;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
-    const int nlut = shared_lut ? 1 : a.pch;
-
-    // shared memory carve-up (see scan_smem_bytes)
-    uint64_t* ckey = reinterpret_cast<uint64_t*>(sm);
-    int64_t* cval = reinterpret_cast<int64_t*>(ckey + a.cap);
-    uint4* lut = reinterpret_cast<uint4*>(cval + a.cap);
-    float* scratch = reinterpret_cast<float*>(lut + static_cast<size_t>(nlut) * v.m_pad);   // per warp: row minimums
-    const int scr_per_warp = v.m_pad;
-    float* qtab = scratch + NW * scr_per_warp;     // mode L2: C (m*16 floats); mode L2-ADC: the query (dim)
-    const int qtab_len = v.mode == kModeL2 ? v.m * 16 : (v.mode == kModeL2Adc ? v.dim : 0);
-    float* p_scale = qtab + qtab_len;
-    float* p_offset = p_scale + a.pch;
-    int* p_smax = reinterpret_cast<int*>(p_offset + a.pch);
-    uint32_t* p_list = reinterpret_cast<uint32_t*>(p_smax + a.pch);
-    uint32_t* p_size = p_list + a.pch;
-    uint32_t* p_push = p_size + a.pch;
-    uint32_t* p_sbpre = p_push + a.pch;   // pch + 1
-    __shared__ ScanSmem st;
-    __shared__ uint32_t red[NW];
-
-    const size_t qp = static_cast<size_t>(qi) * a.P;
-    if (tid == 0) {
-        st.count = 0;
-        st.overflow = 0;
-        st.thr = ~0ull;
-    }
-    // vectors in probes before this chunk: the push index base
-    uint32_t before = 0;
-    for (int p = tid; p < p0; p += NT) before += v.list_size[a.probe[qp + p]];
-    for (int o = 16; o > 0; o >>= 1) before += __shfl_xor_sync(0xffffffffu, before, o);
-    if (lane == 0) red[warp] = before;
-    for (int p = tid; p < np; p += NT) {
-        const uint32_t l = a.probe[qp + p0 + p];
-        p_list[p] = l;
-        p_size[p] = v.list_size[l];
-    }
-    if (v.mode == kModeL2)
-        for (int t = tid; t < v.m * 16; t += NT) qtab[t] = a.qC[static_cast<size_t>(qi) * v.m * 16 + t];
-    if (v.mode == kModeL2Adc)
-        for (int t = tid; t < v.dim; t += NT) qtab[t] = a.q[static_cast<size_t>(qi) * v.dim + t];
-    __syncthreads();
-    if (tid == 0) {
-        uint32_t base = 0;
-        for (int w = 0; w < NW; ++w) base += red[w];
-        uint32_t sb = 0;
-        for (int p = 0; p < np; ++p) {
-            p_push[p] = base;
-            base += p_size[p];
-            p_sbpre[p] = sb;
-            sb += (p_size[p] + kSuperBlock - 1) / kSuperBlock;
-        }
-        p_sbpre[np] = sb;
-    }
-
-    // ---- LUTs, scales and offsets -------------------------------------------
-    if (shared_lut) {
-        for (int r = tid; r < v.m_pad; r += NT) lut[r] = a.qlut[static_cast<size_t>(qi) * v.m_pad + r];
-        for (int p = tid; p < np; p += NT) {
-            p_scale[p] = a.qscale[qi];
-            p_offset[p] = __fadd_rn(a.qoffset[qi], a.pterm[qp + p0 + p]);
-        }
-    } else {
-        float* rmin = scratch + warp * scr_per_warp;
-        for (int p = warp; p < np; p += NW) {
-            const uint32_t l = a.probe[qp + p0 + p];
-            float s, o;
-            if (v.mode == kModeL2) {
-                const float A = a.pterm[qp + p0 + p];
-                const float* B = v.B + static_cast<size_t>(l) * v.m * 16;
-                warp_quantize_lut(
-                    [&](int r, float* out) {
-#pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            float t = __fadd_rn(B[r * 16 + j], qtab[r * 16 + j]);
-                            if (r == 0) t = __fadd_rn(t, A);
-                            out[j] = t;
-                        }
-                    },
-                    v.m, v.m_pad, rmin, lut + static_cast<size_t>(p) * v.m_pad, s, o);
-            } else {
-                // the residual (q - center) is formed per element inside the table
-                // loop, as compute_adc_table reads it (reference src/ivf_index.cpp:594-610)
-                const float* ctr = v.resid + static_cast<size_t>(l) * v.dim;
-                warp_quantize_lut(
-                    [&](int r, float* out) {
-#pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            float acc = 0.0f;
-                            for (int u = 0; u < v.sd; ++u) {
-                                const int e = r * v.sd + u;
-                                const float diff = __fsub_rn(__fsub_rn(qtab[e], ctr[e]), v.pq_t[e * 16 + j]);
-                                acc = __fmaf_rn(diff, diff, acc);
-                            }
-                            out[j] = acc;
-                        }
-                    },
-                    v.m, v.m_pad, rmin, lut + static_cast<size_t>(p) * v.m_pad, s, o);
-            }
-            if (lane == 0) {
-                p_scale[p] = s;
-                p_offset[p] = o;
-            }
-        }
-    }
-    __syncthreads();
-    for (int p = tid; p < np; p += NT) p_smax[p] = 65535;
-    __syncthreads();
-
-    // ---- rounds over superblocks --------------------------------------------
-    const int total = static_cast<int>(p_sbpre[np]);
-    const int oct = tid >> 3, r = tid & 7;
-    for (int base = 0; base < total; base += NOCT) {
-        const int item = base + oct;
-        if (item < total) {
-            int pl = 0;
-            while (pl + 1 < np && static_cast<int>(p_sbpre[pl + 1]) <= item) ++pl;
-            const int sbl = item - static_cast<int>(p_sbpre[pl]);
-            const uint32_t l = p_list[pl];
-            const size_t sbg = static_cast<size_t>(v.sb_off[l]) + sbl;
-            const uint4* sbp = v.codes + sbg * static_cast<size_t>(2 * v.m_pad);
-            const uint4* L = lut + static_cast<size_t>(shared_lut ? 0 : pl) * v.m_pad;
-            uint32_t sums[8];
-            octet_sums(sbp, L, v.m_pad, r, sums);
-            const int smax = p_smax[pl];
-            const uint32_t size = p_size[pl];
-            const float scale = p_scale[pl], offset = p_offset[pl];
-            const uint64_t thr = st.thr;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const uint32_t pos = static_cast<uint32_t>(sbl) * kSuperBlock + 8 * r + i;
-                if (pos < size && static_cast<int>(sums[i]) <= smax) {
-                    const float dist = fs_dist(sums[i], scale, offset);
-                    const uint64_t key = (static_cast<uint64_t>(float_key(dist)) << 32) | (p_push[pl] + pos);
-                    if (key < thr) {
-                        const uint32_t slot = v.ids[sbg * kSuperBlock + 8 * r + i];
-                        const bool ok = a.filter ? ((a.filter[slot >> 6] >> (slot & 63)) & 1ull)
-                                                 : !(v.deleted && ((v.deleted[slot >> 6] >> (slot & 63)) & 1ull));
-                        if (ok) {
-                            const int idx = atomicAdd(&st.count, 1);
-                            if (idx < a.cap) {
-                                ckey[idx] = key;
-                                cval[idx] = slot;
-                            } else {
-                                st.overflow = 1;
-                            }
-                        }
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        const bool last = base + NOCT >= total;
-        if (st.count > a.cap - NOCT * kSuperBlock || (last && st.count > 0)) {
-            const int n = min(st.count, a.cap);
-            const int npow = max(2, next_pow2(n));
-            for (int i = n + tid; i < npow; i += NT) {
-                ckey[i] = ~0ull;
-                cval[i] = INT64_MAX;
-            }
-            bitonic_sort(ckey, cval, npow);
-            if (tid == 0) {
-                if (n >= a.kp) st.thr = ckey[a.kp - 1];
-                st.count = min(n, a.kp);
-            }
-            __syncthreads();
-            const uint32_t tk = static_cast<uint32_t>(st.thr >> 32);
-            for (int p = tid; p < np; p += NT) p_smax[p] = sum_limit(st.thr == ~0ull ? 0xFFFFFFFFu : tk, p_scale[p], p_offset[p]);
-            __syncthreads();
-        }
-    }
-    // ---- output: this chunk's k' best, sorted by key64 ----------------------------
-    const int n = st.count;
-    const size_t ob = static_cast<size_t>(blockIdx.x) * a.kp;
-    for (int i = tid; i < a.kp; i += NT) {
-        a.out_key[ob + i] = i < n ? ckey[i] : ~0ull;
-        a.out_slot[ob + i] = i < n ? static_cast<uint32_t>(cval[i]) : 0xFFFFFFFFu;
-    }
-    if (tid == 0 && st.overflow) atomicExch(a.err, 1);
-}
-
-size_t scan_smem_bytes(const IvfView& v, int pch, int cap, int nt) {
-    const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
-    const int nlut = shared_lut ? 1 : pch;
-    const int nw = nt / 32;
-    const int scr = v.m_pad;
-    const int qtab = v.mode == kModeL2 ? v.m * 16 : (v.mode == kModeL2Adc ? v.dim : 0);
-    size_t b = static_cast<size_t>(cap) * 16;
-    b += static_cast<size_t>(nlut) * v.m_pad * 16;
-    b += static_cast<size_t>(nw) * scr * 4;
-    b += static_cast<size_t>(qtab) * 4;
-    b += static_cast<size_t>(pch) * 4 * 7 + 4 + 16;   // per-probe arrays: 7 of pch words, plus p_sbpre's last
-    return b;
-}
-
-// ---------------------------------------------------------------------------
 // Merge: the k' smallest key64 of a query's chunk outputs, sorted. The buffer
 // holds the current best k' and the next batch of entries.
 // ---------------------------------------------------------------------------
@@ -689,94 +458,24 @@ void normalize_rows(const float* x, float* y, int n, int d, int* d_zero, cudaStr
     QG_LAUNCH_CHECK();
 }
 
-int scan_cap(int kp) {
-    // room for k' kept entries plus one full round of candidates (16 octets of a
-    // 128-thread block, 64 vectors each)
-    return next_pow2(kp + 16 * kSuperBlock);
+
+void probe_terms(const IvfView& v, const float* q, int nq, int P, const uint32_t* probe, const float* pdist, float* term,
+                 cudaStream_t st) {
+    const size_t n = static_cast<size_t>(nq) * P;
+    if (n == 0) return;
+    k_probe_terms<<<static_cast<unsigned>(ceil_div(n, 256)), 256, 0, st>>>(v, q, nq, P, probe, pdist, term);
+    QG_LAUNCH_CHECK();
 }
 
-void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st) {
-    const int nq = s.nq, P = s.nprobe, kp = s.kp;
+void query_tables(const IvfView& v, const float* q, int nq, float* qC, uint4* qlut, float* qscale, float* qoffset,
+                  cudaStream_t st) {
     if (nq == 0) return;
-    constexpr int NT = 128;
-    // coarse: all pair scores, then the P nearest lists per query
-    DevBuf<float> scores(static_cast<size_t>(nq) * v.nlist, st);
-    pair_scores(s.q, nq, v.centroids, v.nlist, v.dim, v.ip_metric, scores.get(), v.nlist, st);
-    DevBuf<uint32_t> probe(static_cast<size_t>(nq) * P, st);
-    DevBuf<float> pdist(static_cast<size_t>(nq) * P, st);
-    // (score, list) compared as the reference's heap of (float, uint16_t) pairs does: -0 == +0
-    select_rows(scores.get(), v.nlist, nq, v.nlist, P, probe.get(), pdist.get(), st, nullptr, nullptr, 0, true);
-    scores.release();
-
-    DevBuf<float> pterm(static_cast<size_t>(nq) * P, st);
-    {
-        const size_t n = static_cast<size_t>(nq) * P;
-        k_probe_terms<<<static_cast<unsigned>(ceil_div(n, 256)), 256, 0, st>>>(v, s.q, nq, P, probe.get(), pdist.get(),
-                                                                                pterm.get());
-        QG_LAUNCH_CHECK();
-    }
-    DevBuf<float> qC, qscale, qoffset;
-    DevBuf<uint4> qlut;
-    if (v.mode == kModeL2) qC.alloc(static_cast<size_t>(nq) * v.m * 16, st);
-    if (v.mode == kModeIP || v.mode == kModeCosIP) {
-        qlut.alloc(static_cast<size_t>(nq) * v.m_pad, st);
-        qscale.alloc(nq, st);
-        qoffset.alloc(nq, st);
-    }
-    if (v.mode != kModeL2Adc) {
-        const size_t smem = static_cast<size_t>(v.m) * 17 * 4;
-        if (smem > 48 * 1024)
-            QG_CUDA(cudaFuncSetAttribute(k_query_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        KernelTimer kt("query_tables", st);
-        k_query_tables<<<nq, 128, smem, st>>>(v, s.q, qC.get(), qlut.get(), qscale.get(), qoffset.get());
-        QG_LAUNCH_CHECK();
-    }
-
-    // chunking: enough blocks to fill the GPU several times over
-    const int sms = s.sm_count > 0 ? s.sm_count : 148;
-    int nchunks = std::clamp(static_cast<int>(ceil_div(static_cast<size_t>(4 * sms), nq)), 1, P);
-    int pch = static_cast<int>(ceil_div(P, nchunks));
-    const int cap = scan_cap(kp);
-    // the per-probe LUTs of a chunk must fit in shared memory
-    while (pch > 1 && scan_smem_bytes(v, pch, cap, NT) > 200 * 1024) pch = (pch + 1) / 2;
-    nchunks = static_cast<int>(ceil_div(P, pch));
-    const size_t smem = scan_smem_bytes(v, pch, cap, NT);
-    require(smem <= 227 * 1024, "fast-scan shared memory exceeds the B200 limit for this m / k * k_factor",
-            kUnsupported);
-
-    const bool direct = nchunks == 1;
-    const size_t nout = static_cast<size_t>(nq) * nchunks * kp;
-    DevBuf<uint64_t> ckey;
-    DevBuf<uint32_t> cslot;
-    if (!direct) {
-        ckey.alloc(nout, st);
-        cslot.alloc(nout, st);
-    }
-    ScanArgs a{};
-    a.v = v;
-    a.q = s.q;
-    a.probe = probe.get();
-    a.pterm = pterm.get();
-    a.qC = qC.get();
-    a.qlut = qlut.get();
-    a.qscale = qscale.get();
-    a.qoffset = qoffset.get();
-    a.filter = s.filter;
-    a.P = P;
-    a.pch = pch;
-    a.nchunks = nchunks;
-    a.kp = kp;
-    a.cap = cap;
-    a.out_key = direct ? out_key : ckey.get();
-    a.out_slot = direct ? out_slot : cslot.get();
-    a.err = s.d_err;
-    QG_CUDA(cudaFuncSetAttribute(k_scan<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    {
-        KernelTimer kt("scan", st);
-        k_scan<NT><<<static_cast<unsigned>(nq * nchunks), NT, smem, st>>>(a);
-    }
+    const size_t smem = static_cast<size_t>(v.m) * 17 * 4;
+    if (smem > 48 * 1024)
+        QG_CUDA(cudaFuncSetAttribute(k_query_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    KernelTimer kt("query_tables", st);
+    k_query_tables<<<nq, 128, smem, st>>>(v, q, qC, qlut, qscale, qoffset);
     QG_LAUNCH_CHECK();
-    if (!direct) merge_candidates(ckey.get(), cslot.get(), nq, nchunks, kp, out_key, out_slot, st);
 }
 
 void merge_candidates(const uint64_t* in_key, const uint32_t* in_slot, int nq, int nchunks, int kp, uint64_t* out_key,

@@ -67,6 +67,12 @@ void pair_scores(const float* A, int na, const float* B, int nb, int d, bool ip,
 void select_rows(const float* scores, size_t ld, int nrows, int ncols, int P, uint32_t* out_col, float* out_score,
                  cudaStream_t st, const uint64_t* allow = nullptr, const uint64_t* deny = nullptr, size_t col_base = 0,
                  bool eq0 = false);
+// Per-probe terms (A, or the cosine-IP base) and per-query tables (C, or the
+// query's uint8 LUT with its scale / offset).
+void probe_terms(const IvfView& v, const float* q, int nq, int P, const uint32_t* probe, const float* pdist, float* term,
+                 cudaStream_t st);
+void query_tables(const IvfView& v, const float* q, int nq, float* qC, uint4* qlut, float* qscale, float* qoffset,
+                  cudaStream_t st);
 // The k' = s.kp best candidates of each query, as sorted (key64, slot) lists
 // (key64 = key(dist) << 32 | push index; 0xFFFF... marks an empty entry).
 void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st);

@@ -252,4 +252,25 @@ __device__ __forceinline__ int sum_limit(uint32_t thr_key, float scale, float of
     return lo;
 }
 
+// sum_limit from an estimate: floor((thr - offset) * scale) is within a unit
+// or two of the answer unless the subtraction cancels badly; a short exact
+// walk settles it, with the binary search as the fallback.
+__device__ __forceinline__ int sum_limit_fast(uint32_t thr_key, float scale, float offset) {
+    if (thr_key == 0xFFFFFFFFu) return 65535;
+    const float x = __fmul_rn(__fsub_rn(key_float(thr_key), offset), scale);
+    if (!(x > -4.0f && x < 65540.0f)) return sum_limit(thr_key, scale, offset);
+    int s = max(-1, min(65535, __float2int_rd(x)));
+    auto pass = [&](int t) { return float_key(fs_dist(static_cast<uint32_t>(t), scale, offset)) <= thr_key; };
+    for (int it = 0; it < 4; ++it) {
+        if (s >= 0 && !pass(s)) {
+            --s;
+        } else if (s < 65535 && pass(s + 1)) {
+            ++s;
+        } else {
+            return s;   // pass(s) (or s == -1) and !pass(s + 1) (or s == 65535)
+        }
+    }
+    return sum_limit(thr_key, scale, offset);
+}
+
 } // namespace qg

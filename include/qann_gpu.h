@@ -154,6 +154,21 @@ int qg_fast_scan_dev(const uint8_t* lut_dev, size_t nluts, size_t m, const uint8
 int qg_exact_scores_dev(const float* a_dev, size_t na, const float* b_dev, size_t nb, size_t dim, int ip,
                         float* out_dev, void* stream);
 
+/* qg_fast_scan_noalloc_dev: qg_fast_scan_dev (same arguments, same sums) for
+ * callers that cannot let the library allocate device memory — processes that
+ * reserve all GPU memory for their own pool, frameworks whose allocator must
+ * be the only one, latency-critical loops where cudaMalloc's device
+ * synchronisation or failure under memory pressure is not acceptable. It
+ * allocates nothing: its scratch is one 32 MiB device array built into the
+ * library (held on every GPU that loads it), which bounds n to what fits
+ * (about 1 million vectors at m = 64; larger n returns QG_INVALID_ARGUMENT).
+ * The first call on a device looks the array up (cudaGetSymbolAddress): make
+ * it before any stream capture. Calls share the array, so calls that overlap
+ * on the GPU race; work is queued on `stream` and not waited for.
+ * No counterpart in the reference, which runs on the CPU only. */
+int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, const uint8_t* codes_dev,
+                             const uint32_t* lut_of_dev, size_t n, uint16_t* sums_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,7 @@ _SIGS = {
     "qg_build_quantize_lut_dev": (C.c_int, [_vp, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _vp]),
     "qg_fast_scan_dev": (C.c_int, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),
     "qg_exact_scores_dev": (C.c_int, [_vp, _sz, _vp, _sz, _sz, C.c_int, _vp, _vp]),
+    "qg_fast_scan_noalloc_dev": (C.c_int, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),
 }
 
 EXPORTS = tuple(_SIGS)

@@ -81,6 +81,11 @@ qg_index* wrap(std::shared_ptr<IndexObj> o) {
 
 } // namespace
 
+namespace qg {
+// lets other translation units' entry points report through qg_last_error
+void set_last_error(const std::string& msg) { t_err = msg; }
+} // namespace qg
+
 extern "C" {
 
 const char* qg_last_error(void) { return t_err.c_str(); }

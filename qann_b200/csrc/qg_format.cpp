@@ -74,7 +74,7 @@ static int64_t find_slot(bool custom, const std::vector<int64_t>& labels,
                          const std::unordered_map<int64_t, uint32_t>& slot_of, size_t slots, int64_t id) {
     if (custom) {
         auto it = slot_of.find(id);
-        return it == slot_of.end() ? -1 : it->second;
+        return it == slot_of.end() ? int64_t{-1} : static_cast<int64_t>(it->second);
     }
     if (labels.empty()) return (id < 0 || static_cast<uint64_t>(id) >= slots) ? -1 : id;
     auto it = std::lower_bound(labels.begin(), labels.end(), id);

@@ -2,8 +2,10 @@
 // add (nearest-centroid assignment, PQ encoding) that run on the GPU.
 #include "qg_device.cuh"
 #include "qg_ops.h"
+#include "qg_train.h"
 
 #include <algorithm>
+#include <cmath>
 #include <numeric>
 
 namespace qg {
@@ -180,6 +182,49 @@ static void check_err(const DevBuf<int>& err, cudaStream_t st) {
     if (h[0]) throw Error(kRuntimeError, "fast-scan candidate buffer overflowed (internal error)");
 }
 
+// Filtered probing of an IVF index (reference src/ivf_index.cpp:501-521): at
+// least min_probes lists, then on until `wanted` allowed vectors were seen.
+static void filter_probing(IvfSearchArgs& a, const IVFModel& M, const SlotBits* f, const uint64_t* f_dev, size_t k) {
+    if (!f) return;
+    a.filter = f_dev;
+    a.wanted = static_cast<int>(std::min(k, f->count));
+    size_t min_probes = M.nprobe;
+    if (M.filter_probe_scaling && f->count > 0) {
+        const double want =
+            std::ceil(0.75 * double(M.nprobe) * std::cbrt(double(M.idmap.live_count()) / double(f->count)));
+        min_probes = std::clamp<size_t>(static_cast<size_t>(std::min(want, double(M.nlist))), M.nprobe, M.nlist);
+    }
+    a.min_probes = static_cast<int>(min_probes);
+}
+
+__global__ void k_cols_to_slots(uint32_t* __restrict__ cs, size_t n, const uint32_t* __restrict__ slots) {
+    const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n && cs[t] != 0xFFFFFFFFu) cs[t] = slots[cs[t]];
+}
+
+// RefineIndex::direct_scan on the GPU: the k best allowed rows by exact score,
+// first pushed (lowest slot) among ties, then sorted by (distance, id).
+static void refine_direct(RefineObj& o, const Prepared& p, const SearchRequest& r, int dim, bool ip, bool cosine,
+                          int64_t* out_ids, float* out_d, cudaStream_t st) {
+    std::vector<uint32_t> slots;
+    slots.reserve(r.filter->count);
+    for (size_t w = 0; w < r.filter->words.size(); ++w)
+        for (uint64_t bits = r.filter->words[w]; bits; bits &= bits - 1)
+            slots.push_back(static_cast<uint32_t>(w * 64 + __builtin_ctzll(bits)));
+    const size_t n = slots.size();
+    DevBuf<uint32_t> ds(n, st);
+    QG_CUDA(cudaMemcpyAsync(ds.get(), slots.data(), n * 4, cudaMemcpyHostToDevice, st));
+    DevBuf<float> rows(n * dim, st);
+    gather_rows(o.dev.rows.get(), ds.get(), n, dim, rows.get(), st);
+    DevBuf<uint64_t> ck(r.nq * r.k, st);
+    DevBuf<uint32_t> cs(r.nq * r.k, st);
+    flat_candidates(p.q.get(), r.nq, rows.get(), n, dim, ip, r.k, nullptr, nullptr, ck.get(), cs.get(), st);
+    k_cols_to_slots<<<static_cast<unsigned>(ceil_div(r.nq * r.k, 256)), 256, 0, st>>>(cs.get(), r.nq * r.k, ds.get());
+    QG_LAUNCH_CHECK();
+    finalize_ivf(ck.get(), cs.get(), static_cast<int>(r.nq), static_cast<int>(r.k), static_cast<int>(r.k),
+                 o.dev.labels.get(), cosine, out_ids, out_d, st);
+}
+
 void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
     if (r.nq == 0) return;
     const bool empty_filter = r.filter && r.filter->count == 0;
@@ -212,7 +257,6 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
             fill_empty(r, st);
             return;
         }
-        require(r.filter == nullptr, "filtered queries on a bare IVFIndex are not on the GPU path yet", kUnsupported);
         ensure_device(o, st);
         Prepared p;
         prepare(idx, r, p, st);
@@ -226,7 +270,7 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
         a.k = static_cast<int>(r.k);
         a.kp = kp;
         a.nprobe = static_cast<int>(o.model.nprobe);
-        a.filter = nullptr;
+        filter_probing(a, o.model, r.filter, p.filter.get(), r.k);
         a.sm_count = sm_count_cached();
         a.d_err = p.err.get();
         ivf_candidates(o.dev.view, a, ck.get(), cs.get(), st);
@@ -266,20 +310,26 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
     ensure_device(o, st);
     Prepared p;
     prepare(idx, r, p, st);
+    // narrow filters through an IVF base: exact scores of the allowed rows
+    // (RefineIndex::use_direct / direct_scan, reference src/refine_index.cpp:59-82)
+    if (r.filter && o.base->kind == Kind::IVF && r.filter->count <= 6 * static_cast<IVFObj&>(*o.base).model.nlist) {
+        refine_direct(o, p, r, dim, ip, cosine, out_ids, out_d, st);
+        finish(p);
+        return;
+    }
     const size_t kp = std::min(r.k * o.k_factor, live);
     require(kp <= 3072, "k * k_factor above 3072 is not supported by the GPU path", kUnsupported);
     DevBuf<uint64_t> ck(r.nq * kp, st);
     DevBuf<uint32_t> cs(r.nq * kp, st);
     if (o.base->kind == Kind::IVF) {
         auto& b = static_cast<IVFObj&>(*o.base);
-        require(r.filter == nullptr, "filtered queries through an IVF base are not on the GPU path yet", kUnsupported);
         IvfSearchArgs a;
         a.q = p.q.get();
         a.nq = static_cast<int>(r.nq);
         a.k = static_cast<int>(r.k);
         a.kp = static_cast<int>(kp);
         a.nprobe = static_cast<int>(b.model.nprobe);
-        a.filter = p.filter.get();
+        filter_probing(a, b.model, r.filter, p.filter.get(), kp);
         a.sm_count = sm_count_cached();
         a.d_err = p.err.get();
         ivf_candidates(b.dev.view, a, ck.get(), cs.get(), st);

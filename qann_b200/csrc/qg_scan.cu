@@ -168,8 +168,15 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
     const int qi = blockIdx.x / a.nchunks;
     const int chunk = blockIdx.x - qi * a.nchunks;
     const int p0 = chunk * a.pch;
-    const int np = min(a.P, p0 + a.pch) - p0;
+    const int np = min(a.nprobe_q ? a.nprobe_q[qi] : a.P, p0 + a.pch) - p0;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (np <= 0) {   // a filtered query that stopped probing before this chunk
+        for (int i = tid; i < a.kp; i += NT) {
+            a.out_key[static_cast<size_t>(blockIdx.x) * a.kp + i] = ~0ull;
+            a.out_slot[static_cast<size_t>(blockIdx.x) * a.kp + i] = 0xFFFFFFFFu;
+        }
+        return;
+    }
     const int oct = lane >> 3, r = lane & 7;
     const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
     const int qtab_len = v.mode == kModeL2 ? v.m * 16 : (v.mode == kModeL2Adc ? v.dim : 0);
@@ -417,16 +424,24 @@ static void launch_scan(const ScanArgs& a, size_t smem, unsigned blocks, cudaStr
 }
 
 void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st) {
-    const int nq = s.nq, P = s.nprobe, kp = s.kp;
+    const int nq = s.nq, kp = s.kp;
     if (nq == 0) return;
-    // coarse: all pair scores, then the P nearest lists per query
-    DevBuf<float> scores(static_cast<size_t>(nq) * v.nlist, st);
-    pair_scores(s.q, nq, v.centroids, v.nlist, v.dim, v.ip_metric, scores.get(), v.nlist, st);
-    DevBuf<uint32_t> probe(static_cast<size_t>(nq) * P, st);
-    DevBuf<float> pdist(static_cast<size_t>(nq) * P, st);
-    // (score, list) compared as the reference's heap of (float, uint16_t) pairs does: -0 == +0
-    select_rows(scores.get(), v.nlist, nq, v.nlist, P, probe.get(), pdist.get(), st, nullptr, nullptr, 0, true);
-    scores.release();
+    int P = s.nprobe;
+    DevBuf<uint32_t> probe;
+    DevBuf<float> pdist;
+    DevBuf<int> nprobe_q;
+    if (s.filter) {
+        // every list ranked, then each query's own probe count (reference src/ivf_index.cpp:501-521)
+        P = filtered_probes(v, s, probe, pdist, nprobe_q, st);
+    } else {
+        // coarse: all pair scores, then the P nearest lists per query
+        DevBuf<float> scores(static_cast<size_t>(nq) * v.nlist, st);
+        pair_scores(s.q, nq, v.centroids, v.nlist, v.dim, v.ip_metric, scores.get(), v.nlist, st);
+        probe.alloc(static_cast<size_t>(nq) * P, st);
+        pdist.alloc(static_cast<size_t>(nq) * P, st);
+        // (score, list) compared as the reference's heap of (float, uint16_t) pairs does: -0 == +0
+        select_rows(scores.get(), v.nlist, nq, v.nlist, P, probe.get(), pdist.get(), st, nullptr, nullptr, 0, true);
+    }
 
     DevBuf<float> pterm(static_cast<size_t>(nq) * P, st);
     probe_terms(v, s.q, nq, P, probe.get(), pdist.get(), pterm.get(), st);
@@ -473,6 +488,7 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     a.qscale = qscale.get();
     a.qoffset = qoffset.get();
     a.filter = s.filter;
+    a.nprobe_q = nprobe_q.get();
     a.P = P;
     a.pch = pch;
     a.nchunks = nchunks;

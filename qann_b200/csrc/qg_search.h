@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include "qg_cuda.h"
+
 #include <cstddef>
 #include <cstdint>
 
@@ -44,6 +46,7 @@ struct ScanArgs {
     const float* qscale;
     const float* qoffset;
     const uint64_t* filter;  // allowed-slot bitmap, or null
+    const int* nprobe_q;     // per-query probe count (filtered queries), or null for P each
     int P, pch, nchunks, kp, cap;
     uint64_t* out_key;       // (nq * nchunks) * kp
     uint32_t* out_slot;
@@ -54,6 +57,9 @@ struct IvfSearchArgs {
     const float* q = nullptr;   // nq * dim, prepared (normalised for cosine)
     int nq = 0, k = 0, kp = 0, nprobe = 0;
     const uint64_t* filter = nullptr;
+    // filtered probing (reference src/ivf_index.cpp:501-521): probes run past
+    // nprobe to at least min_probes, then until `wanted` allowed vectors were seen
+    int min_probes = 0, wanted = 0;
     int sm_count = 0;
     int* d_err = nullptr;
 };
@@ -73,6 +79,11 @@ void probe_terms(const IvfView& v, const float* q, int nq, int P, const uint32_t
                  cudaStream_t st);
 void query_tables(const IvfView& v, const float* q, int nq, float* qC, uint4* qlut, float* qscale, float* qoffset,
                   cudaStream_t st);
+// Probe lists of filtered queries: every list ranked by (score, list), each
+// query's probe count (nprobe_q) from the filter's per-list allowed counts;
+// probe / pdist are nq x Pmax, and Pmax is returned.
+int filtered_probes(const IvfView& v, const IvfSearchArgs& s, DevBuf<uint32_t>& probe, DevBuf<float>& pdist,
+                    DevBuf<int>& nprobe_q, cudaStream_t st);
 // The k' = s.kp best candidates of each query, as sorted (key64, slot) lists
 // (key64 = key(dist) << 32 | push index; 0xFFFF... marks an empty entry).
 void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st);

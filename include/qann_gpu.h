@@ -169,6 +169,16 @@ int qg_exact_scores_dev(const float* a_dev, size_t na, const float* b_dev, size_
 int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, const uint8_t* codes_dev,
                              const uint32_t* lut_of_dev, size_t n, uint16_t* sums_dev, void* stream);
 
+/* --- host-side pieces of training (parity tests; no GPU needed) ------------------
+ * qg_symmetric_eigen: eigenvalues (d) and eigenvectors (d x d, as columns) of a
+ *   symmetric d x d matrix by cyclic Jacobi sweeps, bit-identical with the
+ *   reference's symmetric_eigen (reference src/rotation.cpp:20-69).
+ * qg_balanced_rotation: the PCA-balanced rotation (d x d, row-major) for m PQ
+ *   subspaces from a d x d covariance, as balanced_pca_rotation derives it
+ *   after its covariance step (reference src/rotation.cpp:106-130). */
+int qg_symmetric_eigen(const double* a, size_t d, double* values, double* vectors);
+int qg_balanced_rotation(const double* cov, size_t d, size_t m, float* rotation);
+
 #ifdef __cplusplus
 }
 #endif

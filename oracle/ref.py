@@ -86,6 +86,8 @@ def lib():
         L.ref_assign_nearest.argtypes = [f32p, sz, sz, f32p, sz, sz, vp]
         L.ref_pq_tables.argtypes = [f32p, sz, sz, sz, f32p, f32p, f32p, f32p, f32p]
         L.ref_pq_encode.argtypes = [f32p, sz, sz, sz, f32p, sz, vp]
+        L.ref_pca_rotation.argtypes = [f32p, sz, sz, sz, f32p]
+        L.ref_symmetric_eigen.argtypes = [vp, sz, vp, vp]
         _lib = L
     return _lib
 
@@ -373,3 +375,20 @@ def pq_encode(centroids, m, K, x):
     codes = np.empty((x.shape[0], m), np.uint8)
     _check(lib().ref_pq_encode(_ptr(cen), x.shape[1], m, K, _ptr(x), x.shape[0], _ptr(codes)))
     return codes
+
+
+def pca_rotation(x, m):
+    """balanced_pca_rotation (reference src/rotation.cpp:71-130): d x d, row-major."""
+    x = _f32(x)
+    out = np.empty((x.shape[1], x.shape[1]), np.float32)
+    _check(lib().ref_pca_rotation(_ptr(x), x.shape[0], x.shape[1], m, _ptr(out)))
+    return out
+
+
+def symmetric_eigen(a):
+    """symmetric_eigen (reference src/rotation.cpp:20-69): (values, vectors as columns)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    d = a.shape[0]
+    values, vectors = np.empty(d), np.empty((d, d))
+    _check(lib().ref_symmetric_eigen(_ptr(a), d, _ptr(values), _ptr(vectors)))
+    return values, vectors

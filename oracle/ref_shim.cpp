@@ -21,6 +21,7 @@
 #include "fast_scan.hpp"
 #include "kmeans.hpp"
 #include "topk.hpp"
+#include "rotation.hpp"
 
 #include <cmath>
 #include <cstdint>
@@ -294,6 +295,23 @@ int ref_pq_encode(const float* centroids, size_t dim, size_t m, size_t K, const 
         ss.write(reinterpret_cast<const char*>(centroids), static_cast<std::streamsize>(m * K * (dim / m) * 4));
         PQCodebook cb = PQCodebook::load(ss);
         for (size_t i = 0; i < n; ++i) cb.encode({x + i * dim, dim}, codes + i * m);
+    });
+}
+
+// PCA-balanced rotation (d x d, row-major) and the symmetric eigen-solver it uses.
+int ref_pca_rotation(const float* x, size_t n, size_t d, size_t m, float* out) {
+    return guarded([&] {
+        auto r = detail::balanced_pca_rotation({x, n * d}, n, d, m);
+        std::memcpy(out, r.data(), r.size() * sizeof(float));
+    });
+}
+
+int ref_symmetric_eigen(const double* a, size_t d, double* values, double* vectors) {
+    return guarded([&] {
+        std::vector<double> v, w;
+        detail::symmetric_eigen(std::vector<double>(a, a + d * d), d, v, w);
+        std::memcpy(values, v.data(), d * sizeof(double));
+        std::memcpy(vectors, w.data(), d * d * sizeof(double));
     });
 }
 

@@ -51,6 +51,8 @@ _SIGS = {
     "qg_fast_scan_dev": (C.c_int, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),
     "qg_exact_scores_dev": (C.c_int, [_vp, _sz, _vp, _sz, _sz, C.c_int, _vp, _vp]),
     "qg_fast_scan_noalloc_dev": (C.c_int, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),
+    "qg_symmetric_eigen": (C.c_int, [_vp, _sz, _vp, _vp]),
+    "qg_balanced_rotation": (C.c_int, [_vp, _sz, _sz, _vp]),
 }
 
 EXPORTS = tuple(_SIGS)

@@ -122,7 +122,6 @@ static void ivf_add_impl(IVFObj& o, const float* x_dev, size_t n, const int64_t*
     IVFModel& M = o.model;
     if (!M.trained) throw Error(kLogicError, "train() has not be run yet");
     require(M.has_pq && M.fast_scan, "the GPU build adds to IVF indexes with fast-scan PQ", kUnsupported);
-    require(!M.rotate, "IVF with a PCA rotation is not on the GPU path yet", kUnsupported);
     M.idmap.check(n, ids);
     const uint32_t first = static_cast<uint32_t>(M.idmap.slots());
     const int dim = static_cast<int>(M.dim), m = static_cast<int>(M.pq.m), sd = static_cast<int>(M.pq.sub_dim);
@@ -141,6 +140,15 @@ static void ivf_add_impl(IVFObj& o, const float* x_dev, size_t n, const int64_t*
         const std::vector<float> yt = M.pq.transposed();
         DevBuf<float> dyt(yt.size(), st);
         QG_CUDA(cudaMemcpyAsync(dyt.get(), yt.data(), dyt.bytes(), cudaMemcpyHostToDevice, st));
+        // a rotating index assigns and encodes the rotated rows (reference src/ivf_index.cpp:111-120)
+        DevBuf<float> xr;
+        if (M.rotate) {
+            DevBuf<float> R(M.rotation.size(), st);
+            QG_CUDA(cudaMemcpyAsync(R.get(), M.rotation.data(), R.bytes(), cudaMemcpyHostToDevice, st));
+            xr.alloc(n * dim, st);
+            rotate_rows(R.get(), x_dev, n, dim, xr.get(), st);
+            x_dev = xr.get();
+        }
         DevBuf<uint32_t> da(n, st);
         assign_nearest(x_dev, n, cent.get(), M.nlist, dim, da.get(), st);
         DevBuf<uint8_t> dc(n * m, st);

@@ -4,6 +4,7 @@
 
 #include "qg_device.cuh"
 #include "qg_ops.h"
+#include "qg_train.h"
 
 #include <limits>
 #include <string>
@@ -507,6 +508,25 @@ int qg_exact_scores_dev(const float* a_dev, size_t na, const float* b_dev, size_
     return guarded([&] {
         pair_scores(a_dev, static_cast<int>(na), b_dev, static_cast<int>(nb), static_cast<int>(dim), ip != 0, out_dev,
                     nb, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int qg_symmetric_eigen(const double* a, size_t d, double* values, double* vectors) {
+    return guarded([&] {
+        require(a && values && vectors, "null buffer");
+        std::vector<double> v, w;
+        symmetric_eigen(std::vector<double>(a, a + d * d), d, v, w);
+        std::copy(v.begin(), v.end(), values);
+        std::copy(w.begin(), w.end(), vectors);
+    });
+}
+
+int qg_balanced_rotation(const double* cov, size_t d, size_t m, float* rotation) {
+    return guarded([&] {
+        require(cov && rotation, "null buffer");
+        require(m > 0 && d % m == 0, "dim must be divisible by num_subspaces");
+        const std::vector<float> r = balanced_rotation(std::vector<double>(cov, cov + d * d), d, m);
+        std::copy(r.begin(), r.end(), rotation);
     });
 }
 

@@ -317,6 +317,18 @@ std::vector<float> PQCodebook::transposed() const {
     return t;
 }
 
+// Columns of R (d x d, row-major) orthonormal within 1e-3, dots in double
+// (reference src/rotation.cpp:132-143, the check load() makes).
+static bool rotation_orthonormal(const std::vector<float>& R, size_t d) {
+    for (size_t a = 0; a < d; ++a)
+        for (size_t b = a; b < d; ++b) {
+            double dot = 0.0;
+            for (size_t k = 0; k < d; ++k) dot += double(R[k * d + a]) * double(R[k * d + b]);
+            if (std::abs(dot - (a == b ? 1.0 : 0.0)) > 1e-3) return false;
+        }
+    return true;
+}
+
 static Metric read_metric(Reader& r) {
     const auto m = r.pod<uint8_t>();
     if (m > 2) Reader::throw_corrupt("unknown metric");
@@ -421,6 +433,8 @@ std::unique_ptr<IVFModel> IVFModel::load_body(Reader& r, uint32_t version) {
             m->rotation = r.vec<float>(m->dim * m->dim);
             if (m->rotation.size() != (rot && trained ? m->dim * m->dim : 0))
                 Reader::throw_corrupt("IVFIndex rotation length mismatch");
+            if (!m->rotation.empty() && !rotation_orthonormal(m->rotation, m->dim))
+                Reader::throw_corrupt("IVFIndex rotation is not orthogonal");
         }
     }
     if (version >= 7) {

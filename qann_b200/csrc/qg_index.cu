@@ -127,9 +127,9 @@ void ensure_device(IVFObj& o, cudaStream_t st) {
     require(M.trained, "train() has not be run yet", kLogicError);
     require(M.has_pq && M.fast_scan, "the GPU search path serves IVF indexes with fast-scan PQ (enable_pq(m, fast_scan=True))",
             kUnsupported);
-    require(!M.rotate, "IVF with a PCA rotation (enable_pq(rotate=True)) is not on the GPU search path yet", kUnsupported);
     DeviceIVF& D = o.dev;
     D = DeviceIVF{};
+    if (M.rotate) upload(D.rot, M.rotation, st);
     const int nlist = static_cast<int>(M.nlist), dim = static_cast<int>(M.dim), m = static_cast<int>(M.pq.m);
     const int m_pad = (m + 3) & ~3;
     upload(D.centroids, M.centroids, st);

@@ -16,6 +16,7 @@ namespace qg {
 struct DeviceIVF {
     IvfView view;
     DevBuf<float> centroids, resid, sqnorm, pq_t, B;
+    DevBuf<float> rot;        // dim x dim PCA rotation, when the index rotates
     DevBuf<uint32_t> sb_off, list_size, ids;
     DevBuf<uint4> codes;
     DevBuf<uint64_t> deleted;

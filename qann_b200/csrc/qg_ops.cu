@@ -159,6 +159,16 @@ static void prepare(IndexObj& idx, const SearchRequest& r, Prepared& p, cudaStre
     }
 }
 
+// IVF stages see rotated queries when the index rotates (reference
+// src/ivf_index.cpp:196-204); a RefineIndex re-ranks with the unrotated ones.
+static const float* ivf_queries(const IVFObj& o, const Prepared& p, size_t nq, DevBuf<float>& rot, cudaStream_t st) {
+    if (!o.model.rotate) return p.q.get();
+    const int dim = static_cast<int>(o.model.dim);
+    rot.alloc(nq * dim, st);
+    rotate_rows(o.dev.rot.get(), p.q.get(), nq, dim, rot.get(), st);
+    return rot.get();
+}
+
 static void fill_empty(const SearchRequest& r, cudaStream_t st) {
     const size_t n = r.nq * r.k;
     if (!n) return;
@@ -264,8 +274,9 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
         require(kp <= 3072, "k above 3072 is not supported by the GPU fast-scan", kUnsupported);
         DevBuf<uint64_t> ck(r.nq * kp, st);
         DevBuf<uint32_t> cs(r.nq * kp, st);
+        DevBuf<float> qrot;
         IvfSearchArgs a;
-        a.q = p.q.get();
+        a.q = ivf_queries(o, p, r.nq, qrot, st);
         a.nq = static_cast<int>(r.nq);
         a.k = static_cast<int>(r.k);
         a.kp = kp;
@@ -323,8 +334,9 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
     DevBuf<uint32_t> cs(r.nq * kp, st);
     if (o.base->kind == Kind::IVF) {
         auto& b = static_cast<IVFObj&>(*o.base);
+        DevBuf<float> qrot;
         IvfSearchArgs a;
-        a.q = p.q.get();
+        a.q = ivf_queries(b, p, r.nq, qrot, st);
         a.nq = static_cast<int>(r.nq);
         a.k = static_cast<int>(r.k);
         a.kp = static_cast<int>(kp);

@@ -458,6 +458,49 @@ void normalize_rows(const float* x, float* y, int n, int d, int* d_zero, cudaStr
     QG_LAUNCH_CHECK();
 }
 
+// Rows times an orthonormal rotation (reference src/rotation.cpp:165-187):
+// out[i][j] accumulates fma(x[i][k], R[k][j], acc) for k = 0..d-1 in order,
+// from +0. A block computes 32 rows x 32 columns, staging 32-deep slices of
+// the rows and of R in shared memory; each thread owns 4 rows of one column.
+__global__ void __launch_bounds__(256) k_rotate(const float* __restrict__ x, size_t n, int d,
+                                                const float* __restrict__ R, float* __restrict__ out) {
+    __shared__ float xs[32][33];
+    __shared__ float rs[32][32];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const size_t r0 = static_cast<size_t>(blockIdx.x) * 32;
+    const int c0 = blockIdx.y * 32;
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int k0 = 0; k0 < d; k0 += 32) {
+        for (int t = threadIdx.x; t < 32 * 32; t += 256) {
+            const int a = t >> 5, b = t & 31;
+            const size_t row = r0 + a;
+            xs[a][b] = row < n && k0 + b < d ? x[row * d + k0 + b] : 0.0f;
+            rs[a][b] = k0 + a < d && c0 + b < d ? R[static_cast<size_t>(k0 + a) * d + c0 + b] : 0.0f;
+        }
+        __syncthreads();
+        const int kn = min(32, d - k0);   // no padded terms: fma(0, r, -0) would turn -0 into +0
+        for (int kk = 0; kk < kn; ++kk) {
+            const float rv = rs[kk][tx];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i] = __fmaf_rn(xs[ty * 4 + i][kk], rv, acc[i]);
+        }
+        __syncthreads();
+    }
+    const int c = c0 + tx;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const size_t row = r0 + ty * 4 + i;
+        if (row < n && c < d) out[row * d + c] = acc[i];
+    }
+}
+
+void rotate_rows(const float* R, const float* x, size_t n, int d, float* out, cudaStream_t st) {
+    if (n == 0) return;
+    const dim3 grid(static_cast<unsigned>(ceil_div(n, 32)), static_cast<unsigned>(ceil_div(d, 32)));
+    k_rotate<<<grid, 256, 0, st>>>(x, n, d, R, out);
+    QG_LAUNCH_CHECK();
+}
+
 
 void probe_terms(const IvfView& v, const float* q, int nq, int P, const uint32_t* probe, const float* pdist, float* term,
                  cudaStream_t st) {

@@ -65,6 +65,8 @@ struct IvfSearchArgs {
 };
 
 void normalize_rows(const float* x, float* y, int n, int d, int* d_zero, cudaStream_t st);
+// out = x R for n rows of d (R: d x d row-major), in the reference's FMA order.
+void rotate_rows(const float* R, const float* x, size_t n, int d, float* out, cudaStream_t st);
 void pair_scores(const float* A, int na, const float* B, int nb, int d, bool ip, float* out, size_t ld_out,
                  cudaStream_t st);
 // The P smallest scores of each row by (key, column), sorted; refused columns

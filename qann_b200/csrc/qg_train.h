@@ -35,7 +35,18 @@ void residuals(const float* x, size_t n, int d, const float* centers, const uint
 // out[p][i][0..d) = x[i][p*d .. (p+1)*d): the subspace columns, problem-major
 void split_columns(const float* x, size_t n, int dim, int d, int P, float* out, cudaStream_t st);
 
-// ---- host algorithms (qg_train_host.cpp) ----------------------------------------
+// The sample covariance of n rows (reference src/rotation.cpp:77-104): column
+// means summed in double in row order, then cov[p][q] (p <= q) accumulated as
+// fma(x[p] - mean[p], x[q] - mean[q], cov) over the rows in order, scaled by
+// 1 / (n - 1) (1 for n = 1) and mirrored. Returned on the host, d x d.
+std::vector<double> covariance(const float* x, size_t n, int d, cudaStream_t st);
+
+// ---- host algorithms (qg_train_host.cpp, qg_rotation.cpp) -----------------------
+
+// Jacobi eigen-decomposition of a symmetric d x d matrix (eigenvectors as columns).
+void symmetric_eigen(std::vector<double> a, size_t d, std::vector<double>& values, std::vector<double>& vectors);
+// The PCA-balanced rotation (d x d, row-major) for m subspaces from a covariance.
+std::vector<float> balanced_rotation(std::vector<double> cov, size_t d, size_t m);
 
 struct KMeansOut {
     std::vector<float> centroids;   // P * k * d

@@ -524,7 +524,6 @@ void train(IVFObj& o, const float* x, size_t n, size_t max_iters, int64_t seed_i
     if (M.idmap.slots() > 0) throw Error(kLogicError, "train() cannot be called after add()");
     if (M.trained) throw Error(kLogicError, "train() has already been called");
     if (n < M.nlist) throw Error(kInvalidArgument, "training set must have at least nlist vectors");
-    require(!M.rotate, "IVF with a PCA rotation (enable_pq(rotate=True)) is not on the GPU path yet", kUnsupported);
     require(M.sq_bits == 0, "SQ lists are not on the GPU path", kUnsupported);
     require(!M.has_pq || M.pq.K <= 256, "PQ needs at most 256 centroids per subspace");
     const std::optional<uint32_t> seed = seed_in >= 0 ? std::optional<uint32_t>(static_cast<uint32_t>(seed_in))
@@ -547,6 +546,18 @@ void train(IVFObj& o, const float* x, size_t n, size_t max_iters, int64_t seed_i
         }
     }
     const int k = static_cast<int>(M.nlist), d = static_cast<int>(dim);
+    // learn the rotation, then cluster and train the codebook on the rotated
+    // rows (reference src/ivf_index.cpp:738-745, src/rotation.cpp:71-130)
+    std::vector<float> rotation;
+    if (M.rotate) {
+        if (M.pq.m == 0 || dim % M.pq.m != 0) throw Error(kInvalidArgument, "dim must be divisible by num_subspaces");
+        rotation = balanced_rotation(covariance(xd.get(), n, d, st), dim, M.pq.m);
+        DevBuf<float> R(rotation.size(), st), xr(n * dim, st);
+        h2d(R.get(), rotation.data(), rotation.size(), st);
+        rotate_rows(R.get(), xd.get(), n, d, xr.get(), st);
+        QG_CUDA(cudaStreamSynchronize(st));
+        xd = std::move(xr);
+    }
     KMeansOut res = clustering == 0 ? emeans(xd.get(), n, d, k, passes, seed, cosine, st)
                                     : kmeans_lloyd(xd.get(), n, d, k, max_iters, {seed}, cosine, 1, st);
     std::vector<float> centroids = std::move(res.centroids);
@@ -624,6 +635,7 @@ void train(IVFObj& o, const float* x, size_t n, size_t max_iters, int64_t seed_i
         }
     }
     M.centroids = std::move(centroids);
+    M.rotation = std::move(rotation);
     M.residual_centers = std::move(residual_centers);
     M.cosine_ip = cosine_ip;
     M.trained = true;

@@ -20,23 +20,27 @@ def clustered(seed, n, d, centres=30, sigma=0.2):
 
 
 CASES = [
-    # metric, clustering, d, m, nlist
-    (0, 0, 32, 16, 100),
-    (0, 1, 32, 16, 100),
-    (1, 0, 32, 16, 100),
-    (1, 1, 24, 12, 120),
-    (2, 0, 16, 8, 100),
-    (0, 0, 100, 50, 128),
+    # metric, clustering, d, m, nlist, PCA rotation
+    (0, 0, 32, 16, 100, False),
+    (0, 1, 32, 16, 100, False),
+    (1, 0, 32, 16, 100, False),
+    (1, 1, 24, 12, 120, False),
+    (2, 0, 16, 8, 100, False),
+    (0, 0, 100, 50, 128, False),
+    (0, 0, 32, 16, 100, True),
+    (1, 1, 24, 12, 120, True),
+    (2, 0, 16, 8, 100, True),
+    (1, 0, 100, 50, 128, True),
 ]
 
 
-@pytest.mark.parametrize("metric,clustering,d,m,nlist", CASES)
-def test_train_add_save_byte_identical(ref, tmp_path, metric, clustering, d, m, nlist):
+@pytest.mark.parametrize("metric,clustering,d,m,nlist,rotate", CASES)
+def test_train_add_save_byte_identical(ref, tmp_path, metric, clustering, d, m, nlist, rotate):
     x = clustered(metric * 10 + clustering + d, 6000, d)
     mine = qb.IVFIndex(d, nlist, 8, metric=qb.Metric(metric))
     theirs = ref.IVFIndex(d, nlist, 8, metric=metric)
     for idx in (mine, theirs):
-        idx.enable_pq(m, fast_scan=True)
+        idx.enable_pq(m, fast_scan=True, rotate=rotate)
         idx.train(x, max_iters=6, seed=11, clustering=clustering, passes=2)
     r_mine, r_theirs = qb.RefineIndex(mine, 4), ref.RefineIndex(theirs, 4)
     r_mine.add(x[:4000])

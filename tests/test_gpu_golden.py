@@ -16,6 +16,7 @@ REF_FS = [
     ("v4_ivf_fs", "v4_queries"),
     ("v11_ivf_cos_fs", "v11_cos_queries"),
     ("v12_ivf_cos_l2", "v12_cos_queries"),
+    ("v9_ip_refine_ivf_fs", "v9_ip_queries"),   # RefineIndex over rotated fast-scan IVF-PQ
 ]
 REF_FLAT = [("v1_flat", "v1_queries"), ("v2_flat", "v2_queries"), ("v3_flat", "v3_queries"),
             ("v4_flat", "v4_queries"), ("v5_flat", "v5_queries"), ("v9_ip_flat", "v9_ip_queries")]

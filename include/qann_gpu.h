@@ -169,6 +169,40 @@ int qg_exact_scores_dev(const float* a_dev, size_t na, const float* b_dev, size_
 int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, const uint8_t* codes_dev,
                              const uint32_t* lut_of_dev, size_t n, uint16_t* sums_dev, void* stream);
 
+/* --- serving (no counterpart in the reference, whose query_batch answers one
+ * call on the calling threads, reference bindings/python_bindings.cpp:600-648) ----
+ * A server keeps the index on the device and runs requests with continuous
+ * batching: `slots` worker threads, each with its own CUDA stream, take the
+ * oldest waiting requests as soon as they are free (at most max_batch at a
+ * time, and only while the estimated device memory of all batches in flight
+ * stays within mem_budget_bytes; 0 = 2 GiB) and search them as one mixed batch.
+ * Each request has its own k, nprobe (<= 0: the index's) and filter, and gets
+ * the results it gets searched alone (qg_search with that nprobe set).
+ *
+ * qg_server_add_filter registers a slot bitmap (deleted slots are masked out)
+ *   that requests then name by filter_id.
+ * qg_server_submit queues one query (dim floats); its filter is `allowed`
+ *   (n_allowed ids, as qg_search) when non-NULL, else filter_id (-1 = none).
+ * qg_server_wait blocks for a ticket's k results and its latency (submission
+ *   to completion, microseconds); each ticket is waited for once.
+ * qg_server_replay runs an open-loop arrival trace: request i is submitted at
+ *   arrival_us[i] after the call starts, whatever the state of the others, with
+ *   k[i], nprobe[i] (NULL = the index's) and filter_id[i] (NULL or -1 = none);
+ *   results are nq x kmax (padded), latency_us[i] from its arrival time.
+ * qg_server_free stops the workers (requests still queued fail); no other call
+ *   on the server may be in progress. The server keeps its index alive. */
+typedef struct qg_server qg_server;
+int qg_server_create(qg_index* h, int slots, int max_batch, size_t mem_budget_bytes, qg_server** out);
+int qg_server_add_filter(qg_server* s, const uint64_t* words, size_t nwords, int* filter_id);
+int qg_server_submit(qg_server* s, const float* q, size_t k, int nprobe, const int64_t* allowed, size_t n_allowed,
+                     int filter_id, uint64_t* ticket);
+int qg_server_wait(qg_server* s, uint64_t ticket, int64_t* out_ids, float* out_dists, double* latency_us);
+int qg_server_replay(qg_server* s, const float* q, size_t nq, const int32_t* k, const int32_t* nprobe,
+                     const int32_t* filter_id, const double* arrival_us, size_t kmax, int64_t* out_ids,
+                     float* out_dists, double* latency_us);
+int qg_server_stats(qg_server* s, int64_t* completed, int64_t* batches, int64_t* peak_bytes);
+void qg_server_free(qg_server* s);
+
 /* --- host-side pieces of training (parity tests; no GPU needed) ------------------
  * qg_symmetric_eigen: eigenvalues (d) and eigenvectors (d x d, as columns) of a
  *   symmetric d x d matrix by cyclic Jacobi sweeps, bit-identical with the

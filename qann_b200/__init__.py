@@ -303,3 +303,91 @@ def load(path, *, mmap=False):
 
 
 Index = DenseIndex
+
+
+class Server:
+    """Continuous-batching server over one device-resident index.
+
+    Requests carry their own k, nprobe and filter; worker slots (one CUDA
+    stream each) take the oldest waiting requests as soon as they are free,
+    up to max_batch at a time while the estimated device memory of all
+    batches in flight fits mem_budget bytes, and search each batch as one
+    mixed batch. Every request gets the results it gets searched alone.
+    """
+
+    def __init__(self, index: DenseIndex, *, slots: int = 4, max_batch: int = 512, mem_budget: int = 2 << 30):
+        self._index = index
+        self._dim = index.dim()
+        h = C.c_void_p()
+        check(_lib.lib.qg_server_create(index._h, int(slots), int(max_batch), int(mem_budget), C.byref(h)))
+        self._s = h
+        self._k = {}
+
+    def close(self) -> None:
+        s = getattr(self, "_s", None)
+        if s is not None and s.value:
+            _lib.lib.qg_server_free(s)
+            self._s = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add_filter(self, words) -> int:
+        """Registers an allowed-slot bitmap (uint64 words); returns its filter id."""
+        w = np.ascontiguousarray(words, dtype=np.uint64)
+        fid = C.c_int()
+        check(_lib.lib.qg_server_add_filter(self._s, w.ctypes.data, w.size, C.byref(fid)))
+        return fid.value
+
+    def submit(self, query, k: int, *, nprobe: int | None = None, allowed=None, filter_id: int = -1) -> int:
+        """Queues one query; returns a ticket for result()."""
+        q = _f32_rows(np.asarray(query, np.float32).reshape(1, -1), self._dim, "query")
+        t = C.c_uint64()
+        np_ = 0 if nprobe is None else int(nprobe)
+        if allowed is not None:
+            al = _ids(allowed)
+            check(_lib.lib.qg_server_submit(self._s, q.ctypes.data, int(k), np_, al.ctypes.data, al.size, -1,
+                                            C.byref(t)))
+        else:
+            check(_lib.lib.qg_server_submit(self._s, q.ctypes.data, int(k), np_, None, 0, int(filter_id), C.byref(t)))
+        self._k[t.value] = int(k)
+        return t.value
+
+    def result(self, ticket: int):
+        """(ids int64 (k,), distances float32 (k,), latency in seconds) of a ticket."""
+        k = self._k.pop(ticket)
+        ids = np.empty(k, np.int64)
+        d = np.empty(k, np.float32)
+        lat = C.c_double()
+        check(_lib.lib.qg_server_wait(self._s, C.c_uint64(ticket), ids.ctypes.data, d.ctypes.data, C.byref(lat)))
+        return ids, d, lat.value * 1e-6
+
+    def replay(self, queries, ks, arrivals_s, *, nprobes=None, filter_ids=None):
+        """Open-loop trace: request i arrives arrivals_s[i] seconds after the
+        start with k = ks[i]. Returns (ids (nq, max k), distances, latencies s)."""
+        q = _f32_rows(queries, self._dim, "query")
+        nq = q.shape[0]
+        ks = np.ascontiguousarray(ks, dtype=np.int32)
+        kmax = int(ks.max()) if nq else 1
+        arr = np.ascontiguousarray(np.asarray(arrivals_s, np.float64) * 1e6)
+        npb = None if nprobes is None else np.ascontiguousarray(nprobes, dtype=np.int32)
+        fid = None if filter_ids is None else np.ascontiguousarray(filter_ids, dtype=np.int32)
+        ids = np.empty((nq, kmax), np.int64)
+        d = np.empty((nq, kmax), np.float32)
+        lat = np.empty(nq, np.float64)
+        check(_lib.lib.qg_server_replay(self._s, q.ctypes.data, nq, ks.ctypes.data,
+                                        None if npb is None else npb.ctypes.data,
+                                        None if fid is None else fid.ctypes.data, arr.ctypes.data, kmax,
+                                        ids.ctypes.data, d.ctypes.data, lat.ctypes.data))
+        return ids, d, lat * 1e-6
+
+    def stats(self) -> dict:
+        c, b, p = C.c_int64(), C.c_int64(), C.c_int64()
+        check(_lib.lib.qg_server_stats(self._s, C.byref(c), C.byref(b), C.byref(p)))
+        return {"completed": c.value, "batches": b.value, "peak_in_flight_bytes": p.value}

@@ -51,6 +51,13 @@ _SIGS = {
     "qg_fast_scan_dev": (C.c_int, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),
     "qg_exact_scores_dev": (C.c_int, [_vp, _sz, _vp, _sz, _sz, C.c_int, _vp, _vp]),
     "qg_fast_scan_noalloc_dev": (C.c_int, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),
+    "qg_server_create": (C.c_int, [_vp, C.c_int, C.c_int, _sz, C.POINTER(_vp)]),
+    "qg_server_add_filter": (C.c_int, [_vp, _vp, _sz, C.POINTER(C.c_int)]),
+    "qg_server_submit": (C.c_int, [_vp, _vp, _sz, C.c_int, _vp, _sz, C.c_int, C.POINTER(C.c_uint64)]),
+    "qg_server_wait": (C.c_int, [_vp, C.c_uint64, _vp, _vp, C.POINTER(C.c_double)]),
+    "qg_server_replay": (C.c_int, [_vp, _vp, _sz, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp]),
+    "qg_server_stats": (C.c_int, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
+    "qg_server_free": (None, [_vp]),
     "qg_symmetric_eigen": (C.c_int, [_vp, _sz, _vp, _vp]),
     "qg_balanced_rotation": (C.c_int, [_vp, _sz, _sz, _vp]),
 }

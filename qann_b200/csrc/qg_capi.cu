@@ -11,9 +11,7 @@
 
 using namespace qg;
 
-struct qg_index {
-    std::shared_ptr<IndexObj> obj;
-};
+// (struct qg_index is defined in qg_ops.h)
 
 namespace {
 
@@ -36,10 +34,12 @@ int guarded(F&& f) {
     }
 }
 
+} // namespace
+
 // The stream-ordered allocator's default pool hands memory back to the driver
 // at every synchronisation (release threshold 0), so each search would pay for
 // fresh allocations; keep freed blocks cached in the pool instead.
-void keep_pool_memory() {
+void qg::keep_pool_memory() {
     static std::once_flag once;
     std::call_once(once, [] {
         int dev = 0;
@@ -50,6 +50,8 @@ void keep_pool_memory() {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     });
 }
+
+namespace {
 
 // One non-blocking stream per host thread, so concurrent searches overlap.
 cudaStream_t thread_stream() {

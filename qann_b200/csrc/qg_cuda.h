@@ -109,6 +109,23 @@ inline int sm_count() {
 }
 
 // Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync on one stream).
+// Lets a kernel take the device's opt-in maximum of dynamic shared memory.
+// Set once per kernel and never lowered: the attribute is process-wide, so a
+// per-launch value set by one thread could undercut another thread's launch.
+template <auto Kernel>
+void allow_large_smem() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int dev = 0, optin = 0;
+        QG_CUDA(cudaGetDevice(&dev));
+        QG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        cudaFuncAttributes fa{};
+        QG_CUDA(cudaFuncGetAttributes(&fa, Kernel));   // dynamic + static must fit the opt-in limit
+        QG_CUDA(cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     optin - static_cast<int>(fa.sharedSizeBytes)));
+    });
+}
+
 template <class T>
 struct DevBuf {
     T* ptr = nullptr;
@@ -137,7 +154,8 @@ struct DevBuf {
         if (n) QG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), s));
     }
     void release() noexcept {
-        if (ptr) cudaFreeAsync(ptr, stream);
+        // a failed free must not surface later as some launch's error
+        if (ptr && cudaFreeAsync(ptr, stream) != cudaSuccess) (void)cudaGetLastError();
         ptr = nullptr;
         count = 0;
     }

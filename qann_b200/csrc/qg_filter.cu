@@ -4,7 +4,9 @@
 // nearest first, until it has seen `wanted` allowed vectors. The reference
 // stops on its TopK's size, which before the first trim (at 2k pushes) counts
 // exactly the allowed vectors scanned; so the probe count of each query is the
-// first p >= min_probes whose lists hold >= wanted allowed vectors.
+// first p >= min_probes whose lists hold >= wanted allowed vectors. Each query
+// may carry its own filter (a mixed batch of served requests); the walk reads
+// only the ids of the lists the query goes on to scan.
 #include "qg_device.cuh"
 #include "qg_search.h"
 
@@ -28,35 +30,43 @@ __global__ void __launch_bounds__(256) k_rank_lists(const float* __restrict__ sc
     }
 }
 
-// warp per list: allowed (filter bit set) vectors of the list
-__global__ void k_list_allowed(IvfView v, const uint64_t* __restrict__ filter, uint32_t* __restrict__ cnt) {
-    const int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// warp per query: its probe count. A query with a filter walks its lists
+// nearest first, counting each list's allowed vectors, and stops at the first
+// p >= min_probes with >= wanted seen (the reference stops on its TopK's size,
+// which before the first trim counts exactly the allowed vectors scanned). A
+// query without one probes its own nprobe.
+__global__ void k_probe_walk(IvfView v, const uint32_t* __restrict__ ranked, int nq, const uint64_t* filter,
+                             const uint64_t* const* filters, int min_probes, int wanted, const int* __restrict__ min_q,
+                             const int* __restrict__ wanted_q, int nprobe, const int* __restrict__ nprobe_q,
+                             int* __restrict__ out) {
+    const int q = static_cast<int>((static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
-    if (l >= v.nlist) return;
-    const size_t b0 = static_cast<size_t>(v.sb_off[l]) * kSuperBlock;
-    const uint32_t n = v.list_size[l];
-    uint32_t c = 0;
-    for (uint32_t j = lane; j < n; j += 32) {
-        const uint32_t slot = v.ids[b0 + j];
-        c += (filter[slot >> 6] >> (slot & 63)) & 1ull;
-    }
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if (lane == 0) cnt[l] = c;
-}
-
-// thread per query: the probe count
-__global__ void k_probe_count(const uint32_t* __restrict__ ranked, const uint32_t* __restrict__ cnt, int nq, int nlist,
-                              int min_probes, int wanted, int* __restrict__ out) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
+    const int nlist = v.nlist;
+    const uint64_t* f = filters ? filters[q] : filter;
+    if (!f) {
+        if (lane == 0) out[q] = min(nprobe_q ? nprobe_q[q] : nprobe, nlist);
+        return;
+    }
+    const int mp = min_q ? min_q[q] : min_probes;
+    const long long want = wanted_q ? wanted_q[q] : wanted;
     const uint32_t* r = ranked + static_cast<size_t>(q) * nlist;
     long long seen = 0;
     int p = 0;
     for (; p < nlist; ++p) {
-        if (p >= min_probes && seen >= wanted) break;
-        seen += cnt[r[p]];
+        if (p >= mp && seen >= want) break;
+        const uint32_t l = r[p];
+        const size_t b0 = static_cast<size_t>(v.sb_off[l]) * kSuperBlock;
+        const uint32_t n = v.list_size[l];
+        uint32_t c = 0;
+        for (uint32_t j = lane; j < n; j += 32) {
+            const uint32_t slot = v.ids[b0 + j];
+            if (slot != 0xFFFFFFFFu) c += (f[slot >> 6] >> (slot & 63)) & 1ull;
+        }
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        seen += c;
     }
-    out[q] = p;
+    if (lane == 0) out[q] = p;
 }
 
 __global__ void k_take_columns(const uint32_t* __restrict__ list_in, const float* __restrict__ score_in, int nq,
@@ -80,20 +90,17 @@ int filtered_probes(const IvfView& v, const IvfSearchArgs& s, DevBuf<uint32_t>& 
     DevBuf<uint32_t> ranked(static_cast<size_t>(nq) * nlist, st);
     DevBuf<float> rscore(static_cast<size_t>(nq) * nlist, st);
     if (smem > 48 * 1024)
-        QG_CUDA(cudaFuncSetAttribute(k_rank_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        allow_large_smem<k_rank_lists>();
     {
         KernelTimer kt("rank_lists", st);
         k_rank_lists<<<nq, 256, smem, st>>>(scores.get(), nlist, npow, ranked.get(), rscore.get());
         QG_LAUNCH_CHECK();
     }
     scores.release();
-    DevBuf<uint32_t> cnt(nlist, st);
-    k_list_allowed<<<static_cast<unsigned>(ceil_div(static_cast<size_t>(nlist) * 32, 256)), 256, 0, st>>>(v, s.filter,
-                                                                                                    cnt.get());
-    QG_LAUNCH_CHECK();
     nprobe_q.alloc(nq, st);
-    k_probe_count<<<static_cast<unsigned>(ceil_div(nq, 128)), 128, 0, st>>>(ranked.get(), cnt.get(), nq, nlist,
-                                                                            s.min_probes, s.wanted, nprobe_q.get());
+    k_probe_walk<<<static_cast<unsigned>(ceil_div(static_cast<size_t>(nq) * 32, 256)), 256, 0, st>>>(
+        v, ranked.get(), nq, s.filter, s.pq.filter, s.min_probes, s.wanted, s.pq.min_probes, s.pq.wanted, s.nprobe,
+        s.pq.nprobe, nprobe_q.get());
     QG_LAUNCH_CHECK();
     std::vector<int> h(nq);
     QG_CUDA(cudaMemcpyAsync(h.data(), nprobe_q.get(), nq * sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -120,7 +120,24 @@ int IVFObj::scan_mode() const {
     return precomputed_available() ? kModeL2 : kModeL2Adc;
 }
 
-void ensure_device(IVFObj& o, cudaStream_t st) {
+// Index-resident arrays are built (and later freed) on a stream the library
+// never destroys: a DevBuf is freed on the stream it was made on, and the
+// caller's stream (a server worker's, say) may be gone by the time the index
+// is rebuilt or dropped. Builds finish before they return, so the caller's
+// stream sees the arrays; they are dropped only when no search is in flight.
+cudaStream_t resident_stream() {
+    static std::mutex mu;
+    static cudaStream_t streams[64] = {};
+    int dev = 0;
+    QG_CUDA(cudaGetDevice(&dev));
+    require(dev >= 0 && dev < 64, "device ordinal out of range", kCudaError);
+    std::lock_guard<std::mutex> g(mu);
+    if (!streams[dev]) QG_CUDA(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking));
+    return streams[dev];
+}
+
+void ensure_device(IVFObj& o, cudaStream_t) {
+    const cudaStream_t st = resident_stream();
     std::lock_guard<std::mutex> g(o.dev_mu);
     if (!o.dev_dirty) return;
     const IVFModel& M = o.model;
@@ -212,10 +229,10 @@ static void upload_rows(DeviceRows& D, const std::vector<float>& rows, const IdM
     QG_CUDA(cudaStreamSynchronize(st));
 }
 
-void ensure_device(FlatObj& o, cudaStream_t st) {
+void ensure_device(FlatObj& o, cudaStream_t) {
     std::lock_guard<std::mutex> g(o.dev_mu);
     if (!o.dev_dirty) return;
-    upload_rows(o.dev, o.model.data, o.model.idmap, st);
+    upload_rows(o.dev, o.model.data, o.model.idmap, resident_stream());
     o.dev_dirty = false;
 }
 
@@ -223,7 +240,7 @@ void ensure_device(RefineObj& o, cudaStream_t st) {
     {
         std::lock_guard<std::mutex> g(o.dev_mu);
         if (o.dev_dirty) {
-            upload_rows(o.dev, o.data, o.map, st);
+            upload_rows(o.dev, o.data, o.map, resident_stream());
             o.dev_dirty = false;
         }
     }

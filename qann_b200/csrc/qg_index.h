@@ -85,7 +85,11 @@ struct RefineObj : IndexObj {
     const IdMap& idmap() const override { return map; }
 };
 
-// Builds / refreshes the device copy (callers hold the object's lock).
+// The library's own stream on the current device (never destroyed).
+cudaStream_t resident_stream();
+
+// Builds / refreshes the device copy (callers hold the object's lock). The
+// arrays are made on resident_stream() and ready when this returns.
 void ensure_device(IVFObj& o, cudaStream_t st);
 void ensure_device(FlatObj& o, cudaStream_t st);
 void ensure_device(RefineObj& o, cudaStream_t st);

@@ -128,8 +128,7 @@ extern "C" int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, si
             std::max<size_t>(1, std::min<size_t>(16, (96 * 1024) / (static_cast<size_t>(m_pad) * 16))));
         const size_t smem = static_cast<size_t>(opb) * m_pad * 16;
         if (smem > 48 * 1024)
-            QG_CUDA(cudaFuncSetAttribute(k_noalloc_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem)));
+            allow_large_smem<k_noalloc_sums>();
         k_noalloc_sums<<<static_cast<unsigned>(ceil_div(nsb, opb)), 8 * opb, smem, st>>>(
             packed, nsb, reinterpret_cast<const uint4*>(lut_dev), mi, m_pad, lut_of_dev, n, sums_dev);
         QG_LAUNCH_CHECK();

@@ -78,7 +78,7 @@ void flat_candidates(const float* q_dev, size_t nq, const float* rows_dev, size_
     const int msm_n = next_pow2(static_cast<int>(2 * k));
     const size_t msm = static_cast<size_t>(msm_n) * 16;
     if (msm > 48 * 1024)
-        QG_CUDA(cudaFuncSetAttribute(k_merge2, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm)));
+        allow_large_smem<k_merge2>();
     for (size_t q0 = 0; q0 < nq; q0 += QB) {
         const size_t nb = std::min(QB, nq - q0);
         for (size_t r0 = 0; r0 < n; r0 += T) {
@@ -194,17 +194,17 @@ static void check_err(const DevBuf<int>& err, cudaStream_t st) {
 
 // Filtered probing of an IVF index (reference src/ivf_index.cpp:501-521): at
 // least min_probes lists, then on until `wanted` allowed vectors were seen.
+static size_t min_probes_for(const IVFModel& M, size_t nprobe, size_t count) {
+    if (!M.filter_probe_scaling || count == 0) return nprobe;
+    const double want = std::ceil(0.75 * double(nprobe) * std::cbrt(double(M.idmap.live_count()) / double(count)));
+    return std::clamp<size_t>(static_cast<size_t>(std::min(want, double(M.nlist))), nprobe, M.nlist);
+}
+
 static void filter_probing(IvfSearchArgs& a, const IVFModel& M, const SlotBits* f, const uint64_t* f_dev, size_t k) {
     if (!f) return;
     a.filter = f_dev;
     a.wanted = static_cast<int>(std::min(k, f->count));
-    size_t min_probes = M.nprobe;
-    if (M.filter_probe_scaling && f->count > 0) {
-        const double want =
-            std::ceil(0.75 * double(M.nprobe) * std::cbrt(double(M.idmap.live_count()) / double(f->count)));
-        min_probes = std::clamp<size_t>(static_cast<size_t>(std::min(want, double(M.nlist))), M.nprobe, M.nlist);
-    }
-    a.min_probes = static_cast<int>(min_probes);
+    a.min_probes = static_cast<int>(min_probes_for(M, static_cast<size_t>(a.nprobe), f->count));
 }
 
 __global__ void k_cols_to_slots(uint32_t* __restrict__ cs, size_t n, const uint32_t* __restrict__ slots) {
@@ -280,7 +280,7 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
         a.nq = static_cast<int>(r.nq);
         a.k = static_cast<int>(r.k);
         a.kp = kp;
-        a.nprobe = static_cast<int>(o.model.nprobe);
+        a.nprobe = r.nprobe > 0 ? r.nprobe : static_cast<int>(o.model.nprobe);
         filter_probing(a, o.model, r.filter, p.filter.get(), r.k);
         a.sm_count = sm_count_cached();
         a.d_err = p.err.get();
@@ -340,7 +340,7 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
         a.nq = static_cast<int>(r.nq);
         a.k = static_cast<int>(r.k);
         a.kp = static_cast<int>(kp);
-        a.nprobe = static_cast<int>(b.model.nprobe);
+        a.nprobe = r.nprobe > 0 ? r.nprobe : static_cast<int>(b.model.nprobe);
         filter_probing(a, b.model, r.filter, p.filter.get(), kp);
         a.sm_count = sm_count_cached();
         a.d_err = p.err.get();
@@ -353,6 +353,153 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
     refine_candidates(p.q.get(), static_cast<int>(r.nq), dim, o.dev.rows.get(), ck.get(), cs.get(), static_cast<int>(kp),
                       static_cast<int>(r.k), ip, o.dev.labels.get(), cosine, out_ids, out_d, st);
     finish(p);
+}
+
+// ---------------------------------------------------------------------------
+// Mixed batches (served requests with their own k, nprobe and filter)
+// ---------------------------------------------------------------------------
+void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs, size_t kmax, int64_t* out_ids,
+                  float* out_d, cudaStream_t st) {
+    std::fill(out_ids, out_ids + nq * kmax, int64_t{-1});
+    std::fill(out_d, out_d + nq * kmax, std::numeric_limits<float>::infinity());
+    if (nq == 0 || kmax == 0) return;
+    const size_t dim = idx.dim();
+    for (size_t i = 0; i < nq; ++i) require(qs[i].k >= 1 && static_cast<size_t>(qs[i].k) <= kmax, "k out of range");
+
+    // one request on its own (indexes without an IVF, and RefineIndex direct scans)
+    std::vector<int64_t> one_ids(kmax);
+    std::vector<float> one_d(kmax);
+    auto alone = [&](size_t i) {
+        SearchRequest r;
+        r.q = q + i * dim;
+        r.nq = 1;
+        r.k = static_cast<size_t>(qs[i].k);
+        r.filter = qs[i].filter;
+        r.out_ids = one_ids.data();
+        r.out_d = one_d.data();
+        r.nprobe = qs[i].nprobe;
+        search(idx, r, st);
+        std::copy_n(one_ids.data(), r.k, out_ids + i * kmax);
+        std::copy_n(one_d.data(), r.k, out_d + i * kmax);
+    };
+    IVFObj* ivf = nullptr;
+    RefineObj* ref = nullptr;
+    if (idx.kind == Kind::IVF) {
+        ivf = static_cast<IVFObj*>(&idx);
+    } else if (idx.kind == Kind::Refine && static_cast<RefineObj&>(idx).base->kind == Kind::IVF) {
+        ref = static_cast<RefineObj*>(&idx);
+        ivf = static_cast<IVFObj*>(ref->base.get());
+    }
+    if (!ivf) {
+        for (size_t i = 0; i < nq; ++i) alone(i);
+        return;
+    }
+    const IVFModel& M = ivf->model;
+    const size_t live = idx.idmap().live_count();
+    std::vector<size_t> batch;
+    for (size_t i = 0; i < nq; ++i) {
+        const SlotBits* f = qs[i].filter;
+        if (live == 0 || (f && f->count == 0)) continue;                      // nothing to return
+        if (ref && f && f->count <= 6 * M.nlist) {                             // RefineIndex::use_direct
+            alone(i);
+            continue;
+        }
+        batch.push_back(i);
+    }
+    if (batch.empty()) return;
+    if (ref) ensure_device(*ref, st);
+    ensure_device(*ivf, st);
+    const size_t nb = batch.size();
+    std::vector<float> qh(nb * dim);
+    for (size_t j = 0; j < nb; ++j) std::copy_n(q + batch[j] * dim, dim, qh.data() + j * dim);
+    SearchRequest pr;
+    pr.q = qh.data();
+    pr.nq = nb;
+    Prepared p;
+    prepare(idx, pr, p, st);
+
+    // per-query settings, and each distinct filter uploaded once
+    enum { kK, kKp, kNprobe, kMin, kWanted, kFields };
+    std::vector<int> h(kFields * nb);
+    std::vector<const SlotBits*> distinct;
+    std::vector<size_t> which(nb, SIZE_MAX);
+    int npmax = 1, kpmax = 1;
+    bool any_filter = false;
+    for (size_t j = 0; j < nb; ++j) {
+        const MixedQuery& m = qs[batch[j]];
+        const size_t np = std::min<size_t>(m.nprobe > 0 ? static_cast<size_t>(m.nprobe) : M.nprobe, M.nlist);
+        const size_t lv = m.filter ? m.filter->count : live;
+        const size_t kp = ref ? std::min(static_cast<size_t>(m.k) * ref->k_factor, lv) : static_cast<size_t>(m.k);
+        h[kK * nb + j] = m.k;
+        h[kKp * nb + j] = static_cast<int>(kp);
+        h[kNprobe * nb + j] = static_cast<int>(np);
+        if (m.filter) {
+            any_filter = true;
+            h[kMin * nb + j] = static_cast<int>(min_probes_for(M, np, m.filter->count));
+            h[kWanted * nb + j] = static_cast<int>(std::min(kp, m.filter->count));
+            auto it = std::find(distinct.begin(), distinct.end(), m.filter);
+            which[j] = static_cast<size_t>(it - distinct.begin());
+            if (it == distinct.end()) distinct.push_back(m.filter);
+        }
+        npmax = std::max(npmax, static_cast<int>(np));
+        kpmax = std::max(kpmax, static_cast<int>(kp));
+    }
+    require(kpmax <= 3072, "k * k_factor above 3072 is not supported by the GPU path", kUnsupported);
+    DevBuf<int> dh(h.size(), st);
+    QG_CUDA(cudaMemcpyAsync(dh.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    DevBuf<uint64_t> fwords;
+    DevBuf<const uint64_t*> fptr;
+    if (any_filter) {
+        const size_t words = distinct.front()->words.size();
+        for (const SlotBits* f : distinct) require(f->words.size() == words, "filters of one batch differ in size");
+        fwords.alloc(words * distinct.size(), st);
+        for (size_t d = 0; d < distinct.size(); ++d)
+            QG_CUDA(cudaMemcpyAsync(fwords.get() + d * words, distinct[d]->words.data(), words * 8,
+                                    cudaMemcpyHostToDevice, st));
+        std::vector<const uint64_t*> ptr(nb, nullptr);
+        for (size_t j = 0; j < nb; ++j)
+            if (which[j] != SIZE_MAX) ptr[j] = fwords.get() + which[j] * words;
+        fptr.alloc(nb, st);
+        QG_CUDA(cudaMemcpyAsync(fptr.get(), ptr.data(), nb * sizeof(void*), cudaMemcpyHostToDevice, st));
+    }
+    DevBuf<float> qrot;
+    IvfSearchArgs a;
+    a.q = ivf_queries(*ivf, p, nb, qrot, st);
+    a.nq = static_cast<int>(nb);
+    a.k = static_cast<int>(kmax);
+    a.kp = kpmax;
+    a.nprobe = npmax;
+    a.pq.k = dh.get() + kK * nb;
+    a.pq.kp = dh.get() + kKp * nb;
+    a.pq.nprobe = dh.get() + kNprobe * nb;
+    a.pq.filter = any_filter ? fptr.get() : nullptr;
+    a.pq.min_probes = dh.get() + kMin * nb;
+    a.pq.wanted = dh.get() + kWanted * nb;
+    a.any_filter = any_filter;
+    a.sm_count = sm_count_cached();
+    a.d_err = p.err.get();
+    DevBuf<uint64_t> ck(nb * kpmax, st);
+    DevBuf<uint32_t> cs(nb * kpmax, st);
+    ivf_candidates(ivf->dev.view, a, ck.get(), cs.get(), st);
+    DevBuf<int64_t> oid(nb * kmax, st);
+    DevBuf<float> od(nb * kmax, st);
+    const bool cosine = idx.metric() == Metric::Cosine, ip = idx.metric() == Metric::InnerProduct;
+    if (ref)
+        refine_candidates(p.q.get(), static_cast<int>(nb), static_cast<int>(dim), ref->dev.rows.get(), ck.get(), cs.get(),
+                          kpmax, static_cast<int>(kmax), ip, ref->dev.labels.get(), cosine, oid.get(), od.get(), st,
+                          a.pq.kp, a.pq.k);
+    else
+        finalize_ivf(ck.get(), cs.get(), static_cast<int>(nb), kpmax, static_cast<int>(kmax), ivf->dev.labels.get(), cosine,
+                     oid.get(), od.get(), st, a.pq.k);
+    std::vector<int64_t> hid(nb * kmax);
+    std::vector<float> hd(nb * kmax);
+    QG_CUDA(cudaMemcpyAsync(hid.data(), oid.get(), hid.size() * 8, cudaMemcpyDeviceToHost, st));
+    QG_CUDA(cudaMemcpyAsync(hd.data(), od.get(), hd.size() * 4, cudaMemcpyDeviceToHost, st));
+    check_err(p.err, st);
+    for (size_t j = 0; j < nb; ++j) {
+        std::copy_n(hid.data() + j * kmax, kmax, out_ids + batch[j] * kmax);
+        std::copy_n(hd.data() + j * kmax, kmax, out_d + batch[j] * kmax);
+    }
 }
 
 } // namespace qg

@@ -6,6 +6,11 @@
 
 namespace qg {
 
+// Keeps freed device memory cached in the default pool (once per process).
+void keep_pool_memory();
+// Sets the calling thread's qg_last_error() message.
+void set_last_error(const std::string& msg);
+
 // Where the query and result buffers live.
 enum class IoSpace { Host, Device };
 
@@ -16,10 +21,26 @@ struct SearchRequest {
     int64_t* out_ids = nullptr;      // nq * k
     float* out_d = nullptr;
     IoSpace io = IoSpace::Host;
+    int nprobe = 0;                  // > 0: probes instead of the IVF index's nprobe
 };
 
 // Runs a batch query on `st` and, for host I/O, waits for it.
 void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st);
+
+// One query of a mixed batch: a served request with its own settings.
+struct MixedQuery {
+    int k = 10;                      // results wanted, >= 1
+    int nprobe = 0;                  // <= 0: the index's nprobe
+    const SlotBits* filter = nullptr;   // allowed slots, or null
+};
+
+// A batch of queries that differ in k, nprobe and filter (host rows q, nq x
+// dim). IVF indexes and RefineIndexes over IVF run the batch as one coarse
+// step, one scan and one re-rank; each query's results are the ones it gets
+// searched alone with its settings. Results are nq x kmax (host), query i's
+// first qs[i].k valid and the rest padded with -1 / +inf.
+void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs, size_t kmax, int64_t* out_ids,
+                  float* out_d, cudaStream_t st);
 
 // add()'s argument checks alone, so they fail before any CUDA work.
 void validate_add(const IndexObj& idx, size_t n, const int64_t* ids);
@@ -54,3 +75,8 @@ void fast_scan_sums(const uint8_t* lut, size_t nluts, size_t m, const uint8_t* c
                     uint16_t* sums, cudaStream_t st);
 
 } // namespace qg
+
+// A C-ABI handle: one reference to an index object.
+struct qg_index {
+    std::shared_ptr<qg::IndexObj> obj;
+};

@@ -170,7 +170,8 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
     const int p0 = chunk * a.pch;
     const int np = min(a.nprobe_q ? a.nprobe_q[qi] : a.P, p0 + a.pch) - p0;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (np <= 0) {   // a filtered query that stopped probing before this chunk
+    const uint64_t* qfilter = a.filters ? a.filters[qi] : a.filter;
+    if (np <= 0) {   // a query whose probes end before this chunk
         for (int i = tid; i < a.kp; i += NT) {
             a.out_key[static_cast<size_t>(blockIdx.x) * a.kp + i] = ~0ull;
             a.out_slot[static_cast<size_t>(blockIdx.x) * a.kp + i] = 0xFFFFFFFFu;
@@ -367,8 +368,8 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
                         const uint64_t key = (static_cast<uint64_t>(float_key(dist)) << 32) | (push0 + pos);
                         if (key < thr) {
                             const uint32_t slot = v.ids[sbg * kSuperBlock + 8 * r + i];
-                            const bool ok = a.filter ? ((a.filter[slot >> 6] >> (slot & 63)) & 1ull)
-                                                     : !(v.deleted && ((v.deleted[slot >> 6] >> (slot & 63)) & 1ull));
+                            const bool ok = qfilter ? ((qfilter[slot >> 6] >> (slot & 63)) & 1ull)
+                                                    : !(v.deleted && ((v.deleted[slot >> 6] >> (slot & 63)) & 1ull));
                             if (ok) {
                                 const int idx = atomicAdd(&s_wcount[warp], 1);
                                 if (idx < wcap) wbuf[idx] = key;
@@ -417,7 +418,7 @@ int scan_cap(int kp) { return scan_layout(kp, 4, 0, 1, true, 1).wcap; }
 
 template <int NW>
 static void launch_scan(const ScanArgs& a, size_t smem, unsigned blocks, cudaStream_t st) {
-    QG_CUDA(cudaFuncSetAttribute(k_scan<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    allow_large_smem<k_scan<NW>>();
     KernelTimer kt("scan", st);
     k_scan<NW><<<blocks, NW * 32, smem, st>>>(a);
     QG_LAUNCH_CHECK();
@@ -430,9 +431,11 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     DevBuf<uint32_t> probe;
     DevBuf<float> pdist;
     DevBuf<int> nprobe_q;
-    if (s.filter) {
+    const int* probes_of = s.pq.nprobe;   // unfiltered mixed batch: each query's own nprobe (<= P)
+    if (s.filter || s.any_filter) {
         // every list ranked, then each query's own probe count (reference src/ivf_index.cpp:501-521)
         P = filtered_probes(v, s, probe, pdist, nprobe_q, st);
+        probes_of = nprobe_q.get();
     } else {
         // coarse: all pair scores, then the P nearest lists per query
         DevBuf<float> scores(static_cast<size_t>(nq) * v.nlist, st);
@@ -488,7 +491,8 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     a.qscale = qscale.get();
     a.qoffset = qoffset.get();
     a.filter = s.filter;
-    a.nprobe_q = nprobe_q.get();
+    a.filters = s.pq.filter;
+    a.nprobe_q = probes_of;
     a.P = P;
     a.pch = pch;
     a.nchunks = nchunks;

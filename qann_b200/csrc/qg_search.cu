@@ -274,7 +274,7 @@ void select_rows(const float* scores, size_t ld, int nrows, int ncols, int P, ui
     if (nrows == 0) return;
     const size_t smem = static_cast<size_t>(next_pow2(P)) * 16;
     if (smem > 48 * 1024)
-        QG_CUDA(cudaFuncSetAttribute(k_select_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        allow_large_smem<k_select_rows>();
     KernelTimer kt("select_rows", st);
     k_select_rows<<<nrows, 256, smem, st>>>(scores, ld, ncols, P, allow, deny, col_base, eq0, out_col, out_score);
     QG_LAUNCH_CHECK();
@@ -373,14 +373,16 @@ __global__ void __launch_bounds__(256) k_merge(const uint64_t* __restrict__ in_k
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_finalize_ivf(const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ slot_in,
                                                       int kp, int k, const int64_t* __restrict__ labels, bool cosine,
-                                                      int64_t* __restrict__ out_ids, float* __restrict__ out_d) {
+                                                      int64_t* __restrict__ out_ids, float* __restrict__ out_d,
+                                                      const int* __restrict__ k_q) {
     extern __shared__ uint8_t sm_raw[];
     const int kpow = max(2, next_pow2(k));
     uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);
     int64_t* val = reinterpret_cast<int64_t*>(key + kpow);
     const int qi = blockIdx.x;
+    const int kq = k_q ? min(k_q[qi], k) : k;   // the query's first kq candidates by key64
     for (int i = threadIdx.x; i < kpow; i += blockDim.x) {
-        const uint64_t k64 = i < k && i < kp ? key_in[static_cast<size_t>(qi) * kp + i] : ~0ull;
+        const uint64_t k64 = i < kq && i < kp ? key_in[static_cast<size_t>(qi) * kp + i] : ~0ull;
         if (k64 == ~0ull) {
             key[i] = ~0ull;
             val[i] = INT64_MAX;
@@ -412,17 +414,20 @@ __global__ void __launch_bounds__(128) k_finalize_ivf(const uint64_t* __restrict
 __global__ void __launch_bounds__(128) k_refine(const float* __restrict__ q, int dim, const float* __restrict__ rows,
                                                 const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ slot_in,
                                                 int kp, int k, bool ip, const int64_t* __restrict__ labels, bool cosine,
-                                                int64_t* __restrict__ out_ids, float* __restrict__ out_d) {
+                                                int64_t* __restrict__ out_ids, float* __restrict__ out_d,
+                                                const int* __restrict__ kp_q, const int* __restrict__ k_q) {
     extern __shared__ uint8_t sm_raw[];
     const int kpow = max(2, next_pow2(kp));
     uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);
     int64_t* val = reinterpret_cast<int64_t*>(key + kpow);
     float* qv = reinterpret_cast<float*>(val + kpow);
     const int qi = blockIdx.x;
+    const int kpq = kp_q ? min(kp_q[qi], kp) : kp;   // the query's first kpq candidates by key64
+    const int kq = k_q ? min(k_q[qi], k) : k;
     for (int t = threadIdx.x; t < dim; t += blockDim.x) qv[t] = q[static_cast<size_t>(qi) * dim + t];
     __syncthreads();
     for (int i = threadIdx.x; i < kpow; i += blockDim.x) {
-        const bool ok = i < kp && key_in[static_cast<size_t>(qi) * kp + i] != ~0ull;
+        const bool ok = i < kpq && key_in[static_cast<size_t>(qi) * kp + i] != ~0ull;
         if (!ok) {
             key[i] = ~0ull;
             val[i] = INT64_MAX;
@@ -436,7 +441,7 @@ __global__ void __launch_bounds__(128) k_refine(const float* __restrict__ q, int
     bitonic_sort(key, val, kpow);
     for (int i = threadIdx.x; i < k; i += blockDim.x) {
         const size_t o = static_cast<size_t>(qi) * k + i;
-        if (key[i] == ~0ull) {
+        if (i >= kq || key[i] == ~0ull) {
             out_ids[o] = -1;
             out_d[o] = __int_as_float(0x7f800000);
         } else {
@@ -515,7 +520,7 @@ void query_tables(const IvfView& v, const float* q, int nq, float* qC, uint4* ql
     if (nq == 0) return;
     const size_t smem = static_cast<size_t>(v.m) * 17 * 4;
     if (smem > 48 * 1024)
-        QG_CUDA(cudaFuncSetAttribute(k_query_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        allow_large_smem<k_query_tables>();
     KernelTimer kt("query_tables", st);
     k_query_tables<<<nq, 128, smem, st>>>(v, q, qC, qlut, qscale, qoffset);
     QG_LAUNCH_CHECK();
@@ -527,30 +532,31 @@ void merge_candidates(const uint64_t* in_key, const uint32_t* in_slot, int nq, i
     const int capm = next_pow2(2 * kp);
     const size_t msm = static_cast<size_t>(capm) * 16;
     if (msm > 48 * 1024)
-        QG_CUDA(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm)));
+        allow_large_smem<k_merge>();
     KernelTimer kt("merge", st);
     k_merge<<<nq, 256, msm, st>>>(in_key, in_slot, nchunks, kp, capm, out_key, out_slot);
     QG_LAUNCH_CHECK();
 }
 
 void finalize_ivf(const uint64_t* key, const uint32_t* slot, int nq, int kp, int k, const int64_t* labels, bool cosine,
-                  int64_t* out_ids, float* out_d, cudaStream_t st) {
+                  int64_t* out_ids, float* out_d, cudaStream_t st, const int* k_q) {
     if (nq == 0 || k == 0) return;
     const int kpow = std::max(2, next_pow2(k));
-    k_finalize_ivf<<<nq, 128, static_cast<size_t>(kpow) * 16, st>>>(key, slot, kp, k, labels, cosine, out_ids, out_d);
+    k_finalize_ivf<<<nq, 128, static_cast<size_t>(kpow) * 16, st>>>(key, slot, kp, k, labels, cosine, out_ids, out_d,
+                                                                      k_q);
     QG_LAUNCH_CHECK();
 }
 
 void refine_candidates(const float* q, int nq, int dim, const float* rows, const uint64_t* key, const uint32_t* slot,
                        int kp, int k, bool ip, const int64_t* labels, bool cosine, int64_t* out_ids, float* out_d,
-                       cudaStream_t st) {
+                       cudaStream_t st, const int* kp_q, const int* k_q) {
     if (nq == 0 || k == 0) return;
     const int kpow = std::max(2, next_pow2(kp));
     const size_t rsm = static_cast<size_t>(kpow) * 16 + static_cast<size_t>(dim) * 4;
     if (rsm > 48 * 1024)
-        QG_CUDA(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(rsm)));
+        allow_large_smem<k_refine>();
     KernelTimer kt("refine", st);
-    k_refine<<<nq, 128, rsm, st>>>(q, dim, rows, key, slot, kp, k, ip, labels, cosine, out_ids, out_d);
+    k_refine<<<nq, 128, rsm, st>>>(q, dim, rows, key, slot, kp, k, ip, labels, cosine, out_ids, out_d, kp_q, k_q);
     QG_LAUNCH_CHECK();
 }
 

@@ -36,6 +36,18 @@ struct IvfView {
     const uint64_t* deleted = nullptr;  // slot bitmap of deleted vectors, or null
 };
 
+// Per-query settings of a mixed batch: served requests that each carry their
+// own k, nprobe and filter. Device arrays of nq entries; a null array means
+// the batch-wide value for every query.
+struct PerQuery {
+    const int* k = nullptr;            // results wanted
+    const int* kp = nullptr;           // candidates kept (k, or min(k * k_factor, live))
+    const int* nprobe = nullptr;       // probes of an unfiltered query
+    const uint64_t* const* filter = nullptr;   // allowed-slot bitmap of each query (null entry: none)
+    const int* min_probes = nullptr;   // filtered queries: probe at least this many lists,
+    const int* wanted = nullptr;       // then on until this many allowed vectors were seen
+};
+
 struct ScanArgs {
     IvfView v;
     const float* q;          // nq * dim prepared queries
@@ -45,8 +57,9 @@ struct ScanArgs {
     const uint4* qlut;       // modes IP / cosine-IP: nq * m_pad rows
     const float* qscale;
     const float* qoffset;
-    const uint64_t* filter;  // allowed-slot bitmap, or null
-    const int* nprobe_q;     // per-query probe count (filtered queries), or null for P each
+    const uint64_t* filter;  // allowed-slot bitmap of every query, or null
+    const uint64_t* const* filters;   // per-query bitmaps (overrides filter), or null
+    const int* nprobe_q;     // per-query probe count, or null for P each
     int P, pch, nchunks, kp, cap;
     uint64_t* out_key;       // (nq * nchunks) * kp
     uint32_t* out_slot;
@@ -60,6 +73,8 @@ struct IvfSearchArgs {
     // filtered probing (reference src/ivf_index.cpp:501-521): probes run past
     // nprobe to at least min_probes, then until `wanted` allowed vectors were seen
     int min_probes = 0, wanted = 0;
+    PerQuery pq;                // mixed batches; nprobe above is then the largest nprobe
+    bool any_filter = false;    // some query of a mixed batch has a filter
     int sm_count = 0;
     int* d_err = nullptr;
 };
@@ -92,13 +107,15 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
 // The kp smallest key64 over nchunks sorted lists per query.
 void merge_candidates(const uint64_t* in_key, const uint32_t* in_slot, int nq, int nchunks, int kp, uint64_t* out_key,
                       uint32_t* out_slot, cudaStream_t st);
-// IVF results from candidates: the first k, sorted by (distance, id).
+// IVF results from candidates: the first k, sorted by (distance, id). With
+// k_q, query i takes its first k_q[i] candidates and pads the rest of its k.
 void finalize_ivf(const uint64_t* key, const uint32_t* slot, int nq, int kp, int k, const int64_t* labels, bool cosine,
-                  int64_t* out_ids, float* out_d, cudaStream_t st);
+                  int64_t* out_ids, float* out_d, cudaStream_t st, const int* k_q = nullptr);
 // Exact re-rank of candidates from raw rows: the k best by (score, slot).
+// With kp_q / k_q, query i re-ranks its first kp_q[i] candidates into k_q[i] results.
 void refine_candidates(const float* q, int nq, int dim, const float* rows, const uint64_t* key, const uint32_t* slot,
                        int kp, int k, bool ip, const int64_t* labels, bool cosine, int64_t* out_ids, float* out_d,
-                       cudaStream_t st);
+                       cudaStream_t st, const int* kp_q = nullptr, const int* k_q = nullptr);
 int scan_cap(int kp);
 
 } // namespace qg

@@ -98,7 +98,7 @@ void fast_scan_sums(const uint8_t* lut, size_t nluts, size_t m, const uint8_t* c
     const int OPB = static_cast<int>(std::max<size_t>(1, std::min<size_t>(16, (96 * 1024) / (static_cast<size_t>(m_pad) * 16))));
     const size_t smem = static_cast<size_t>(OPB) * m_pad * 16;
     if (smem > 48 * 1024)
-        QG_CUDA(cudaFuncSetAttribute(k_scan_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        allow_large_smem<k_scan_sums>();
     k_scan_sums<<<static_cast<unsigned>(ceil_div(nsb, OPB)), 8 * OPB, smem, st>>>(
         packed.get(), nsb, reinterpret_cast<const uint4*>(lut), mi, m_pad, lut_of, n, sums);
     QG_LAUNCH_CHECK();

@@ -169,6 +169,19 @@ int qg_exact_scores_dev(const float* a_dev, size_t na, const float* b_dev, size_
 int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, const uint8_t* codes_dev,
                              const uint32_t* lut_of_dev, size_t n, uint16_t* sums_dev, void* stream);
 
+/* --- process-wide options ---------------------------------------------------------
+ * "tensor_filter": exact top-k searches over many rows (flat search, RefineIndex
+ *   direct scans, nearest-centroid assignment in add and k-means) first filter
+ *   candidates with a BF16 tcgen05 GEMM and a rigorous error bound, then rescore
+ *   them exactly; the results are those of the exact path either way.
+ *   0 = never, 1 = when the work is large enough to pay (default), 2 = whenever
+ *   the dimension is supported (<= 128). qg_get_option also reads
+ *   "tensor_filter_queries" (queries answered through the filter so far) and
+ *   "tensor_filter_redone" (those redone exactly after a candidate overflow). No counterpart in the reference, whose
+ *   exact scores always come from its CPU distance kernels (reference src/flat_index.cpp:33-64). */
+int qg_set_option(const char* key, int64_t value);
+int qg_get_option(const char* key, int64_t* value);
+
 /* --- serving (no counterpart in the reference, whose query_batch answers one
  * call on the calling threads, reference bindings/python_bindings.cpp:600-648) ----
  * A server keeps the index on the device and runs requests with continuous

@@ -77,6 +77,30 @@ def _ids(ids) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(list(ids) if not hasattr(ids, "__len__") else ids, dtype=np.int64).ravel())
 
 
+def set_tensor_filter(mode: int) -> None:
+    """Exact top-k over many rows through the BF16 tensor-core filter and FP32
+    recheck: 0 never, 1 when it pays (default), 2 whenever supported. Results
+    are identical in every mode."""
+    check(_lib.lib.qg_set_option(b"tensor_filter", int(mode)))
+
+
+def tensor_filter() -> int:
+    v = C.c_int64()
+    check(_lib.lib.qg_get_option(b"tensor_filter", C.byref(v)))
+    return v.value
+
+
+def tensor_filter_counts() -> dict:
+    """Queries answered through the tensor-core filter so far, and how many of
+    them were redone exactly because their candidate lists overflowed."""
+    out = {}
+    for key in ("queries", "redone"):
+        v = C.c_int64()
+        check(_lib.lib.qg_get_option(f"tensor_filter_{key}".encode(), C.byref(v)))
+        out[key] = v.value
+    return out
+
+
 class DenseIndex:
     """An index of dense float32 vectors. Not constructed directly."""
 

@@ -51,6 +51,8 @@ _SIGS = {
     "qg_fast_scan_dev": (C.c_int, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),
     "qg_exact_scores_dev": (C.c_int, [_vp, _sz, _vp, _sz, _sz, C.c_int, _vp, _vp]),
     "qg_fast_scan_noalloc_dev": (C.c_int, [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]),
+    "qg_set_option": (C.c_int, [C.c_char_p, _i64]),
+    "qg_get_option": (C.c_int, [C.c_char_p, C.POINTER(_i64)]),
     "qg_server_create": (C.c_int, [_vp, C.c_int, C.c_int, _sz, C.POINTER(_vp)]),
     "qg_server_add_filter": (C.c_int, [_vp, _vp, _sz, C.POINTER(C.c_int)]),
     "qg_server_submit": (C.c_int, [_vp, _vp, _sz, C.c_int, _vp, _sz, C.c_int, C.POINTER(C.c_uint64)]),

@@ -34,6 +34,12 @@ __global__ void k_row_argmin(const float* __restrict__ scores, size_t ld, int nr
 void assign_nearest(const float* x_dev, size_t n, const float* c_dev, size_t k, int dim, uint32_t* out_dev,
                     cudaStream_t st) {
     if (n == 0) return;
+    if (use_tensor_filter(n, k, dim, 1)) {
+        // the smallest (score, centroid): the same first-index-on-ties rule
+        DevBuf<uint64_t> key(n, st);
+        flat_candidates(x_dev, n, c_dev, k, dim, false, 1, nullptr, nullptr, key.get(), out_dev, st);
+        return;
+    }
     const size_t T = std::max<size_t>(1, std::min<size_t>(n, (size_t{512} << 20) / (k * sizeof(float))));
     DevBuf<float> scores(T * k, st);
     for (size_t r0 = 0; r0 < n; r0 += T) {

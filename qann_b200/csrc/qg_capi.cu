@@ -513,6 +513,32 @@ int qg_exact_scores_dev(const float* a_dev, size_t na, const float* b_dev, size_
     });
 }
 
+int qg_set_option(const char* key, int64_t value) {
+    return guarded([&] {
+        require(key != nullptr, "null key");
+        const std::string k(key);
+        if (k == "tensor_filter") {
+            require(value >= 0 && value <= 2, "tensor_filter must be 0, 1 or 2");
+            set_tensor_filter(static_cast<int>(value));
+        } else {
+            throw Error(kInvalidArgument, "unknown option: " + k);
+        }
+    });
+}
+
+int qg_get_option(const char* key, int64_t* value) {
+    return guarded([&] {
+        require(key != nullptr && value != nullptr, "null argument");
+        const std::string k(key);
+        int64_t queries = 0, redone = 0;
+        tensor_filter_counts(&queries, &redone);
+        if (k == "tensor_filter") *value = tensor_filter();
+        else if (k == "tensor_filter_queries") *value = queries;
+        else if (k == "tensor_filter_redone") *value = redone;
+        else throw Error(kInvalidArgument, "unknown option: " + k);
+    });
+}
+
 int qg_symmetric_eigen(const double* a, size_t d, double* values, double* vectors) {
     return guarded([&] {
         require(a && values && vectors, "null buffer");

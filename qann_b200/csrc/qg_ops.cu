@@ -5,6 +5,7 @@
 #include "qg_train.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <numeric>
 
@@ -60,9 +61,9 @@ __global__ void __launch_bounds__(256) k_merge2(uint64_t* __restrict__ akey, uin
     }
 }
 
-void flat_candidates(const float* q_dev, size_t nq, const float* rows_dev, size_t n, int dim, bool ip, size_t k,
-                     const uint64_t* allow_dev, const uint64_t* deny_dev, uint64_t* out_key, uint32_t* out_slot,
-                     cudaStream_t st) {
+static void flat_candidates_fp32(const float* q_dev, size_t nq, const float* rows_dev, size_t n, int dim, bool ip,
+                                 size_t k, const uint64_t* allow_dev, const uint64_t* deny_dev, uint64_t* out_key,
+                                 uint32_t* out_slot, cudaStream_t st) {
     if (nq == 0 || k == 0) return;
     require(k <= 4096, "k above 4096 is not supported by the GPU flat search", kUnsupported);
     QG_CUDA(cudaMemsetAsync(out_key, 0xFF, nq * k * sizeof(uint64_t), st));
@@ -97,6 +98,66 @@ void flat_candidates(const float* q_dev, size_t nq, const float* rows_dev, size_
             QG_LAUNCH_CHECK();
         }
     }
+}
+
+namespace {
+std::atomic<int> g_tensor_filter{1};
+std::atomic<int64_t> g_filter_queries{0}, g_filter_redone{0};
+}
+
+void tensor_filter_counts(int64_t* queries, int64_t* redone) {
+    *queries = g_filter_queries.load();
+    *redone = g_filter_redone.load();
+}
+
+void set_tensor_filter(int mode) { g_tensor_filter.store(mode); }
+int tensor_filter() { return g_tensor_filter.load(); }
+
+// The exact top-k either way; the tensor-core filter when the work is large
+// enough to pay for its bf16 copies (or always, in mode 2), the FP32 tiles
+// otherwise.
+bool use_tensor_filter(size_t nq, size_t n, int dim, size_t k) {
+    const int mode = g_tensor_filter.load();
+    const size_t seed = std::max<size_t>(4096, 4 * k);
+    return mode > 0 && mm_supported(dim) && k <= 1024 && n > 2 * seed &&
+           (mode == 2 || (nq >= 64 && static_cast<double>(nq) * double(n) * dim >= 2e10));
+}
+
+void flat_candidates(const float* q_dev, size_t nq, const float* rows_dev, size_t n, int dim, bool ip, size_t k,
+                     const uint64_t* allow_dev, const uint64_t* deny_dev, uint64_t* out_key, uint32_t* out_slot,
+                     cudaStream_t st, bool allow_mm, const MmRows* pre) {
+    if (!allow_mm || !use_tensor_filter(nq, n, dim, k)) {
+        flat_candidates_fp32(q_dev, nq, rows_dev, n, dim, ip, k, allow_dev, deny_dev, out_key, out_slot, st);
+        return;
+    }
+    MmRows tmp;
+    const MmRows* base = pre;
+    if (!base) {
+        mm_prepare(rows_dev, n, dim, tmp, st);
+        base = &tmp;
+    }
+    std::vector<int> ovf;
+    mm_topk(q_dev, nq, rows_dev, *base, ip, k, allow_dev, deny_dev, out_key, out_slot, ovf, st);
+    g_filter_queries += static_cast<int64_t>(nq);
+    g_filter_redone += static_cast<int64_t>(ovf.size());
+    if (ovf.empty()) return;
+    // queries whose candidate list overflowed: the exact FP32 tiles over every row
+    const size_t m = ovf.size();
+    DevBuf<uint32_t> idx(m, st);
+    std::vector<uint32_t> hidx(ovf.begin(), ovf.end());
+    QG_CUDA(cudaMemcpyAsync(idx.get(), hidx.data(), m * 4, cudaMemcpyHostToDevice, st));
+    DevBuf<float> qs(m * dim, st);
+    gather_rows(q_dev, idx.get(), m, dim, qs.get(), st);
+    DevBuf<uint64_t> sk(m * k, st);
+    DevBuf<uint32_t> ss(m * k, st);
+    flat_candidates_fp32(qs.get(), m, rows_dev, n, dim, ip, k, allow_dev, deny_dev, sk.get(), ss.get(), st);
+    for (size_t j = 0; j < m; ++j) {
+        QG_CUDA(cudaMemcpyAsync(out_key + static_cast<size_t>(ovf[j]) * k, sk.get() + j * k, k * 8,
+                                cudaMemcpyDeviceToDevice, st));
+        QG_CUDA(cudaMemcpyAsync(out_slot + static_cast<size_t>(ovf[j]) * k, ss.get() + j * k, k * 4,
+                                cudaMemcpyDeviceToDevice, st));
+    }
+    QG_CUDA(cudaStreamSynchronize(st));
 }
 
 // Flat results in (score, slot) order with ids and the exact score.

@@ -52,11 +52,38 @@ void add(IndexObj& idx, const float* x, size_t n, const int64_t* ids, int64_t* o
 void train(IVFObj& o, const float* x, size_t n, size_t max_iters, int64_t seed, int clustering, size_t passes,
            cudaStream_t st);
 
+// A row set's bf16 copy for the tensor-core filter (rows zero-padded to dpad,
+// a multiple of 8) and each row's squared norm.
+struct MmRows {
+    size_t n = 0;
+    int dim = 0, dpad = 0;
+    DevBuf<uint16_t> bf16;
+    DevBuf<float> sq;
+};
+bool mm_supported(int dim);
+void mm_prepare(const float* rows, size_t n, int dim, MmRows& out, cudaStream_t st);
+// The exact top-k by the BF16 tensor-core filter and FP32 recheck (qg_mm.cu);
+// queries whose candidate lists overflowed are listed in overflow_q and must
+// be redone exactly.
+void mm_topk(const float* q, size_t nq, const float* rows, const MmRows& base, bool ip, size_t k, const uint64_t* allow,
+             const uint64_t* deny, uint64_t* out_key, uint32_t* out_slot, std::vector<int>& overflow_q,
+             cudaStream_t st);
+// 0: never use the tensor-core filter; 1: when the work pays for it; 2: whenever supported.
+void set_tensor_filter(int mode);
+int tensor_filter();
+// Queries answered through the filter so far, and those of them redone exactly
+// because their candidate lists overflowed.
+void tensor_filter_counts(int64_t* queries, int64_t* redone);
+// Whether an exact top-k of nq queries over n rows goes through the filter.
+bool use_tensor_filter(size_t nq, size_t n, int dim, size_t k);
+
 // Flat exact search over device rows: the k smallest by (score, slot) per
 // query, as (key64 = key_eq0(score) << 32 | slot) sorted lists of length k.
+// Large problems go through the tensor-core filter (identical results) unless
+// allow_mm is false; pre is the rows' prepared bf16 copy, if the caller keeps one.
 void flat_candidates(const float* q_dev, size_t nq, const float* rows_dev, size_t n, int dim, bool ip, size_t k,
                      const uint64_t* allow_dev, const uint64_t* deny_dev, uint64_t* out_key, uint32_t* out_slot,
-                     cudaStream_t st);
+                     cudaStream_t st, bool allow_mm = true, const MmRows* pre = nullptr);
 
 // Nearest centroid (squared L2, first index on ties) of each row, as the
 // reference's assign_nearest without BLAS (reference src/kmeans.cpp:34-115).

@@ -199,27 +199,38 @@ inline constexpr int kSuperBlock = 64;
 // Sums of the 8 vectors of one octet lane over m_pad subspaces (m_pad % 4 == 0).
 // lut: m_pad rows as uint4 (shared memory). Sums are exact uint16 values
 // (m_pad * 63 <= 64512).
+__device__ __forceinline__ void octet_step(const uint4& w, const uint4* __restrict__ lut, uint32_t& a0, uint32_t& b0,
+                                           uint32_t& a1, uint32_t& b1) {
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+    uint32_t g0 = 0, g1 = 0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const uint4 L = lut[t];
+        const uint32_t c = ws[t];
+        const uint32_t cx = c ^ 0x88888888u;
+        g0 += prmt(L.x, L.y, c) + prmt(L.z, L.w, cx);
+        g1 += prmt(L.x, L.y, c >> 16) + prmt(L.z, L.w, cx >> 16);
+    }
+    a0 += g0 & 0x00FF00FFu;
+    b0 += (g0 >> 8) & 0x00FF00FFu;
+    a1 += g1 & 0x00FF00FFu;
+    b1 += (g1 >> 8) & 0x00FF00FFu;
+}
+
 __device__ __forceinline__ void octet_sums(const uint4* __restrict__ sb, const uint4* __restrict__ lut, int m_pad,
                                            int r, uint32_t sums[8]) {
     uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
     const int nq = m_pad >> 2;
-    for (int q = 0; q < nq; ++q) {
-        const uint4 w = __ldg(sb + q * 8 + r);
-        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
-        uint32_t g0 = 0, g1 = 0;
+    int q = 0;
+    // four 16-byte code loads in flight before their lookups
+    for (; q + 4 <= nq; q += 4) {
+        uint4 w[4];
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const uint4 L = lut[4 * q + t];
-            const uint32_t c = ws[t];
-            const uint32_t cx = c ^ 0x88888888u;
-            g0 += prmt(L.x, L.y, c) + prmt(L.z, L.w, cx);
-            g1 += prmt(L.x, L.y, c >> 16) + prmt(L.z, L.w, cx >> 16);
-        }
-        a0 += g0 & 0x00FF00FFu;
-        b0 += (g0 >> 8) & 0x00FF00FFu;
-        a1 += g1 & 0x00FF00FFu;
-        b1 += (g1 >> 8) & 0x00FF00FFu;
+        for (int u = 0; u < 4; ++u) w[u] = __ldg(sb + (q + u) * 8 + r);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) octet_step(w[u], lut + 4 * (q + u), a0, b0, a1, b1);
     }
+    for (; q < nq; ++q) octet_step(__ldg(sb + q * 8 + r), lut + 4 * q, a0, b0, a1, b1);
     sums[0] = a0 & 0xFFFFu;
     sums[1] = b0 & 0xFFFFu;
     sums[2] = a0 >> 16;

@@ -1,25 +1,31 @@
 // The code scan with fused top-k' selection (reference src/ivf_index.cpp:421-641,
 // src/topk.hpp), and the orchestration of one IVF fast-scan search.
 //
-// A block takes one query and a chunk of its probes. The chunk's lists are cut
-// into work items of at most 8 superblocks (64 vectors each), in probe order.
-// Warps run independently: a warp takes the next 4 items, builds their uint8
-// LUTs with its 32 lanes (mode L2: B + C + A rounded, as build_quantize_lut;
-// mode L2-ADC: the residual's ADC table rounded; modes IP / cosine-IP use the
-// query's one LUT and skip this), and its 4 octets (8 lanes each) scan one
-// item each with register-resident 4-bit lookups.
+// Work units are (query, chunk of at most 256 of its probes). The kernel is
+// persistent: a block takes the next unit from a global counter until none
+// is left. Inside a unit the block walks the probes in groups of `lc` lists.
+// For each group the warps first build the lists' uint8 LUTs into one half
+// of a double-buffered LUT ring (mode L2: B + C + A rounded as
+// build_quantize_lut; mode L2-ADC: the residual's ADC table rounded; modes IP
+// and cosine-IP share the query's one LUT and only set each list's
+// scale / offset). Then every octet (8 lanes) of every warp takes superblocks
+// (64 vectors) of the group from a shared counter, so uneven lists spread
+// over all octets. A warp that finds no superblock left goes on to build the
+// next group's LUTs in the other half: one block barrier per group.
 //
 // Selection keeps the k' smallest candidates by key64 = key(dist) << 32 |
 // push index, the push index being the vector's position in the query's
 // sequence of probed lists: exactly the set the reference's TopK keeps
-// (distance first, first pushed among ties). Each warp buffers the candidates
-// that beat the block's threshold; when its buffer fills it keeps its own k'
-// best and lowers the block threshold to its k'-th key (an upper bound of the
-// block's k'-th, so the pruning is exact). Deleted (or filtered-out) vectors
-// are skipped before they can enter, as the reference's push() does. The
-// integer pre-test `sum <= S*` is exact: S* is the largest sum whose distance
-// is <= the threshold distance (sum_limit). At the end the warps' lists are
-// merged and the k' survivors' slots are looked up from their push index.
+// (distance first, first pushed among ties). Each warp appends the candidates
+// that beat the block's threshold to its own buffer; when the buffer is
+// nearly full it keeps its k' best (radix select) and lowers the block
+// threshold to its k'-th key (an upper bound of the block's k'-th, so the
+// pruning is exact). Deleted (or filtered-out) vectors are skipped before
+// they can enter, as the reference's push() does. The integer pre-test
+// `sum <= S*` is exact: S* is the largest sum whose distance is <= the
+// threshold distance (sum_limit). At the end of a unit the warps' survivors
+// are gathered, cut to k', sorted, and their slots looked up from the push
+// index.
 #include "qg_device.cuh"
 #include "qg_search.h"
 
@@ -28,9 +34,8 @@
 namespace qg {
 
 namespace {
-constexpr int kItemSb = 8;       // superblocks per work item
-constexpr int kMaxChunk = 256;   // probes per block at most
-constexpr int kItemsPerWarp = 4;
+constexpr int kMaxChunk = 256;   // probes per work unit at most
+constexpr int kSbPerWarp = 4;    // superblocks a warp takes at a time, one per octet
 }
 
 // The 16 entries of LUT rows rounded and packed: round-half-even of
@@ -47,15 +52,17 @@ __device__ __forceinline__ uint4 round_row(const float* v, float mn, float scale
                       prmt(prmt(b[12], b[13], 0x0040), prmt(b[14], b[15], 0x0040), 0x5410));
 }
 
-// LUT of one list by one warp (rows cached in registers for m <= 64; larger
-// m recomputes rows in the second pass). Same arithmetic as quantize_lut.
+// LUT of one list by one warp. Same arithmetic as quantize_lut; the rows are
+// formed twice (for their ranges, then for rounding) rather than held in
+// registers across the warp-wide reductions.
 template <class RowFn>
 __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* row_min, uint4* lut_out, float& scale_out,
                                           float& offset_out) {
     const int lane = threadIdx.x & 31;
-    float v0[16], v1[16];
     float widest = 0.0f;
-    auto ranges = [&](int r, float* v) {
+    for (int r = lane; r < m; r += 32) {
+        float v[16];
+        row(r, v);
         float lo = v[0], hi = v[0];
 #pragma unroll
         for (int j = 1; j < 16; ++j) {
@@ -65,21 +72,6 @@ __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* ro
         row_min[r] = lo;
         const float w = __fsub_rn(hi, lo);
         widest = widest < w ? w : widest;
-    };
-    if (m <= 64) {
-        if (lane < m) {
-            row(lane, v0);
-            ranges(lane, v0);
-        }
-        if (lane + 32 < m) {
-            row(lane + 32, v1);
-            ranges(lane + 32, v1);
-        }
-    } else {
-        for (int r = lane; r < m; r += 32) {
-            row(r, v0);
-            ranges(r, v0);
-        }
     }
     widest = warp_max(widest);
     __syncwarp();
@@ -90,19 +82,67 @@ __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* ro
     const float p2 = __shfl_sync(0xffffffffu, part, 2), p3 = __shfl_sync(0xffffffffu, part, 3);
     const float offset = __fadd_rn(__fadd_rn(p0, p1), __fadd_rn(p2, p3));
     const float scale = widest > 0.0f ? __fdiv_rn(static_cast<float>(kLutMax), widest) : 1.0f;
-    if (m <= 64) {
-        if (lane < m) lut_out[lane] = round_row(v0, row_min[lane], scale);
-        if (lane + 32 < m) lut_out[lane + 32] = round_row(v1, row_min[lane + 32], scale);
-    } else {
-        for (int r = lane; r < m; r += 32) {
-            row(r, v0);
-            lut_out[r] = round_row(v0, row_min[r], scale);
-        }
+    for (int r = lane; r < m; r += 32) {
+        float v[16];
+        row(r, v);
+        lut_out[r] = round_row(v, row_min[r], scale);
     }
     for (int r = m + lane; r < m_pad; r += 32) lut_out[r] = make_uint4(0, 0, 0, 0);
     scale_out = scale;
     offset_out = offset;
     __syncwarp();
+}
+
+// Mode L2: the LUT of B[list] + C[query] (+ A on row 0), as build_quantize_lut
+// sums them (reference src/fast_scan.cpp:243-254).
+__device__ __noinline__ void warp_lut_l2(const float* __restrict__ B, const float* qtab, float A, int m, int m_pad,
+                                         float* row_min, uint4* lut_out, float* scale_out, float* offset_out) {
+    float sc, of;
+    warp_lut3(
+        [&](int rr, float* o) {
+            const float4* b4 = reinterpret_cast<const float4*>(B + rr * 16);
+            const float4* c4 = reinterpret_cast<const float4*>(qtab + rr * 16);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float4 bb = __ldg(b4 + u), cc = c4[u];
+                o[4 * u + 0] = __fadd_rn(bb.x, cc.x);
+                o[4 * u + 1] = __fadd_rn(bb.y, cc.y);
+                o[4 * u + 2] = __fadd_rn(bb.z, cc.z);
+                o[4 * u + 3] = __fadd_rn(bb.w, cc.w);
+            }
+            if (rr == 0) {
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj) o[jj] = __fadd_rn(o[jj], A);
+            }
+        },
+        m, m_pad, row_min, lut_out, sc, of);
+    *scale_out = sc;
+    *offset_out = of;
+}
+
+// Mode L2-ADC: the LUT of the residual's ADC table; the residual (q - center)
+// is formed per element inside the table loop, as compute_adc_table reads it
+// (reference src/ivf_index.cpp:594-610).
+__device__ __noinline__ void warp_lut_adc(const float* __restrict__ ctr, const float* q, const float* __restrict__ pq_t,
+                                          int sd, int m, int m_pad, float* row_min, uint4* lut_out, float* scale_out,
+                                          float* offset_out) {
+    float sc, of;
+    warp_lut3(
+        [&](int rr, float* o) {
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) {
+                float acc = 0.0f;
+                for (int u = 0; u < sd; ++u) {
+                    const int e = rr * sd + u;
+                    const float diff = __fsub_rn(__fsub_rn(q[e], ctr[e]), pq_t[e * 16 + jj]);
+                    acc = __fmaf_rn(diff, diff, acc);
+                }
+                o[jj] = acc;
+            }
+        },
+        m, m_pad, row_min, lut_out, sc, of);
+    *scale_out = sc;
+    *offset_out = of;
 }
 
 __device__ __forceinline__ int upper_index(const uint32_t* pre, int n, uint32_t x) {
@@ -116,47 +156,126 @@ __device__ __forceinline__ int upper_index(const uint32_t* pre, int n, uint32_t 
     return lo;
 }
 
-// Keys only, one warp, n a power of two.
-__device__ __forceinline__ void warp_sort_keys(uint64_t* key, int n) {
+// One warp keeps the `keep` smallest of the n distinct keys buf[0, n) in
+// buf[0, keep) (in no particular order) and returns the largest kept key.
+// Radix select, 8 bits at a time from the top: each pass counts the keys
+// that share the prefix chosen so far by their next digit, and takes the
+// digit whose bin holds the keep-th key; it stops once every key of that
+// bin is kept. hist: 256 ints of warp-private shared scratch. n > keep >= 1.
+__device__ __noinline__ uint64_t warp_select_keep(uint64_t* buf, int n, int keep, int* hist) {
     const int lane = threadIdx.x & 31;
-    for (int size = 2; size <= n; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            __syncwarp();
-            for (int t = lane; t < (n >> 1); t += 32) {
-                const int lo = 2 * t - (t & (stride - 1));
-                const int hi = lo + stride;
-                const bool up = (lo & size) == 0;
-                const uint64_t k0 = key[lo], k1 = key[hi];
-                if (up ? (k1 < k0) : (k0 < k1)) {
-                    key[lo] = k1;
-                    key[hi] = k0;
+    constexpr unsigned kFull = 0xffffffffu;
+    uint64_t prefix = 0, mask = 0;
+    int need = keep;   // keys still to take among those that match the prefix
+    int shift = 56;
+    for (;; shift -= 8) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) hist[8 * lane + j] = 0;
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            const uint64_t k = buf[i];
+            if ((k & mask) == prefix) atomicAdd(&hist[static_cast<int>(k >> shift) & 255], 1);
+        }
+        __syncwarp();
+        int c[8], own = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            c[j] = hist[8 * lane + j];
+            own += c[j];
+        }
+        int incl = own;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int excl = incl - own;
+        const unsigned owner = __ballot_sync(kFull, excl < need && need <= incl);
+        const int ol = __ffs(owner) - 1;
+        int digit = 0, below = 0, cnt = 0;
+        if (lane == ol) {
+            int acc = excl;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (cnt == 0 && acc + c[j] >= need) {
+                    digit = 8 * lane + j;
+                    below = acc;
+                    cnt = c[j];
                 }
+                acc += c[j];
             }
         }
+        digit = __shfl_sync(kFull, digit, ol);
+        below = __shfl_sync(kFull, below, ol);
+        cnt = __shfl_sync(kFull, cnt, ol);
+        need -= below;
+        prefix |= static_cast<uint64_t>(digit) << shift;
+        mask |= 0xFFull << shift;
+        __syncwarp();
+        if (cnt == need || shift == 0) break;   // (at shift 0 the bin is one key)
+    }
+    // kept: every key whose bits above `shift` do not exceed the prefix
+    const uint64_t lim = prefix | ((1ull << shift) - 1);
+    int out = 0;
+    uint64_t kmax = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + lane;
+        uint64_t k = 0;
+        bool in = false;
+        if (i < n) {
+            k = buf[i];
+            in = k <= lim;
+        }
+        const unsigned bal = __ballot_sync(kFull, in);
+        __syncwarp();
+        if (in) {
+            buf[out + __popc(bal & ((1u << lane) - 1))] = k;
+            kmax = k > kmax ? k : kmax;
+        }
+        out += __popc(bal);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const uint64_t t = __shfl_xor_sync(kFull, kmax, o);
+        kmax = t > kmax ? t : kmax;
     }
     __syncwarp();
+    return kmax;
 }
 
+// Shared memory of one block. The LUT ring shares its space with the
+// end-of-unit gather of candidates and their final sort.
 struct ScanLayout {
-    int wcap;    // per-warp candidate buffer (keys)
-    int nw;      // warps per block
-    size_t bytes;
+    int nw, lc, wcap, lut_stride;   // lut_stride: uint4s per LUT (m_pad + 2: 32 bytes keep
+                                    // consecutive LUTs of a warp's octets on distinct banks)
+    size_t off_wbuf, off_hist, off_rmin, off_group, off_probe, off_qtab, bytes;
 };
 
-__host__ __device__ inline ScanLayout scan_layout(int kp, int m_pad, int qtab_len, int pch, bool shared_lut, int nw) {
+__host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~static_cast<size_t>(15); }
+
+__host__ __device__ inline ScanLayout scan_layout(int kp, int m_pad, int qtab_len, int pch, bool shared_lut, int nw,
+                                                  int lc) {
     ScanLayout L;
     L.nw = nw;
-    int w = 1;
-    while (w < kp + kItemsPerWarp * kSuperBlock) w <<= 1;
-    L.wcap = w;
-    size_t b = static_cast<size_t>(nw) * w * 8;                                          // candidate buffers
-    b += shared_lut ? static_cast<size_t>(m_pad) * 16
-                    : static_cast<size_t>(nw) * kItemsPerWarp * m_pad * 16;              // LUTs
-    b += shared_lut ? 0 : static_cast<size_t>(nw) * m_pad * 4;                           // row minimums
-    b += static_cast<size_t>(nw) * kItemsPerWarp * 8;                                    // per-warp scale / offset
+    L.lc = lc;
+    L.wcap = (kp + kSbPerWarp * kSuperBlock + 31) & ~31;
+    L.lut_stride = m_pad + 2;
+    const size_t lut = shared_lut ? static_cast<size_t>(m_pad) * 16 : static_cast<size_t>(2) * lc * L.lut_stride * 16;
+    const size_t gather = static_cast<size_t>(nw) * kp * 8;
+    const size_t sortb = static_cast<size_t>(next_pow2(kp < 2 ? 2 : kp)) * 8;
+    size_t b = align16(lut > gather ? (lut > sortb ? lut : sortb) : (gather > sortb ? gather : sortb));
+    L.off_wbuf = b;
+    b += static_cast<size_t>(nw) * L.wcap * 8;
+    L.off_hist = b;
+    b += static_cast<size_t>(nw) * 256 * 4;
+    L.off_rmin = b;
+    b += shared_lut ? 0 : static_cast<size_t>(nw) * m_pad * 4;
+    L.off_group = b;
+    b += static_cast<size_t>(2) * lc * 8;                         // scale, offset of both halves
+    L.off_probe = b;
+    b += static_cast<size_t>(pch) * 12 + static_cast<size_t>(pch + 1) * 4;   // list, size, push, superblock prefix
+    b = align16(b);
+    L.off_qtab = b;
     b += static_cast<size_t>(qtab_len) * 4;
-    b += static_cast<size_t>(pch) * 4 * 6 + 4 * 2;                                       // per-probe arrays
-    L.bytes = b;
+    L.bytes = align16(b);
     return L;
 }
 
@@ -164,261 +283,266 @@ template <int NW>
 __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
     extern __shared__ __align__(16) uint8_t sm[];
     constexpr int NT = NW * 32;
+    constexpr unsigned kFull = 0xffffffffu;
     const IvfView& v = a.v;
-    const int qi = blockIdx.x / a.nchunks;
-    const int chunk = blockIdx.x - qi * a.nchunks;
-    const int p0 = chunk * a.pch;
-    const int np = min(a.nprobe_q ? a.nprobe_q[qi] : a.P, p0 + a.pch) - p0;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint64_t* qfilter = a.filters ? a.filters[qi] : a.filter;
-    if (np <= 0) {   // a query whose probes end before this chunk
-        for (int i = tid; i < a.kp; i += NT) {
-            a.out_key[static_cast<size_t>(blockIdx.x) * a.kp + i] = ~0ull;
-            a.out_slot[static_cast<size_t>(blockIdx.x) * a.kp + i] = 0xFFFFFFFFu;
-        }
-        return;
-    }
     const int oct = lane >> 3, r = lane & 7;
     const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
     const int qtab_len = v.mode == kModeL2 ? v.m * 16 : (v.mode == kModeL2Adc ? v.dim : 0);
-    const ScanLayout lay = scan_layout(a.kp, v.m_pad, qtab_len, a.pch, shared_lut, NW);
-    const int wcap = lay.wcap;
+    const ScanLayout lay = scan_layout(a.kp, v.m_pad, qtab_len, a.pch, shared_lut, NW, a.lc);
+    const int wcap = lay.wcap, LC = lay.lc, LS = lay.lut_stride, kp = a.kp;
 
-    uint64_t* wbuf_all = reinterpret_cast<uint64_t*>(sm);
-    uint4* lut_all = reinterpret_cast<uint4*>(wbuf_all + static_cast<size_t>(NW) * wcap);
-    float* rmin_all = reinterpret_cast<float*>(
-        lut_all + (shared_lut ? static_cast<size_t>(v.m_pad) : static_cast<size_t>(NW) * kItemsPerWarp * v.m_pad));
-    float* wscale_all = rmin_all + (shared_lut ? 0 : NW * v.m_pad);
-    float* woffset_all = wscale_all + NW * kItemsPerWarp;
-    float* qtab = woffset_all + NW * kItemsPerWarp;
-    float* p_scale = qtab + qtab_len;
-    float* p_offset = p_scale + a.pch;
-    uint32_t* p_list = reinterpret_cast<uint32_t*>(p_offset + a.pch);
+    uint4* lut_ring = reinterpret_cast<uint4*>(sm);
+    uint64_t* gath = reinterpret_cast<uint64_t*>(sm);
+    uint64_t* wbuf = reinterpret_cast<uint64_t*>(sm + lay.off_wbuf) + static_cast<size_t>(warp) * wcap;
+    int* hist = reinterpret_cast<int*>(sm + lay.off_hist) + warp * 256;
+    float* wrmin = reinterpret_cast<float*>(sm + lay.off_rmin) + warp * v.m_pad;
+    float* g_scale = reinterpret_cast<float*>(sm + lay.off_group);   // [2][LC]
+    float* g_offset = g_scale + 2 * LC;
+    uint32_t* p_list = reinterpret_cast<uint32_t*>(sm + lay.off_probe);
     uint32_t* p_size = p_list + a.pch;
     uint32_t* p_push = p_size + a.pch;
-    uint32_t* p_itpre = p_push + a.pch;   // np + 1 item prefix (pch + 2 slots)
-    __shared__ int s_next, s_overflow;
-    __shared__ int s_wcount[NW];
+    uint32_t* p_sbpre = p_push + a.pch;   // pch + 1
+    float* qtab = reinterpret_cast<float*>(sm + lay.off_qtab);
+    __shared__ int s_unit, s_overflow;
+    __shared__ int s_next[2];
     __shared__ unsigned long long s_thr;
-    __shared__ uint32_t red[NW];
-
-    const size_t qp = static_cast<size_t>(qi) * a.P;
-    if (tid == 0) {
-        s_next = 0;
-        s_overflow = 0;
-        s_thr = ~0ull;
-    }
-    if (tid < NW) s_wcount[tid] = 0;
-    uint32_t before = 0;
-    for (int p = tid; p < p0; p += NT) before += v.list_size[a.probe[qp + p]];
-    for (int o = 16; o > 0; o >>= 1) before += __shfl_xor_sync(0xffffffffu, before, o);
-    if (lane == 0) red[warp] = before;
-    for (int p = tid; p < np; p += NT) {
-        const uint32_t l = a.probe[qp + p0 + p];
-        p_list[p] = l;
-        p_size[p] = v.list_size[l];
-    }
-    if (v.mode == kModeL2)
-        for (int t = tid; t < v.m * 16; t += NT) qtab[t] = a.qC[static_cast<size_t>(qi) * v.m * 16 + t];
-    if (v.mode == kModeL2Adc)
-        for (int t = tid; t < v.dim; t += NT) qtab[t] = a.q[static_cast<size_t>(qi) * v.dim + t];
-    if (shared_lut) {
-        for (int rr = tid; rr < v.m_pad; rr += NT) lut_all[rr] = a.qlut[static_cast<size_t>(qi) * v.m_pad + rr];
-        for (int p = tid; p < np; p += NT) {
-            p_scale[p] = a.qscale[qi];
-            p_offset[p] = __fadd_rn(a.qoffset[qi], a.pterm[qp + p0 + p]);
-        }
-    }
-    __syncthreads();
-    if (tid == 0) {
-        uint32_t b = 0, it = 0;
-        for (int w = 0; w < NW; ++w) b += red[w];
-        for (int p = 0; p < np; ++p) {
-            p_push[p] = b;
-            b += p_size[p];
-            p_itpre[p] = it;
-            it += (((p_size[p] + kSuperBlock - 1) / kSuperBlock) + kItemSb - 1) / kItemSb;
-        }
-        p_itpre[np] = it;
-    }
-    __syncthreads();
-    const uint32_t total_items = p_itpre[np];
-
-    uint64_t* wbuf = wbuf_all + static_cast<size_t>(warp) * wcap;
-    uint4* wlut = lut_all + (shared_lut ? 0 : static_cast<size_t>(warp) * kItemsPerWarp * v.m_pad);
-    float* wrmin = rmin_all + warp * v.m_pad;
-    float* wscale = wscale_all + warp * kItemsPerWarp;
-    float* woffset = woffset_all + warp * kItemsPerWarp;
-    const unsigned octmask = 0xFFu << (oct * 8);
-
-    // candidate buffer of this warp: trims keep the warp's k' best and lower the block threshold
-    auto warp_trim = [&]() {
-        __syncwarp();
-        const int n = min(s_wcount[warp], wcap);
-        int npow = 2;
-        while (npow < n) npow <<= 1;
-        for (int i = n + lane; i < npow; i += 32) wbuf[i] = ~0ull;
-        warp_sort_keys(wbuf, npow);
-        if (lane == 0) {
-            if (n >= a.kp) atomicMin(&s_thr, static_cast<unsigned long long>(wbuf[a.kp - 1]));
-            s_wcount[warp] = min(n, a.kp);
-        }
-        __syncwarp();
-    };
+    __shared__ int s_wcount[NW];
+    __shared__ uint32_t s_red[NW];
 
     for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = static_cast<uint32_t>(atomicAdd(&s_next, kItemsPerWarp));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= total_items) break;
-        const int nit = static_cast<int>(min(static_cast<uint32_t>(kItemsPerWarp), total_items - base));
-        // this octet's item: probe, superblock range
-        const bool has = oct < nit;
-        const uint32_t item = base + min(oct, nit - 1);
-        const int p = upper_index(p_itpre, np, item);
-        const uint32_t l = p_list[p];
-        const uint32_t nsb_list = (p_size[p] + kSuperBlock - 1) / kSuperBlock;
-        const uint32_t sb0 = (item - p_itpre[p]) * kItemSb;
-        const int cnt = has ? static_cast<int>(min(static_cast<uint32_t>(kItemSb), nsb_list - sb0)) : 0;
-        float scale, offset;
-        const uint4* L;
-        if (shared_lut) {
-            scale = p_scale[p];
-            offset = p_offset[p];
-            L = wlut;
-        } else {
-            // LUTs of the (up to 4) items, built by the whole warp one after another
-            for (int j = 0; j < nit; ++j) {
-                const uint32_t it_j = base + j;
-                const int pj = upper_index(p_itpre, np, it_j);
-                const uint32_t lj = p_list[pj];
-                float s, o;
-                if (v.mode == kModeL2) {
-                    const float A = a.pterm[qp + p0 + pj];
-                    const float* B = v.B + static_cast<size_t>(lj) * v.m * 16;
-                    warp_lut3(
-                        [&](int rr, float* out) {
-                            const float4* b4 = reinterpret_cast<const float4*>(B + rr * 16);
-                            const float4* c4 = reinterpret_cast<const float4*>(qtab + rr * 16);
-#pragma unroll
-                            for (int u = 0; u < 4; ++u) {
-                                const float4 bb = __ldg(b4 + u), cc = c4[u];
-                                out[4 * u + 0] = __fadd_rn(bb.x, cc.x);
-                                out[4 * u + 1] = __fadd_rn(bb.y, cc.y);
-                                out[4 * u + 2] = __fadd_rn(bb.z, cc.z);
-                                out[4 * u + 3] = __fadd_rn(bb.w, cc.w);
-                            }
-                            if (rr == 0) {
-#pragma unroll
-                                for (int jj = 0; jj < 16; ++jj) out[jj] = __fadd_rn(out[jj], A);
-                            }
-                        },
-                        v.m, v.m_pad, wrmin, wlut + static_cast<size_t>(j) * v.m_pad, s, o);
-                } else {
-                    // the residual (q - center) is formed per element inside the table
-                    // loop, as compute_adc_table reads it (reference src/ivf_index.cpp:594-610)
-                    const float* ctr = v.resid + static_cast<size_t>(lj) * v.dim;
-                    warp_lut3(
-                        [&](int rr, float* out) {
-#pragma unroll
-                            for (int jj = 0; jj < 16; ++jj) {
-                                float acc = 0.0f;
-                                for (int u = 0; u < v.sd; ++u) {
-                                    const int e = rr * v.sd + u;
-                                    const float diff = __fsub_rn(__fsub_rn(qtab[e], ctr[e]), v.pq_t[e * 16 + jj]);
-                                    acc = __fmaf_rn(diff, diff, acc);
-                                }
-                                out[jj] = acc;
-                            }
-                        },
-                        v.m, v.m_pad, wrmin, wlut + static_cast<size_t>(j) * v.m_pad, s, o);
+        __syncthreads();   // the previous unit is done with every shared array
+        if (tid == 0) s_unit = atomicAdd(a.work, 1);
+        __syncthreads();
+        const int unit = s_unit;
+        if (unit >= a.nunits) break;
+        const int qi = unit / a.nchunks;
+        const int chunk = unit - qi * a.nchunks;
+        const int p0 = chunk * a.pch;
+        const int np = min(a.nprobe_q ? a.nprobe_q[qi] : a.P, p0 + a.pch) - p0;
+        const size_t ob = static_cast<size_t>(unit) * kp;
+        if (np <= 0) {   // a query whose probes end before this chunk
+            for (int i = tid; i < kp; i += NT) {
+                a.out_key[ob + i] = ~0ull;
+                a.out_slot[ob + i] = 0xFFFFFFFFu;
+            }
+            continue;
+        }
+        const uint64_t* qfilter = a.filters ? a.filters[qi] : a.filter;
+        const size_t qp = static_cast<size_t>(qi) * a.P;
+
+        // ---- the unit's probes, tables and counters ----
+        uint32_t before = 0;   // vectors pushed by the query's earlier chunks
+        for (int p = tid; p < p0; p += NT) before += v.list_size[a.probe[qp + p]];
+        for (int o = 16; o > 0; o >>= 1) before += __shfl_xor_sync(kFull, before, o);
+        if (lane == 0) s_red[warp] = before;
+        for (int p = tid; p < np; p += NT) {
+            const uint32_t l = a.probe[qp + p0 + p];
+            p_list[p] = l;
+            p_size[p] = v.list_size[l];
+        }
+        if (v.mode == kModeL2)
+            for (int t = tid; t < v.m * 16; t += NT) qtab[t] = a.qC[static_cast<size_t>(qi) * v.m * 16 + t];
+        if (v.mode == kModeL2Adc)
+            for (int t = tid; t < v.dim; t += NT) qtab[t] = a.q[static_cast<size_t>(qi) * v.dim + t];
+        if (shared_lut)
+            for (int rr = tid; rr < v.m_pad; rr += NT) lut_ring[rr] = a.qlut[static_cast<size_t>(qi) * v.m_pad + rr];
+        if (tid == 0) {
+            s_overflow = 0;
+            s_thr = ~0ull;
+            s_next[0] = 0;
+            s_next[1] = 0;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            // push offsets and superblock prefix of the unit's probes
+            uint32_t run_push = 0, run_sb = 0;
+            for (int w = 0; w < NW; ++w) run_push += s_red[w];
+            for (int base = 0; base < np; base += 32) {
+                const int p = base + lane;
+                const uint32_t sz = p < np ? p_size[p] : 0;
+                const uint32_t nsb = (sz + kSuperBlock - 1) / kSuperBlock;
+                uint32_t ip = sz, is = nsb;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t1 = __shfl_up_sync(kFull, ip, o), t2 = __shfl_up_sync(kFull, is, o);
+                    if (lane >= o) {
+                        ip += t1;
+                        is += t2;
+                    }
                 }
+                if (p < np) {
+                    p_push[p] = run_push + ip - sz;
+                    p_sbpre[p] = run_sb + is - nsb;
+                }
+                run_push += __shfl_sync(kFull, ip, 31);
+                run_sb += __shfl_sync(kFull, is, 31);
+            }
+            if (lane == 0) p_sbpre[np] = run_sb;
+        }
+
+        // LUTs (or scale / offset) of group g into half g & 1, lists split over the warps
+        auto build_group = [&](int g) {
+            const int h = g & 1, gp0 = g * LC, nc = min(LC, np - gp0);
+            if (tid == 0) s_next[h] = 0;   // its last user, group g - 2, is done
+            for (int j = warp; j < nc; j += NW) {
+                const int p = gp0 + j;
+                if (shared_lut) {
+                    if (lane == 0) {
+                        g_scale[h * LC + j] = a.qscale[qi];
+                        g_offset[h * LC + j] = __fadd_rn(a.qoffset[qi], a.pterm[qp + p0 + p]);
+                    }
+                    continue;
+                }
+                const uint32_t lj = p_list[p];
+                uint4* out = lut_ring + static_cast<size_t>(h * LC + j) * LS;
+                float sc, of;
+                if (v.mode == kModeL2)
+                    warp_lut_l2(v.B + static_cast<size_t>(lj) * v.m * 16, qtab, a.pterm[qp + p0 + p], v.m, v.m_pad,
+                                wrmin, out, &sc, &of);
+                else
+                    warp_lut_adc(v.resid + static_cast<size_t>(lj) * v.dim, qtab, v.pq_t, v.sd, v.m, v.m_pad, wrmin,
+                                 out, &sc, &of);
                 if (lane == 0) {
-                    wscale[j] = s;
-                    woffset[j] = o;
+                    g_scale[h * LC + j] = sc;
+                    g_offset[h * LC + j] = of;
                 }
             }
-            __syncwarp();
-            scale = wscale[min(oct, nit - 1)];
-            offset = woffset[min(oct, nit - 1)];
-            L = wlut + static_cast<size_t>(min(oct, nit - 1)) * v.m_pad;
-        }
-        // the integer limit of this item's list for the current threshold
-        unsigned long long thr_seen = s_thr;
-        int smax = sum_limit_fast(static_cast<uint32_t>(thr_seen >> 32), scale, offset);
-        int maxcnt = cnt;
-        for (int o = 8; o < 32; o <<= 1) maxcnt = max(maxcnt, __shfl_xor_sync(0xffffffffu, maxcnt, o));
-        const uint32_t size = p_size[p], push0 = p_push[p];
-        for (int j = 0; j < maxcnt; ++j) {
-            if (j < cnt) {
-                const unsigned long long thr = s_thr;
-                if (thr != thr_seen) {
-                    thr_seen = thr;
-                    smax = sum_limit_fast(static_cast<uint32_t>(thr >> 32), scale, offset);
-                }
-                const uint32_t sbl = sb0 + j;
-                const size_t sbg = static_cast<size_t>(v.sb_off[l]) + sbl;
+        };
+
+        const int ngroups = (np + LC - 1) / LC;
+        build_group(0);
+        int wcount = 0;   // entries in this warp's buffer (the same in every lane)
+        for (int g = 0; g < ngroups; ++g) {
+            __syncthreads();   // group g's LUTs and the unit's prefix arrays are complete
+            const int h = g & 1, gp0 = g * LC, nc = min(LC, np - gp0);
+            const uint32_t sbb = p_sbpre[gp0], sbe = p_sbpre[gp0 + nc];
+            int cur = -1;   // this octet's current list (index into the unit's probes)
+            uint32_t lst = 0, size = 0, push0 = 0, sb_first = 0, thr_hi = 0;
+            float scale = 1.0f, offset = 0.0f;
+            int smax = 0;
+            const uint4* L = lut_ring;
+            for (;;) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&s_next[h], kSbPerWarp);
+                base = __shfl_sync(kFull, base, 0);
+                if (sbb + static_cast<uint32_t>(base) >= sbe) break;
+                const uint32_t i = sbb + base + oct;
+                const uint64_t thr = *reinterpret_cast<volatile unsigned long long*>(&s_thr);
                 uint32_t sums[8];
-                octet_sums(v.codes + sbg * static_cast<size_t>(2 * v.m_pad), L, v.m_pad, r, sums);
+                uint32_t cmask = 0, sbl = 0;
+                size_t sbg = 0;
+                if (i < sbe) {
+                    const int p = gp0 + upper_index(p_sbpre + gp0, nc, i);
+                    if (p != cur) {
+                        cur = p;
+                        lst = p_list[p];
+                        size = p_size[p];
+                        push0 = p_push[p];
+                        sb_first = p_sbpre[p];
+                        scale = g_scale[h * LC + p - gp0];
+                        offset = g_offset[h * LC + p - gp0];
+                        L = shared_lut ? lut_ring : lut_ring + static_cast<size_t>(h * LC + p - gp0) * LS;
+                        thr_hi = static_cast<uint32_t>(thr >> 32);
+                        smax = sum_limit_fast(thr_hi, scale, offset);
+                    } else if (static_cast<uint32_t>(thr >> 32) != thr_hi) {
+                        thr_hi = static_cast<uint32_t>(thr >> 32);
+                        smax = sum_limit_fast(thr_hi, scale, offset);
+                    }
+                    sbl = i - sb_first;
+                    sbg = static_cast<size_t>(v.sb_off[lst]) + sbl;
+                    octet_sums(v.codes + sbg * static_cast<size_t>(2 * v.m_pad), L, v.m_pad, r, sums);
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const uint32_t pos = sbl * kSuperBlock + 8 * r + i;
-                    if (pos < size && static_cast<int>(sums[i]) <= smax) {
-                        const float dist = fs_dist(sums[i], scale, offset);
-                        const uint64_t key = (static_cast<uint64_t>(float_key(dist)) << 32) | (push0 + pos);
-                        if (key < thr) {
-                            const uint32_t slot = v.ids[sbg * kSuperBlock + 8 * r + i];
-                            const bool ok = qfilter ? ((qfilter[slot >> 6] >> (slot & 63)) & 1ull)
-                                                    : !(v.deleted && ((v.deleted[slot >> 6] >> (slot & 63)) & 1ull));
-                            if (ok) {
-                                const int idx = atomicAdd(&s_wcount[warp], 1);
-                                if (idx < wcap) wbuf[idx] = key;
-                                else s_overflow = 1;
+                    for (int e = 0; e < 8; ++e) {
+                        const uint32_t pos = sbl * kSuperBlock + 8 * r + e;
+                        if (pos < size && static_cast<int>(sums[e]) <= smax) cmask |= 1u << e;
+                    }
+                }
+                if (__any_sync(kFull, cmask != 0)) {
+#pragma unroll 1
+                    for (int e = 0; e < 8; ++e) {
+                        bool want = false;
+                        uint64_t key = 0;
+                        if ((cmask >> e) & 1u) {
+                            const uint32_t pos = sbl * kSuperBlock + 8 * r + e;
+                            const float dist = fs_dist(sums[e], scale, offset);
+                            key = (static_cast<uint64_t>(float_key(dist)) << 32) | (push0 + pos);
+                            if (key < thr) {
+                                const uint32_t slot = v.ids[sbg * kSuperBlock + 8 * r + e];
+                                want = qfilter ? ((qfilter[slot >> 6] >> (slot & 63)) & 1ull)
+                                               : !(v.deleted && ((v.deleted[slot >> 6] >> (slot & 63)) & 1ull));
                             }
                         }
+                        const unsigned bal = __ballot_sync(kFull, want);
+                        if (want) {
+                            const int idx = wcount + __popc(bal & ((1u << lane) - 1));
+                            if (idx < wcap) wbuf[idx] = key;
+                            else s_overflow = 1;
+                        }
+                        wcount += __popc(bal);
+                    }
+                    if (wcount > wcap - kSbPerWarp * kSuperBlock && wcount > kp) {
+                        __syncwarp();
+                        const uint64_t kth = warp_select_keep(wbuf, min(wcount, wcap), kp, hist);
+                        if (lane == 0) atomicMin(&s_thr, static_cast<unsigned long long>(kth));
+                        wcount = kp;
                     }
                 }
             }
-            __syncwarp();
-            if (s_wcount[warp] > wcap - kItemsPerWarp * kSuperBlock) warp_trim();
+            // out of superblocks of group g: build group g + 1 in the other half
+            if (g + 1 < ngroups) build_group(g + 1);
         }
-        (void)octmask;
-    }
-    // ---- merge the warps' lists: each keeps its k' best, then the block sorts them all ----
-    warp_trim();
-    __syncthreads();
-    const int region = NW * wcap;
-    for (int i = tid; i < region; i += NT) {
-        const int w = i / wcap, e = i - w * wcap;
-        if (e >= s_wcount[w]) wbuf_all[i] = ~0ull;
-    }
-    bitonic_sort_keys(wbuf_all, region);
-    int kept = 0;
-    for (int w = 0; w < NW; ++w) kept += s_wcount[w];
-    kept = min(kept, a.kp);
-    const size_t ob = static_cast<size_t>(blockIdx.x) * a.kp;
-    for (int i = tid; i < a.kp; i += NT) {
-        if (i < kept) {
-            const uint64_t key = wbuf_all[i];
-            const uint32_t push = static_cast<uint32_t>(key);
-            const int pp = upper_index(p_push, np, push);
-            const uint32_t pos = push - p_push[pp];
-            const size_t sbg = static_cast<size_t>(v.sb_off[p_list[pp]]) + pos / kSuperBlock;
-            a.out_key[ob + i] = key;
-            a.out_slot[ob + i] = v.ids[sbg * kSuperBlock + pos % kSuperBlock];
-        } else {
-            a.out_key[ob + i] = ~0ull;
-            a.out_slot[ob + i] = 0xFFFFFFFFu;
+
+        // ---- the unit's k' best: each warp's own, gathered, cut to k', sorted ----
+        __syncwarp();
+        if (wcount > kp) {
+            warp_select_keep(wbuf, min(wcount, wcap), kp, hist);
+            wcount = kp;
         }
+        if (lane == 0) s_wcount[warp] = min(wcount, wcap);
+        __syncthreads();   // every warp is done with the LUT ring: gather over it
+        int off = 0, total = 0;
+        for (int w = 0; w < NW; ++w) {
+            if (w < warp) off += s_wcount[w];
+            total += s_wcount[w];
+        }
+        for (int i = lane; i < s_wcount[warp]; i += 32) gath[off + i] = wbuf[i];
+        __syncthreads();
+        if (total > kp) {
+            if (warp == 0) warp_select_keep(gath, total, kp, hist);
+            __syncthreads();
+        }
+        const int kept = min(total, kp);
+        const int ns = next_pow2(kept < 2 ? 2 : kept);
+        for (int i = kept + tid; i < ns; i += NT) gath[i] = ~0ull;
+        bitonic_sort_keys(gath, ns);
+        for (int i = tid; i < kp; i += NT) {
+            if (i < kept) {
+                const uint64_t key = gath[i];
+                const uint32_t push = static_cast<uint32_t>(key);
+                const int pp = upper_index(p_push, np, push);
+                const uint32_t pos = push - p_push[pp];
+                const size_t sbg = static_cast<size_t>(v.sb_off[p_list[pp]]) + pos / kSuperBlock;
+                a.out_key[ob + i] = key;
+                a.out_slot[ob + i] = v.ids[sbg * kSuperBlock + pos % kSuperBlock];
+            } else {
+                a.out_key[ob + i] = ~0ull;
+                a.out_slot[ob + i] = 0xFFFFFFFFu;
+            }
+        }
+        if (tid == 0 && s_overflow) atomicExch(a.err, 1);
     }
-    if (tid == 0 && s_overflow) atomicExch(a.err, 1);
 }
 
-int scan_cap(int kp) { return scan_layout(kp, 4, 0, 1, true, 1).wcap; }
-
 template <int NW>
-static void launch_scan(const ScanArgs& a, size_t smem, unsigned blocks, cudaStream_t st) {
+static void launch_scan(const ScanArgs& a, size_t smem, cudaStream_t st) {
     allow_large_smem<k_scan<NW>>();
+    int per_sm = 0;
+    QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan<NW>, NW * 32, smem));
+    require(per_sm > 0, "fast-scan launch configuration does not fit on the device", kUnsupported);
+    int dev = 0, sms = 0;
+    QG_CUDA(cudaGetDevice(&dev));
+    QG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const unsigned blocks = static_cast<unsigned>(std::min<long long>(a.nunits, static_cast<long long>(per_sm) * sms));
     KernelTimer kt("scan", st);
     k_scan<NW><<<blocks, NW * 32, smem, st>>>(a);
     QG_LAUNCH_CHECK();
@@ -466,12 +590,23 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     nchunks = static_cast<int>(ceil_div(P, pch));
     const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
     const int qtab_len = v.mode == kModeL2 ? v.m * 16 : (v.mode == kModeL2Adc ? v.dim : 0);
-    // warps per block: 8 when the candidate buffers and LUTs fit in ~100 KB, fewer otherwise
-    int nw = 8;
-    while (nw > 1 && scan_layout(kp, v.m_pad, qtab_len, pch, shared_lut, nw).bytes > 100 * 1024) nw >>= 1;
-    const ScanLayout lay = scan_layout(kp, v.m_pad, qtab_len, pch, shared_lut, nw);
-    require(lay.bytes <= 227 * 1024, "fast-scan shared memory exceeds the B200 limit for this m / k * k_factor",
-            kUnsupported);
+    // warps per block and lists per LUT group: the first shape whose shared
+    // memory lets two blocks share an SM, else the first that fits at all
+    static constexpr int kShapes[][2] = {{8, 32}, {8, 16}, {4, 32}, {4, 16}, {8, 8}, {4, 8}, {2, 8}, {2, 4}, {1, 4}, {1, 1}};
+    int nw = 0, lc = 0;
+    for (int pass = 0; pass < 2 && !nw; ++pass) {
+        const size_t limit = pass == 0 ? 110 * 1024 : 226 * 1024;
+        for (const auto& sh : kShapes) {
+            const int lcs = shared_lut ? 64 : sh[1];
+            if (scan_layout(kp, v.m_pad, qtab_len, pch, shared_lut, sh[0], lcs).bytes <= limit) {
+                nw = sh[0];
+                lc = lcs;
+                break;
+            }
+        }
+    }
+    require(nw > 0, "fast-scan shared memory exceeds the B200 limit for this m / k * k_factor", kUnsupported);
+    const ScanLayout lay = scan_layout(kp, v.m_pad, qtab_len, pch, shared_lut, nw, lc);
 
     const bool direct = nchunks == 1;
     const size_t nout = static_cast<size_t>(nq) * nchunks * kp;
@@ -481,6 +616,8 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
         ckey.alloc(nout, st);
         cslot.alloc(nout, st);
     }
+    DevBuf<int> work(1, st);
+    QG_CUDA(cudaMemsetAsync(work.get(), 0, sizeof(int), st));
     ScanArgs a{};
     a.v = v;
     a.q = s.q;
@@ -497,16 +634,17 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     a.pch = pch;
     a.nchunks = nchunks;
     a.kp = kp;
-    a.cap = lay.wcap;
+    a.nunits = nq * nchunks;
+    a.lc = lc;
+    a.work = work.get();
     a.out_key = direct ? out_key : ckey.get();
     a.out_slot = direct ? out_slot : cslot.get();
     a.err = s.d_err;
-    const unsigned blocks = static_cast<unsigned>(nq * nchunks);
     switch (nw) {
-        case 8: launch_scan<8>(a, lay.bytes, blocks, st); break;
-        case 4: launch_scan<4>(a, lay.bytes, blocks, st); break;
-        case 2: launch_scan<2>(a, lay.bytes, blocks, st); break;
-        default: launch_scan<1>(a, lay.bytes, blocks, st); break;
+        case 8: launch_scan<8>(a, lay.bytes, st); break;
+        case 4: launch_scan<4>(a, lay.bytes, st); break;
+        case 2: launch_scan<2>(a, lay.bytes, st); break;
+        default: launch_scan<1>(a, lay.bytes, st); break;
     }
     if (!direct) merge_candidates(ckey.get(), cslot.get(), nq, nchunks, kp, out_key, out_slot, st);
 }

@@ -60,7 +60,10 @@ struct ScanArgs {
     const uint64_t* filter;  // allowed-slot bitmap of every query, or null
     const uint64_t* const* filters;   // per-query bitmaps (overrides filter), or null
     const int* nprobe_q;     // per-query probe count, or null for P each
-    int P, pch, nchunks, kp, cap;
+    int P, pch, nchunks, kp;
+    int nunits;              // nq * nchunks work units (query, chunk of pch probes)
+    int lc;                  // lists per LUT group
+    int* work;               // next unit to take (zero at launch)
     uint64_t* out_key;       // (nq * nchunks) * kp
     uint32_t* out_slot;
     int* err;
@@ -116,6 +119,4 @@ void finalize_ivf(const uint64_t* key, const uint32_t* slot, int nq, int kp, int
 void refine_candidates(const float* q, int nq, int dim, const float* rows, const uint64_t* key, const uint32_t* slot,
                        int kp, int k, bool ip, const int64_t* labels, bool cosine, int64_t* out_ids, float* out_d,
                        cudaStream_t st, const int* kp_q = nullptr, const int* k_q = nullptr);
-int scan_cap(int kp);
-
 } // namespace qg

@@ -439,6 +439,9 @@ def main():
             dist.destroy_process_group()
         return 0
 
+    so = qb.scan_options()["last_shape"]
+    scan_shape = {"warps": so // 1000, "lists_per_group": (so % 1000) // 10, "codes": "staged" if so % 10 else "global",
+                  "autotuned": bool(qb.scan_options()["autotune"])}
     rec = recall(got, gt)
     assert np.array_equal(got, ids_h), "device-resident and host-API results differ"
     alg_bytes = algorithmic_scan_bytes(cfg, index, queries, nprobe, dev)
@@ -459,7 +462,8 @@ def main():
                    "sweep": sel["sweep"], "l2": "flushed between steps (256 MB write)",
                    "parallelism": f"replicas x{world}", "batch_latency_ms": {
                        "p50": round(srt[len(srt) // 2], 4), "p99": round(srt[min(len(srt) - 1, int(0.99 * len(srt)))], 4)},
-                   "kernel_ms_total": {kk: round(v[0], 3) for kk, v in kernel_ms.items() if v[1]}},
+                   "kernel_ms_total": {kk: round(v[0], 3) for kk, v in kernel_ms.items() if v[1]},
+                   "scan_shape": scan_shape},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
                      "kernel": "k_scan", "algorithmic_bytes_per_launch": alg_bytes,

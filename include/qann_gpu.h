@@ -178,7 +178,17 @@ int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, con
  *   the dimension is supported (<= 128). qg_get_option also reads
  *   "tensor_filter_queries" (queries answered through the filter so far) and
  *   "tensor_filter_redone" (those redone exactly after a candidate overflow). No counterpart in the reference, whose
- *   exact scores always come from its CPU distance kernels (reference src/flat_index.cpp:33-64). */
+ *   exact scores always come from its CPU distance kernels (reference src/flat_index.cpp:33-64).
+ * "scan_autotune": 1 (default) times the fast-scan kernel's candidate shapes
+ *   (warps per block, lists per LUT group, codes read from global memory or
+ *   staged through shared memory by bulk copies) on the first large search of
+ *   each problem (scoring mode, m, k', nprobe, batch size) and keeps the
+ *   fastest; 0 uses the first shape. "scan_variant": -1 (default) any shape,
+ *   0 only unstaged, 1 only staged. qg_get_option also reads
+ *   "scan_tuned_shapes" (problems tuned so far) and "scan_last_shape" (the
+ *   last scan's shape: warps * 1000 + lists per group * 10 + staged). Results are the same under
+ *   every shape. No counterpart in the reference, whose scan kernel is fixed
+ *   (reference src/fast_scan.cpp:306-338). */
 int qg_set_option(const char* key, int64_t value);
 int qg_get_option(const char* key, int64_t* value);
 

@@ -101,6 +101,26 @@ def tensor_filter_counts() -> dict:
     return out
 
 
+def set_scan_options(autotune: bool | None = None, variant: int | None = None) -> None:
+    """Fast-scan kernel shapes. autotune: time the candidate shapes on the
+    first large search of each problem and keep the fastest (default on).
+    variant: -1 any shape, 0 codes read from global memory, 1 codes staged
+    through shared memory by bulk copies. Results are identical under every shape."""
+    if autotune is not None:
+        check(_lib.lib.qg_set_option(b"scan_autotune", int(bool(autotune))))
+    if variant is not None:
+        check(_lib.lib.qg_set_option(b"scan_variant", int(variant)))
+
+
+def scan_options() -> dict:
+    out = {}
+    for key in ("autotune", "variant", "tuned_shapes", "last_shape"):
+        v = C.c_int64()
+        check(_lib.lib.qg_get_option(f"scan_{key}".encode(), C.byref(v)))
+        out[key] = v.value
+    return out
+
+
 class DenseIndex:
     """An index of dense float32 vectors. Not constructed directly."""
 
@@ -110,8 +130,9 @@ class DenseIndex:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            _lib.lib.qg_free(h)
+        lib = getattr(_lib, "lib", None) if _lib is not None else None
+        if h is not None and h.value and lib is not None:   # (module globals may be gone at interpreter exit)
+            lib.qg_free(h)
             self._h = None
 
     # -- properties -----------------------------------------------------------------

@@ -520,6 +520,12 @@ int qg_set_option(const char* key, int64_t value) {
         if (k == "tensor_filter") {
             require(value >= 0 && value <= 2, "tensor_filter must be 0, 1 or 2");
             set_tensor_filter(static_cast<int>(value));
+        } else if (k == "scan_autotune") {
+            require(value == 0 || value == 1, "scan_autotune must be 0 or 1");
+            set_scan_autotune(static_cast<int>(value));
+        } else if (k == "scan_variant") {
+            require(value >= -1 && value <= 1, "scan_variant must be -1, 0 or 1");
+            set_scan_variant(static_cast<int>(value));
         } else {
             throw Error(kInvalidArgument, "unknown option: " + k);
         }
@@ -535,6 +541,10 @@ int qg_get_option(const char* key, int64_t* value) {
         if (k == "tensor_filter") *value = tensor_filter();
         else if (k == "tensor_filter_queries") *value = queries;
         else if (k == "tensor_filter_redone") *value = redone;
+        else if (k == "scan_autotune") *value = scan_autotune();
+        else if (k == "scan_variant") *value = scan_variant();
+        else if (k == "scan_tuned_shapes") *value = scan_tuned_shapes();
+        else if (k == "scan_last_shape") *value = scan_last_shape();
         else throw Error(kInvalidArgument, "unknown option: " + k);
     });
 }

@@ -221,16 +221,20 @@ __device__ __forceinline__ void octet_sums(const uint4* __restrict__ sb, const u
                                            int r, uint32_t sums[8]) {
     uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
     const int nq = m_pad >> 2;
+    // two 16-byte code words in use and the next two in flight
+    const uint4 zero = make_uint4(0, 0, 0, 0);
+    uint4 c0 = nq > 0 ? __ldg(sb + r) : zero;
+    uint4 c1 = nq > 1 ? __ldg(sb + 8 + r) : zero;
     int q = 0;
-    // four 16-byte code loads in flight before their lookups
-    for (; q + 4 <= nq; q += 4) {
-        uint4 w[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) w[u] = __ldg(sb + (q + u) * 8 + r);
-#pragma unroll
-        for (int u = 0; u < 4; ++u) octet_step(w[u], lut + 4 * (q + u), a0, b0, a1, b1);
+    for (; q + 2 <= nq; q += 2) {
+        const uint4 n0 = q + 2 < nq ? __ldg(sb + (q + 2) * 8 + r) : zero;
+        const uint4 n1 = q + 3 < nq ? __ldg(sb + (q + 3) * 8 + r) : zero;
+        octet_step(c0, lut + 4 * q, a0, b0, a1, b1);
+        octet_step(c1, lut + 4 * (q + 1), a0, b0, a1, b1);
+        c0 = n0;
+        c1 = n1;
     }
-    for (; q < nq; ++q) octet_step(__ldg(sb + q * 8 + r), lut + 4 * q, a0, b0, a1, b1);
+    if (q < nq) octet_step(c0, lut + 4 * q, a0, b0, a1, b1);
     sums[0] = a0 & 0xFFFFu;
     sums[1] = b0 & 0xFFFFu;
     sums[2] = a0 >> 16;

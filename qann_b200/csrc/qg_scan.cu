@@ -28,14 +28,22 @@
 // index.
 #include "qg_device.cuh"
 #include "qg_search.h"
+#include "qg_sm100.cuh"
 
 #include <algorithm>
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace qg {
 
 namespace {
 constexpr int kMaxChunk = 256;   // probes per work unit at most
 constexpr int kSbPerWarp = 4;    // superblocks a warp takes at a time, one per octet
+// Row stride (floats) of the query's table C in shared memory: 80 bytes puts
+// the 16-byte reads of 8 lanes (one row each) on distinct banks.
+constexpr int kQtabStride = 20;
 }
 
 // The 16 entries of LUT rows rounded and packed: round-half-even of
@@ -52,17 +60,15 @@ __device__ __forceinline__ uint4 round_row(const float* v, float mn, float scale
                       prmt(prmt(b[12], b[13], 0x0040), prmt(b[14], b[15], 0x0040), 0x5410));
 }
 
-// LUT of one list by one warp. Same arithmetic as quantize_lut; the rows are
-// formed twice (for their ranges, then for rounding) rather than held in
-// registers across the warp-wide reductions.
+// LUT of one list by one warp. Same arithmetic as quantize_lut; each lane
+// forms its rows twice (for their ranges, then for rounding) rather than
+// holding them in registers across the warp-wide reductions.
 template <class RowFn>
 __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* row_min, uint4* lut_out, float& scale_out,
                                           float& offset_out) {
     const int lane = threadIdx.x & 31;
     float widest = 0.0f;
-    for (int r = lane; r < m; r += 32) {
-        float v[16];
-        row(r, v);
+    auto ranges = [&](int r, const float* v) {
         float lo = v[0], hi = v[0];
 #pragma unroll
         for (int j = 1; j < 16; ++j) {
@@ -72,6 +78,11 @@ __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* ro
         row_min[r] = lo;
         const float w = __fsub_rn(hi, lo);
         widest = widest < w ? w : widest;
+    };
+    float v0[16];
+    for (int r = lane; r < m; r += 32) {
+        row(r, v0);
+        ranges(r, v0);
     }
     widest = warp_max(widest);
     __syncwarp();
@@ -83,9 +94,8 @@ __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* ro
     const float offset = __fadd_rn(__fadd_rn(p0, p1), __fadd_rn(p2, p3));
     const float scale = widest > 0.0f ? __fdiv_rn(static_cast<float>(kLutMax), widest) : 1.0f;
     for (int r = lane; r < m; r += 32) {
-        float v[16];
-        row(r, v);
-        lut_out[r] = round_row(v, row_min[r], scale);
+        row(r, v0);
+        lut_out[r] = round_row(v0, row_min[r], scale);
     }
     for (int r = m + lane; r < m_pad; r += 32) lut_out[r] = make_uint4(0, 0, 0, 0);
     scale_out = scale;
@@ -101,7 +111,7 @@ __device__ __noinline__ void warp_lut_l2(const float* __restrict__ B, const floa
     warp_lut3(
         [&](int rr, float* o) {
             const float4* b4 = reinterpret_cast<const float4*>(B + rr * 16);
-            const float4* c4 = reinterpret_cast<const float4*>(qtab + rr * 16);
+            const float4* c4 = reinterpret_cast<const float4*>(qtab + rr * kQtabStride);
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const float4 bb = __ldg(b4 + u), cc = c4[u];
@@ -143,6 +153,28 @@ __device__ __noinline__ void warp_lut_adc(const float* __restrict__ ctr, const f
         m, m_pad, row_min, lut_out, sc, of);
     *scale_out = sc;
     *offset_out = of;
+}
+
+// octet_sums over a superblock staged in shared memory.
+__device__ __forceinline__ void octet_sums_shared(const uint4* sb, const uint4* __restrict__ lut, int m_pad, int r,
+                                                  uint32_t sums[8]) {
+    uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+    const int nq = m_pad >> 2;
+    int q = 0;
+    for (; q + 2 <= nq; q += 2) {
+        const uint4 w0 = sb[q * 8 + r], w1 = sb[(q + 1) * 8 + r];
+        octet_step(w0, lut + 4 * q, a0, b0, a1, b1);
+        octet_step(w1, lut + 4 * (q + 1), a0, b0, a1, b1);
+    }
+    if (q < nq) octet_step(sb[q * 8 + r], lut + 4 * q, a0, b0, a1, b1);
+    sums[0] = a0 & 0xFFFFu;
+    sums[1] = b0 & 0xFFFFu;
+    sums[2] = a0 >> 16;
+    sums[3] = b0 >> 16;
+    sums[4] = a1 & 0xFFFFu;
+    sums[5] = b1 & 0xFFFFu;
+    sums[6] = a1 >> 16;
+    sums[7] = b1 >> 16;
 }
 
 __device__ __forceinline__ int upper_index(const uint32_t* pre, int n, uint32_t x) {
@@ -246,13 +278,13 @@ __device__ __noinline__ uint64_t warp_select_keep(uint64_t* buf, int n, int keep
 struct ScanLayout {
     int nw, lc, wcap, lut_stride;   // lut_stride: uint4s per LUT (m_pad + 2: 32 bytes keep
                                     // consecutive LUTs of a warp's octets on distinct banks)
-    size_t off_wbuf, off_hist, off_rmin, off_group, off_probe, off_qtab, bytes;
+    size_t off_wbuf, off_hist, off_rmin, off_group, off_probe, off_qtab, off_stage, off_cbar, bytes;
 };
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~static_cast<size_t>(15); }
 
 __host__ __device__ inline ScanLayout scan_layout(int kp, int m_pad, int qtab_len, int pch, bool shared_lut, int nw,
-                                                  int lc) {
+                                                  int lc, bool staged) {
     ScanLayout L;
     L.nw = nw;
     L.lc = lc;
@@ -271,16 +303,21 @@ __host__ __device__ inline ScanLayout scan_layout(int kp, int m_pad, int qtab_le
     L.off_group = b;
     b += static_cast<size_t>(2) * lc * 8;                         // scale, offset of both halves
     L.off_probe = b;
-    b += static_cast<size_t>(pch) * 12 + static_cast<size_t>(pch + 1) * 4;   // list, size, push, superblock prefix
+    b += static_cast<size_t>(pch) * 16 + static_cast<size_t>(pch + 1) * 4;   // list, size, push, first superblock, prefix
     b = align16(b);
     L.off_qtab = b;
     b += static_cast<size_t>(qtab_len) * 4;
+    b = (b + 127) & ~static_cast<size_t>(127);
+    L.off_stage = b;   // staged: per warp, two stages of kSbPerWarp superblocks
+    b += staged ? static_cast<size_t>(nw) * 2 * kSbPerWarp * m_pad * 32 : 0;
+    L.off_cbar = b;    // staged: per warp, one mbarrier per stage
+    b += staged ? static_cast<size_t>(nw) * 2 * 8 : 0;
     L.bytes = align16(b);
     return L;
 }
 
-template <int NW>
-__global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
+template <int NW, bool kStaged>
+__global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
     extern __shared__ __align__(16) uint8_t sm[];
     constexpr int NT = NW * 32;
     constexpr unsigned kFull = 0xffffffffu;
@@ -288,9 +325,14 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int oct = lane >> 3, r = lane & 7;
     const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
-    const int qtab_len = v.mode == kModeL2 ? v.m * 16 : (v.mode == kModeL2Adc ? v.dim : 0);
-    const ScanLayout lay = scan_layout(a.kp, v.m_pad, qtab_len, a.pch, shared_lut, NW, a.lc);
+    const int qtab_len = v.mode == kModeL2 ? v.m * kQtabStride : (v.mode == kModeL2Adc ? v.dim : 0);
+    const ScanLayout lay = scan_layout(a.kp, v.m_pad, qtab_len, a.pch, shared_lut, NW, a.lc, kStaged);
     const int wcap = lay.wcap, LC = lay.lc, LS = lay.lut_stride, kp = a.kp;
+    const uint32_t sb_bytes = static_cast<uint32_t>(v.m_pad) * 32;   // one superblock of codes
+    uint8_t* cstage = sm + lay.off_stage + static_cast<size_t>(warp) * 2 * kSbPerWarp * sb_bytes;
+    uint64_t* cbar = reinterpret_cast<uint64_t*>(sm + lay.off_cbar) + 2 * warp;
+    int cst = 0;         // stage the next take fills
+    uint32_t cpar = 0;   // bit s: parity of stage s's next completion
 
     uint4* lut_ring = reinterpret_cast<uint4*>(sm);
     uint64_t* gath = reinterpret_cast<uint64_t*>(sm);
@@ -302,14 +344,21 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
     uint32_t* p_list = reinterpret_cast<uint32_t*>(sm + lay.off_probe);
     uint32_t* p_size = p_list + a.pch;
     uint32_t* p_push = p_size + a.pch;
-    uint32_t* p_sbpre = p_push + a.pch;   // pch + 1
+    uint32_t* p_sboff = p_push + a.pch;   // each probe's first superblock in the code array
+    uint32_t* p_sbpre = p_sboff + a.pch;  // pch + 1
     float* qtab = reinterpret_cast<float*>(sm + lay.off_qtab);
-    __shared__ int s_unit, s_overflow;
-    __shared__ int s_next[2];
+    __shared__ int s_unit, s_overflow, s_abort;
+    __shared__ int s_next[2], s_build[2];
     __shared__ unsigned long long s_thr;
     __shared__ int s_wcount[NW];
     __shared__ uint32_t s_red[NW];
 
+    if (tid == 0) s_abort = 0;
+    if (kStaged && lane == 0) {
+        sm100::mbar_init(&cbar[0], 1);
+        sm100::mbar_init(&cbar[1], 1);
+        sm100::fence_barrier_init();
+    }
     for (;;) {
         __syncthreads();   // the previous unit is done with every shared array
         if (tid == 0) s_unit = atomicAdd(a.work, 1);
@@ -340,9 +389,11 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
             const uint32_t l = a.probe[qp + p0 + p];
             p_list[p] = l;
             p_size[p] = v.list_size[l];
+            p_sboff[p] = v.sb_off[l];
         }
         if (v.mode == kModeL2)
-            for (int t = tid; t < v.m * 16; t += NT) qtab[t] = a.qC[static_cast<size_t>(qi) * v.m * 16 + t];
+            for (int t = tid; t < v.m * 16; t += NT)
+                qtab[(t >> 4) * kQtabStride + (t & 15)] = a.qC[static_cast<size_t>(qi) * v.m * 16 + t];
         if (v.mode == kModeL2Adc)
             for (int t = tid; t < v.dim; t += NT) qtab[t] = a.q[static_cast<size_t>(qi) * v.dim + t];
         if (shared_lut)
@@ -352,6 +403,7 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
             s_thr = ~0ull;
             s_next[0] = 0;
             s_next[1] = 0;
+            s_build[0] = 0;
         }
         __syncthreads();
         if (warp == 0) {
@@ -380,11 +432,20 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
             if (lane == 0) p_sbpre[np] = run_sb;
         }
 
-        // LUTs (or scale / offset) of group g into half g & 1, lists split over the warps
+        // LUTs (or scale / offset) of group g into half g & 1. Warps take the
+        // lists from a counter, so warps that finish scanning group g - 1 early
+        // build more of them.
         auto build_group = [&](int g) {
             const int h = g & 1, gp0 = g * LC, nc = min(LC, np - gp0);
-            if (tid == 0) s_next[h] = 0;   // its last user, group g - 2, is done
-            for (int j = warp; j < nc; j += NW) {
+            if (tid == 0) {
+                s_next[h] = 0;        // its last user, group g - 2, is done
+                s_build[h ^ 1] = 0;   // group g + 1's; its last user, group g - 1, is done
+            }
+            for (;;) {
+                int j = 0;
+                if (lane == 0) j = atomicAdd(&s_build[h], 1);
+                j = __shfl_sync(kFull, j, 0);
+                if (j >= nc) break;
                 const int p = gp0 + j;
                 if (shared_lut) {
                     if (lane == 0) {
@@ -417,25 +478,44 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
             const int h = g & 1, gp0 = g * LC, nc = min(LC, np - gp0);
             const uint32_t sbb = p_sbpre[gp0], sbe = p_sbpre[gp0 + nc];
             int cur = -1;   // this octet's current list (index into the unit's probes)
-            uint32_t lst = 0, size = 0, push0 = 0, sb_first = 0, thr_hi = 0;
+            uint32_t list_sb = 0, size = 0, push0 = 0, sb_first = 0, thr_hi = 0;
             float scale = 1.0f, offset = 0.0f;
             int smax = 0;
             const uint4* L = lut_ring;
-            for (;;) {
+            // A take: the warp's next kSbPerWarp superblocks of the group, one per
+            // octet: ti (valid while < sbe) and its probe tp. Staged, the octets'
+            // leaders start bulk copies of the taken superblocks into stage `cst`.
+            auto take = [&](uint32_t& ti, int& tp) -> bool {
                 int base = 0;
                 if (lane == 0) base = atomicAdd(&s_next[h], kSbPerWarp);
                 base = __shfl_sync(kFull, base, 0);
-                if (sbb + static_cast<uint32_t>(base) >= sbe) break;
-                const uint32_t i = sbb + base + oct;
+                if (sbb + static_cast<uint32_t>(base) >= sbe) return false;
+                ti = sbb + base + oct;
+                tp = ti < sbe ? gp0 + upper_index(p_sbpre + gp0, nc, ti) : -1;
+                if constexpr (kStaged) {
+                    const uint32_t nvalid = min(static_cast<uint32_t>(kSbPerWarp), sbe - (sbb + base));
+                    if (lane == 0) sm100::mbar_expect_tx(&cbar[cst], nvalid * sb_bytes);
+                    __syncwarp();
+                    if (r == 0 && tp >= 0) {
+                        const size_t sbg = static_cast<size_t>(p_sboff[tp]) + (ti - p_sbpre[tp]);
+                        sm100::bulk_load(cstage + static_cast<size_t>(cst * kSbPerWarp + oct) * sb_bytes,
+                                         v.codes + sbg * static_cast<size_t>(2 * v.m_pad), sb_bytes, &cbar[cst]);
+                    }
+                    cst ^= 1;
+                }
+                return true;
+            };
+            // The sums of take (i, p) and its candidates; codes from `src` (the
+            // stage in shared memory, or global memory).
+            auto process = [&](uint32_t i, int p, int stage) {
                 const uint64_t thr = *reinterpret_cast<volatile unsigned long long*>(&s_thr);
                 uint32_t sums[8];
                 uint32_t cmask = 0, sbl = 0;
                 size_t sbg = 0;
-                if (i < sbe) {
-                    const int p = gp0 + upper_index(p_sbpre + gp0, nc, i);
+                if (p >= 0) {
                     if (p != cur) {
                         cur = p;
-                        lst = p_list[p];
+                        list_sb = p_sboff[p];
                         size = p_size[p];
                         push0 = p_push[p];
                         sb_first = p_sbpre[p];
@@ -449,8 +529,13 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
                         smax = sum_limit_fast(thr_hi, scale, offset);
                     }
                     sbl = i - sb_first;
-                    sbg = static_cast<size_t>(v.sb_off[lst]) + sbl;
-                    octet_sums(v.codes + sbg * static_cast<size_t>(2 * v.m_pad), L, v.m_pad, r, sums);
+                    sbg = static_cast<size_t>(list_sb) + sbl;
+                    if constexpr (kStaged)
+                        octet_sums_shared(reinterpret_cast<const uint4*>(
+                                              cstage + static_cast<size_t>(stage * kSbPerWarp + oct) * sb_bytes),
+                                          L, v.m_pad, r, sums);
+                    else
+                        octet_sums(v.codes + sbg * static_cast<size_t>(2 * v.m_pad), L, v.m_pad, r, sums);
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
                         const uint32_t pos = sbl * kSuperBlock + 8 * r + e;
@@ -458,34 +543,83 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
                     }
                 }
                 if (__any_sync(kFull, cmask != 0)) {
-#pragma unroll 1
+                    // keys of this lane's passing vectors; slots (and their filter
+                    // or deletion bits) are read only when a filter or deletions
+                    // exist, all loads of the lane in flight together
+                    uint64_t keys[8];
+                    uint32_t kmask = 0;
+#pragma unroll
                     for (int e = 0; e < 8; ++e) {
-                        bool want = false;
-                        uint64_t key = 0;
+                        keys[e] = ~0ull;
                         if ((cmask >> e) & 1u) {
                             const uint32_t pos = sbl * kSuperBlock + 8 * r + e;
                             const float dist = fs_dist(sums[e], scale, offset);
-                            key = (static_cast<uint64_t>(float_key(dist)) << 32) | (push0 + pos);
-                            if (key < thr) {
-                                const uint32_t slot = v.ids[sbg * kSuperBlock + 8 * r + e];
-                                want = qfilter ? ((qfilter[slot >> 6] >> (slot & 63)) & 1ull)
-                                               : !(v.deleted && ((v.deleted[slot >> 6] >> (slot & 63)) & 1ull));
-                            }
+                            keys[e] = (static_cast<uint64_t>(float_key(dist)) << 32) | (push0 + pos);
+                            if (keys[e] < thr) kmask |= 1u << e;
                         }
-                        const unsigned bal = __ballot_sync(kFull, want);
-                        if (want) {
-                            const int idx = wcount + __popc(bal & ((1u << lane) - 1));
-                            if (idx < wcap) wbuf[idx] = key;
-                            else s_overflow = 1;
-                        }
-                        wcount += __popc(bal);
                     }
+                    const uint64_t* bits = qfilter ? qfilter : v.deleted;
+                    if (bits && kmask) {
+                        uint32_t slot[8];
+#pragma unroll
+                        for (int e = 0; e < 8; ++e)
+                            slot[e] = (kmask >> e) & 1u ? v.ids[sbg * kSuperBlock + 8 * r + e] : 0u;
+                        uint64_t word[8];
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) word[e] = (kmask >> e) & 1u ? bits[slot[e] >> 6] : 0ull;
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) {
+                            const bool set = (word[e] >> (slot[e] & 63)) & 1ull;
+                            // a filter lists the allowed slots; the deletion bitmap the removed ones
+                            if (set != (qfilter != nullptr)) kmask &= ~(1u << e);
+                        }
+                    }
+                    // append: this lane's keys after those of the lanes below it
+                    const int mine = __popc(kmask);
+                    int incl = mine;
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int t = __shfl_up_sync(kFull, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    int idx = wcount + incl - mine;
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        if ((kmask >> e) & 1u) {
+                            if (idx < wcap) wbuf[idx] = keys[e];
+                            else s_overflow = 1;
+                            ++idx;
+                        }
+                    }
+                    wcount += __shfl_sync(kFull, incl, 31);
                     if (wcount > wcap - kSbPerWarp * kSuperBlock && wcount > kp) {
                         __syncwarp();
                         const uint64_t kth = warp_select_keep(wbuf, min(wcount, wcap), kp, hist);
                         if (lane == 0) atomicMin(&s_thr, static_cast<unsigned long long>(kth));
                         wcount = kp;
                     }
+                }
+            };
+            uint32_t i0 = 0, i1 = 0;
+            int q0 = -1, q1 = -1;
+            int s0 = cst;
+            bool v0 = take(i0, q0);
+            while (v0) {
+                if constexpr (kStaged) {
+                    const bool v1 = take(i1, q1);   // the next take's copies overlap this one's sums
+                    if (!sm100::mbar_wait(&cbar[s0], (cpar >> s0) & 1u, &s_abort)) {
+                        s_abort = 1;
+                        atomicExch(a.err, 2);
+                    }
+                    cpar ^= 1u << s0;
+                    process(i0, q0, s0);
+                    __syncwarp();   // stage s0 is free again
+                    s0 ^= 1;
+                    i0 = i1;
+                    q0 = q1;
+                    v0 = v1;
+                } else {
+                    process(i0, q0, 0);
+                    v0 = take(i0, q0);
                 }
             }
             // out of superblocks of group g: build group g + 1 in the other half
@@ -521,7 +655,7 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
                 const uint32_t push = static_cast<uint32_t>(key);
                 const int pp = upper_index(p_push, np, push);
                 const uint32_t pos = push - p_push[pp];
-                const size_t sbg = static_cast<size_t>(v.sb_off[p_list[pp]]) + pos / kSuperBlock;
+                const size_t sbg = static_cast<size_t>(p_sboff[pp]) + pos / kSuperBlock;
                 a.out_key[ob + i] = key;
                 a.out_slot[ob + i] = v.ids[sbg * kSuperBlock + pos % kSuperBlock];
             } else {
@@ -533,19 +667,114 @@ __global__ void __launch_bounds__(NW * 32, 2) k_scan(ScanArgs a) {
     }
 }
 
-template <int NW>
+template <int NW, bool kStaged>
 static void launch_scan(const ScanArgs& a, size_t smem, cudaStream_t st) {
-    allow_large_smem<k_scan<NW>>();
+    allow_large_smem<k_scan<NW, kStaged>>();
     int per_sm = 0;
-    QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan<NW>, NW * 32, smem));
+    QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan<NW, kStaged>, NW * 32, smem));
     require(per_sm > 0, "fast-scan launch configuration does not fit on the device", kUnsupported);
-    int dev = 0, sms = 0;
-    QG_CUDA(cudaGetDevice(&dev));
-    QG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const unsigned blocks = static_cast<unsigned>(std::min<long long>(a.nunits, static_cast<long long>(per_sm) * sms));
+    const unsigned blocks = static_cast<unsigned>(std::min<long long>(a.nunits, static_cast<long long>(per_sm) * sm_count()));
     KernelTimer kt("scan", st);
-    k_scan<NW><<<blocks, NW * 32, smem, st>>>(a);
+    k_scan<NW, kStaged><<<blocks, NW * 32, smem, st>>>(a);
     QG_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Scan shapes and their autotuner. A shape is (warps per block, lists per LUT
+// group, codes read from global memory or staged through shared memory by
+// bulk copies). Every shape gives the same results; the autotuner times the
+// candidates on the first large search of each problem key and keeps the
+// fastest for the rest of the process.
+// ---------------------------------------------------------------------------
+namespace {
+struct ScanShape {
+    int nw = 0, lc = 0;
+    bool staged = false;
+};
+
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int, int>, ScanShape> g_tuned;   // (mode, m_pad, kp, P, log2 nq, variant) -> shape
+std::atomic<int> g_autotune{1};    // 0: the first fitting unstaged shape, 1: tune
+std::atomic<int> g_force{-1};      // -1: any; 0: unstaged only; 1: staged only
+std::atomic<int> g_last_shape{0};  // the last scan's shape: warps * 1000 + lists per group * 10 + staged
+}
+
+void set_scan_autotune(int on) { g_autotune.store(on); }
+int scan_autotune() { return g_autotune.load(); }
+void set_scan_variant(int v) { g_force.store(v); }
+int scan_variant() { return g_force.load(); }
+int scan_last_shape() { return g_last_shape.load(); }
+int scan_tuned_shapes() {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    return static_cast<int>(g_tuned.size());
+}
+
+// Candidate shapes whose shared memory fits: unstaged ones for two blocks per
+// SM, staged ones for one.
+static std::vector<ScanShape> scan_shapes(int kp, int m_pad, int qtab_len, int pch, bool shared_lut) {
+    static constexpr int kUnstaged[][2] = {{8, 32}, {8, 16}, {4, 32}, {4, 16}, {8, 8}, {4, 8}, {2, 8}, {2, 4}, {1, 4}, {1, 1}};
+    static constexpr int kStagedShapes[][2] = {{8, 16}, {8, 8}, {4, 32}, {4, 16}, {4, 8}};
+    std::vector<ScanShape> out;
+    const int force = g_force.load();
+    auto first_fit = [&](const auto& table, bool staged, size_t limit) {
+        for (const auto& sh : table) {
+            const int lc = shared_lut ? 64 : sh[1];
+            if (scan_layout(kp, m_pad, qtab_len, pch, shared_lut, sh[0], lc, staged).bytes <= limit) {
+                out.push_back({sh[0], lc, staged});
+                return true;
+            }
+        }
+        return false;
+    };
+    if (force != 1 && !first_fit(kUnstaged, false, 110 * 1024)) first_fit(kUnstaged, false, 226 * 1024);
+    if (force != 0) first_fit(kStagedShapes, true, 226 * 1024);
+    return out;
+}
+
+static void run_scan(const ScanShape& sh, ScanArgs a, const IvfView& v, int qtab_len, cudaStream_t st) {
+    const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
+    a.lc = sh.lc;
+    const size_t smem = scan_layout(a.kp, v.m_pad, qtab_len, a.pch, shared_lut, sh.nw, sh.lc, sh.staged).bytes;
+    QG_CUDA(cudaMemsetAsync(a.work, 0, sizeof(int), st));
+    if (sh.staged) {
+        switch (sh.nw) {
+            case 8: launch_scan<8, true>(a, smem, st); break;
+            default: launch_scan<4, true>(a, smem, st); break;
+        }
+    } else {
+        switch (sh.nw) {
+            case 8: launch_scan<8, false>(a, smem, st); break;
+            case 4: launch_scan<4, false>(a, smem, st); break;
+            case 2: launch_scan<2, false>(a, smem, st); break;
+            default: launch_scan<1, false>(a, smem, st); break;
+        }
+    }
+}
+
+// Times each candidate once on this search's own inputs (its outputs are
+// the same every time) and returns the fastest.
+static ScanShape tune_scan(const std::vector<ScanShape>& cands, const ScanArgs& a, const IvfView& v, int qtab_len,
+                           cudaStream_t st) {
+    cudaEvent_t e0, e1;
+    QG_CUDA(cudaEventCreate(&e0));
+    QG_CUDA(cudaEventCreate(&e1));
+    ScanShape best = cands.front();
+    float best_ms = 0.0f;
+    for (size_t c = 0; c < cands.size(); ++c) {
+        QG_CUDA(cudaEventRecord(e0, st));
+        run_scan(cands[c], a, v, qtab_len, st);
+        QG_CUDA(cudaEventRecord(e1, st));
+        QG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (c == 0 || ms < best_ms) {
+            best_ms = ms;
+            best = cands[c];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
 }
 
 void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st) {
@@ -589,24 +818,9 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     const int pch = static_cast<int>(ceil_div(P, nchunks));
     nchunks = static_cast<int>(ceil_div(P, pch));
     const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
-    const int qtab_len = v.mode == kModeL2 ? v.m * 16 : (v.mode == kModeL2Adc ? v.dim : 0);
-    // warps per block and lists per LUT group: the first shape whose shared
-    // memory lets two blocks share an SM, else the first that fits at all
-    static constexpr int kShapes[][2] = {{8, 32}, {8, 16}, {4, 32}, {4, 16}, {8, 8}, {4, 8}, {2, 8}, {2, 4}, {1, 4}, {1, 1}};
-    int nw = 0, lc = 0;
-    for (int pass = 0; pass < 2 && !nw; ++pass) {
-        const size_t limit = pass == 0 ? 110 * 1024 : 226 * 1024;
-        for (const auto& sh : kShapes) {
-            const int lcs = shared_lut ? 64 : sh[1];
-            if (scan_layout(kp, v.m_pad, qtab_len, pch, shared_lut, sh[0], lcs).bytes <= limit) {
-                nw = sh[0];
-                lc = lcs;
-                break;
-            }
-        }
-    }
-    require(nw > 0, "fast-scan shared memory exceeds the B200 limit for this m / k * k_factor", kUnsupported);
-    const ScanLayout lay = scan_layout(kp, v.m_pad, qtab_len, pch, shared_lut, nw, lc);
+    const int qtab_len = v.mode == kModeL2 ? v.m * kQtabStride : (v.mode == kModeL2Adc ? v.dim : 0);
+    const std::vector<ScanShape> cands = scan_shapes(kp, v.m_pad, qtab_len, pch, shared_lut);
+    require(!cands.empty(), "fast-scan shared memory exceeds the B200 limit for this m / k * k_factor", kUnsupported);
 
     const bool direct = nchunks == 1;
     const size_t nout = static_cast<size_t>(nq) * nchunks * kp;
@@ -635,17 +849,32 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     a.nchunks = nchunks;
     a.kp = kp;
     a.nunits = nq * nchunks;
-    a.lc = lc;
     a.work = work.get();
     a.out_key = direct ? out_key : ckey.get();
     a.out_slot = direct ? out_slot : cslot.get();
     a.err = s.d_err;
-    switch (nw) {
-        case 8: launch_scan<8>(a, lay.bytes, st); break;
-        case 4: launch_scan<4>(a, lay.bytes, st); break;
-        case 2: launch_scan<2>(a, lay.bytes, st); break;
-        default: launch_scan<1>(a, lay.bytes, st); break;
+    // the shape: tuned once per problem key on a search large enough to fill
+    // the GPU several times over, else the first candidate
+    const int nq_bucket = 31 - __builtin_clz(static_cast<unsigned>(std::max(1, nq)));
+    const auto key = std::make_tuple(v.mode, v.m_pad, kp, P, nq_bucket, g_force.load());
+    ScanShape shape = cands.front();
+    bool tuned = !g_autotune.load();
+    if (!tuned) {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        const auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            shape = it->second;
+            tuned = true;
+        }
     }
+    const bool big = static_cast<long long>(nq) * P >= 4 * 148 * 256;
+    if (!tuned && cands.size() > 1 && big) {
+        shape = tune_scan(cands, a, v, qtab_len, st);
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        g_tuned[key] = shape;
+    }
+    g_last_shape.store(shape.nw * 1000 + shape.lc * 10 + (shape.staged ? 1 : 0));
+    run_scan(shape, a, v, qtab_len, st);
     if (!direct) merge_candidates(ckey.get(), cslot.get(), nq, nchunks, kp, out_key, out_slot, st);
 }
 

@@ -410,33 +410,76 @@ __global__ void __launch_bounds__(128) k_finalize_ivf(const uint64_t* __restrict
 // Re-rank (reference src/refine_index.cpp:112-140): the exact score of every
 // candidate from the raw rows, then the k smallest by (score, slot), compared
 // as floats (so -0 == +0), ids mapped through the refine index's labels.
+// Candidate rows are gathered a tile at a time into shared memory, each warp
+// reading whole rows with coalesced loads, at an odd row stride so that the
+// threads' walks along their own rows fall on distinct banks.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_refine(const float* __restrict__ q, int dim, const float* __restrict__ rows,
                                                 const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ slot_in,
                                                 int kp, int k, bool ip, const int64_t* __restrict__ labels, bool cosine,
                                                 int64_t* __restrict__ out_ids, float* __restrict__ out_d,
-                                                const int* __restrict__ kp_q, const int* __restrict__ k_q) {
+                                                const int* __restrict__ kp_q, const int* __restrict__ k_q, int tile) {
     extern __shared__ uint8_t sm_raw[];
     const int kpow = max(2, next_pow2(kp));
     uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);
     int64_t* val = reinterpret_cast<int64_t*>(key + kpow);
     float* qv = reinterpret_cast<float*>(val + kpow);
+    float* trow = qv + dim;
+    const int stride = dim | 1;
     const int qi = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     const int kpq = kp_q ? min(kp_q[qi], kp) : kp;   // the query's first kpq candidates by key64
     const int kq = k_q ? min(k_q[qi], k) : k;
     for (int t = threadIdx.x; t < dim; t += blockDim.x) qv[t] = q[static_cast<size_t>(qi) * dim + t];
-    __syncthreads();
-    for (int i = threadIdx.x; i < kpow; i += blockDim.x) {
-        const bool ok = i < kpq && key_in[static_cast<size_t>(qi) * kp + i] != ~0ull;
-        if (!ok) {
-            key[i] = ~0ull;
-            val[i] = INT64_MAX;
-            continue;
+    for (int i = kpq + threadIdx.x; i < kpow; i += blockDim.x) {
+        key[i] = ~0ull;
+        val[i] = INT64_MAX;
+    }
+    for (int t0 = 0; t0 < kpq; t0 += tile) {
+        const int nt = min(tile, kpq - t0);
+        __syncthreads();   // the previous tile's rows are consumed
+        // each warp gathers 4 rows at a time, 16 loads per lane in flight
+        for (int c0 = warp; c0 < nt; c0 += 4 * nwarps) {
+            const float* src[4];
+            bool ok[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int c = c0 + u * nwarps;
+                const size_t ci = static_cast<size_t>(qi) * kp + t0 + c;
+                ok[u] = c < nt && key_in[ci] != ~0ull;
+                src[u] = ok[u] ? rows + static_cast<size_t>(slot_in[ci]) * dim : rows;
+            }
+            for (int e0 = 0; e0 < dim; e0 += 128) {
+                float x[4][4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int e = e0 + lane + 32 * j;
+                        x[u][j] = ok[u] && e < dim ? __ldg(src[u] + e) : 0.0f;
+                    }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int e = e0 + lane + 32 * j;
+                        if (ok[u] && e < dim) trow[(c0 + u * nwarps) * stride + e] = x[u][j];
+                    }
+            }
         }
-        const uint32_t slot = slot_in[static_cast<size_t>(qi) * kp + i];
-        const float d = exact_score(qv, rows + static_cast<size_t>(slot) * dim, dim, ip);
-        key[i] = float_key_eq0(d);
-        val[i] = slot;
+        __syncthreads();
+        for (int c = threadIdx.x; c < nt; c += blockDim.x) {
+            const int i = t0 + c;
+            const size_t ci = static_cast<size_t>(qi) * kp + i;
+            if (key_in[ci] == ~0ull) {
+                key[i] = ~0ull;
+                val[i] = INT64_MAX;
+                continue;
+            }
+            const float d = exact_score(qv, trow + c * stride, dim, ip);
+            key[i] = float_key_eq0(d);
+            val[i] = slot_in[ci];
+        }
     }
     bitonic_sort(key, val, kpow);
     for (int i = threadIdx.x; i < k; i += blockDim.x) {
@@ -552,11 +595,16 @@ void refine_candidates(const float* q, int nq, int dim, const float* rows, const
                        cudaStream_t st, const int* kp_q, const int* k_q) {
     if (nq == 0 || k == 0) return;
     const int kpow = std::max(2, next_pow2(kp));
-    const size_t rsm = static_cast<size_t>(kpow) * 16 + static_cast<size_t>(dim) * 4;
-    if (rsm > 48 * 1024)
-        allow_large_smem<k_refine>();
+    // candidate rows staged per tile: up to 128 rows within ~96 KB
+    const size_t row_bytes = static_cast<size_t>(dim | 1) * 4;
+    const int tile = static_cast<int>(std::clamp<size_t>((96 * 1024) / row_bytes, 1, 128));
+    const size_t rsm = static_cast<size_t>(kpow) * 16 + static_cast<size_t>(dim) * 4 + tile * row_bytes;
+    require(rsm <= 200 * 1024, "re-rank shared memory exceeds the B200 limit for this k * k_factor and dim",
+            kUnsupported);
+    allow_large_smem<k_refine>();
     KernelTimer kt("refine", st);
-    k_refine<<<nq, 128, rsm, st>>>(q, dim, rows, key, slot, kp, k, ip, labels, cosine, out_ids, out_d, kp_q, k_q);
+    k_refine<<<nq, 128, rsm, st>>>(q, dim, rows, key, slot, kp, k, ip, labels, cosine, out_ids, out_d, kp_q, k_q,
+                                   tile);
     QG_LAUNCH_CHECK();
 }
 

@@ -107,6 +107,17 @@ int filtered_probes(const IvfView& v, const IvfSearchArgs& s, DevBuf<uint32_t>& 
 // The k' = s.kp best candidates of each query, as sorted (key64, slot) lists
 // (key64 = key(dist) << 32 | push index; 0xFFFF... marks an empty entry).
 void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st);
+// The scan's shape autotuner: on (1, the default) it times the candidate
+// shapes on the first large search of each problem key; off (0) every search
+// uses the first candidate. The variant restricts the candidates: -1 any, 0
+// codes read from global memory, 1 codes staged through shared memory.
+void set_scan_autotune(int on);
+int scan_autotune();
+void set_scan_variant(int v);
+int scan_variant();
+int scan_tuned_shapes();
+// The last scan's shape: warps * 1000 + lists per LUT group * 10 + staged.
+int scan_last_shape();
 // The kp smallest key64 over nchunks sorted lists per query.
 void merge_candidates(const uint64_t* in_key, const uint32_t* in_slot, int nq, int nchunks, int kp, uint64_t* out_key,
                       uint32_t* out_slot, cudaStream_t st);

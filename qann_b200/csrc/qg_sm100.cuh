@@ -69,6 +69,16 @@ __device__ __forceinline__ void tma_load_2d(const void* tmap, void* dst, uint64_
         : "memory");
 }
 
+// Contiguous bulk copy (no tensor map, no multicast) of `bytes` from global
+// memory into this CTA's shared memory, counted as transaction bytes on
+// `bar`. Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :
+                 : "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
 // TMEM: allocate / free `cols` columns (a power of two >= 32) by one whole warp.
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t cols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),

@@ -51,3 +51,24 @@ def test_generated_indexes(golden, kind, name):
     ids, d = idx.batch_query(q, 10)
     np.testing.assert_array_equal(ids, np.load(golden / "gen" / f"{kind}_{name}_ids.npy"))
     np.testing.assert_array_equal(d, np.load(golden / "gen" / f"{kind}_{name}_dists.npy"))
+
+
+@pytest.fixture
+def scan_variant(request):
+    qb.set_scan_options(autotune=False, variant=request.param)
+    yield request.param
+    qb.set_scan_options(autotune=True, variant=-1)
+
+
+@pytest.mark.parametrize("scan_variant", [0, 1], indirect=True)
+@pytest.mark.parametrize("kind", ["ivf", "refine"])
+@pytest.mark.parametrize("name", GEN)
+def test_scan_shapes_identical(golden, scan_variant, kind, name):
+    """Each fast-scan kernel shape (codes from global memory, or staged through
+    shared memory) returns the reference's results."""
+    idx = qb.load(golden / "gen" / f"{kind}_{name}.qann")
+    q = np.load(golden / "gen" / "queries.npy")
+    assert qb.scan_options()["variant"] == scan_variant
+    ids, d = idx.batch_query(q, 10)
+    np.testing.assert_array_equal(ids, np.load(golden / "gen" / f"{kind}_{name}_ids.npy"))
+    np.testing.assert_array_equal(d, np.load(golden / "gen" / f"{kind}_{name}_dists.npy"))

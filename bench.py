@@ -335,6 +335,256 @@ def cpu_baseline(cfg, path, queries, nprobe):
             "sample": f"{sample} of the {queries.shape[0]} queries, one batch_query on {cores} threads"}
 
 
+# ---- other workloads (--workload): flat search, index training, served stream -------------------
+
+def gaussian_mixture(n, d, centres, sigma, seed_rows, seed_centres=12345):
+    """Uniform choice among `centres` N(0, I) centres plus sigma * N(0, I) noise."""
+    c = np.random.default_rng(seed_centres).standard_normal((centres, d), dtype=np.float32)
+    rng = np.random.default_rng(seed_rows)
+    x = np.empty((n, d), np.float32)
+    for s in range(0, n, 1 << 20):
+        e = min(n, s + (1 << 20))
+        x[s:e] = c[rng.integers(0, centres, e - s)] + np.float32(sigma) * rng.standard_normal((e - s, d), dtype=np.float32)
+    return x
+
+
+def device_steps(index, q_dev, nq, k, steps, warmup, flush=None):
+    """CUDA-event times (ms) of `steps` device-resident searches of the nq queries."""
+    import torch
+    oi = torch.empty((nq, k), dtype=torch.int64, device=q_dev.device)
+    od = torch.empty((nq, k), dtype=torch.float32, device=q_dev.device)
+    st = torch.cuda.current_stream()
+    for _ in range(warmup):
+        index.search_device(q_dev.data_ptr(), nq, k, oi.data_ptr(), od.data_ptr(), st.cuda_stream)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        if flush is not None:
+            flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        index.search_device(q_dev.data_ptr(), nq, k, oi.data_ptr(), od.data_ptr(), st.cuda_stream)
+        e1.record(st)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times, oi, od
+
+
+def flat_workload(args):
+    """Exact flat search as a GEMM: 10,000,000 x 96 float32 (N(0,1) per
+    dimension, rows scaled by LogNormal(0, 0.25)), 10,000 queries of the same
+    law, k = 100, squared L2 and inner product. Exact results through the BF16
+    tensor-core filter and FP32 recheck; per-distance error against FP64."""
+    import torch
+    import qann_b200 as qb
+    from qann_b200 import profiling
+    n, d, nq, k = (1_000_000, 96, 2_000, 100) if args.small else (10_000_000, 96, 10_000, 100)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((n, d), dtype=np.float32)
+    x *= np.exp(rng.normal(0.0, 0.25, size=(n, 1))).astype(np.float32)
+    rq = np.random.default_rng(1)
+    q = rq.standard_normal((nq, d), dtype=np.float32) * np.exp(rq.normal(0.0, 0.25, size=(nq, 1))).astype(np.float32)
+    dev = torch.device("cuda:0")
+    q_dev = torch.from_numpy(q).to(dev)
+    per_metric = {}
+    peak, peak_src = measured_peak("bf16_tflops", 1590.0)
+    for metric, name in ((qb.Metric.L2, "l2"), (qb.Metric.InnerProduct, "ip")):
+        idx = qb.FlatIndex(d, metric=metric)
+        idx.add(x)
+        profiling.enable(True)
+        profiling.reset()
+        launches0 = profiling.launch_count()
+        times, oi, od = device_steps(idx, q_dev, nq, k, args.steps, args.warmup)
+        launches = profiling.launch_count() - launches0
+        mm_ms, mm_n = profiling.get("mm_filter")
+        profiling.enable(False)
+        total = sum(times)
+        ids, dist = oi.cpu().numpy(), od.cpu().numpy()
+        # the exact FP32 path on a sample: identical results
+        qb.set_tensor_filter(0)
+        i0, d0 = idx.batch_query(q[:32], k)
+        qb.set_tensor_filter(1)
+        same = bool(np.array_equal(i0, ids[:32]) and d0.tobytes() == dist[:32].tobytes())
+        # per-distance error against FP64 on a sample
+        s = 256
+        rows = torch.from_numpy(x[ids[:s].ravel()].reshape(s, k, d)).to(dev).double()
+        qq = q_dev[:s].double()[:, None, :]
+        d64 = ((qq - rows) ** 2).sum(-1) if name == "l2" else -(qq * rows).sum(-1)
+        err = (torch.from_numpy(dist[:s]).to(dev).double() - d64).abs() / d64.abs().clamp_min(1e-30)
+        t = time.perf_counter()
+        idx.batch_query(q, k)
+        e2e = nq / (time.perf_counter() - t)
+        flops = 2.0 * nq * n * d
+        per_metric[name] = {
+            "qps": round(nq * args.steps / (total / 1e3), 1), "ms_per_step": round(total / args.steps, 2),
+            "e2e_qps": round(e2e, 1), "identical_to_exact_fp32": same,
+            "rel_err_vs_fp64": {"max": float(err.max()), "mean": float(err.mean())},
+            "tensor_tflops": round(flops / (total / args.steps / 1e3) / 1e12, 1),
+            "filter_kernel_tflops": round(flops * args.steps / (mm_ms / 1e3) / 1e12, 1) if mm_ms else None,
+            "gpu_launches": launches}
+        del idx
+        log(f"flat {name}: {per_metric[name]}")
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            cores = os.cpu_count() or 1
+            ref.set_num_threads(cores)
+            r = ref.FlatIndex(d)
+            r.add(x)
+            sample = 16
+            t = time.perf_counter()
+            r.batch_query(q[:sample], k)
+            dt = time.perf_counter() - t
+            cpu = {"value": round(sample / dt, 2), "unit": "queries/s", "cores": cores, "kind": "reference",
+                   "sample": f"{sample} queries, L2, one batch_query on {cores} threads"}
+    l2 = per_metric["l2"]
+    print(json.dumps({
+        "metric": "exact flat search QPS (10M x 96, k=100)", "value": l2["qps"], "unit": "queries/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": l2["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16 filter + f32 recheck", "data": "synthetic",
+        "config": {"workload": f"flat_{n}x{d}_k{k}", "nq": nq, "l2": "inputs larger than L2 (3.84 GB rows)"},
+        "per_metric": per_metric,
+        "roofline": {"bound": "tensor", "achieved": l2["tensor_tflops"], "peak": peak, "unit": "TFLOP/s",
+                     "frac": round(l2["tensor_tflops"] / peak, 4), "traffic": None, "peak_source": peak_src},
+        "e2e": {"value": l2["e2e_qps"], "unit": "queries/s", "h2d_bytes_per_step": nq * d * 4,
+                "d2h_bytes_per_step": nq * k * 12},
+        "gpu_launches": l2["gpu_launches"], "cpu_baseline": cpu}))
+    return 0
+
+
+def train_workload(args):
+    """Index training, batched: 2,000,000 x 128 Gaussian mixture (8,192
+    centres, sigma 0.2, uniform sizes); coarse k-means nlist 16,384 for 20
+    Lloyd iterations, then PQ 64 x 4-bit; seed 1."""
+    import torch
+    import qann_b200 as qb
+    n, nlist = (200_000, 2048) if args.small else (2_000_000, 16384)
+    d, m, iters = 128, 64, 20
+    x = gaussian_mixture(n, d, 8192, 0.2, seed_rows=0)
+    # warm-up: context, kernels and pools on a small problem
+    w = qb.IVFIndex(d, 256, 8)
+    w.enable_pq(m, fast_scan=True)
+    w.train(x[:20000], max_iters=2, seed=1, clustering=qb.Clustering.Lloyd)
+    del w
+    torch.cuda.synchronize()
+    ivf = qb.IVFIndex(d, nlist, 16)
+    ivf.enable_pq(m, fast_scan=True)
+    t = time.perf_counter()
+    ivf.train(x, max_iters=iters, seed=1, clustering=qb.Clustering.Lloyd)
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t
+    pairs = float(n) * nlist * (iters + 1)   # assignments: every iteration plus the final one
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            cores = os.cpu_count() or 1
+            ref.set_num_threads(cores)
+            sample = 50_000
+            r = ref.IVFIndex(d, nlist, 16)
+            r.enable_pq(m, fast_scan=True)
+            t = time.perf_counter()
+            r.train(x[:sample], max_iters=1, seed=1, clustering=ref.LLOYD)
+            dt = time.perf_counter() - t
+            rate = 2.0 * sample * nlist / dt   # one iteration and the final assignment
+            cpu = {"value": round(pairs / rate, 1), "unit": "s (extrapolated)", "cores": cores, "kind": "reference",
+                   "sample": f"train() of {sample} points, 1 Lloyd iteration, {dt:.1f} s: "
+                             f"{rate:.3g} point-list pairs/s extrapolated to the full training"}
+    print(json.dumps({
+        "metric": "IVF training time (2M x 128, nlist 16384, 20 Lloyd iterations, PQ 64x4)", "value": round(secs, 2),
+        "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": round(secs * 1e3, 1),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 filter + f32/f64",
+        "data": "synthetic", "config": {"workload": f"train_{n}x{d}_nl{nlist}_lloyd{iters}_pq{m}"},
+        "assign_pairs_per_s": round(pairs / secs, 1), "cpu_baseline": cpu}))
+    return 0
+
+
+def served_workload(args):
+    """Served stream over a device-resident IVF-PQ fast-scan + refine index of
+    5,000,000 x 128 (Gaussian mixture, 8,192 centres, sigma 0.2), nlist 16,384,
+    PQ 64 x 4-bit, k_factor 10: Poisson arrivals at 5k-200k queries/s, k in
+    {10, 100}, nprobe log-uniform in 8..256, 30% of requests with an allowed-id
+    bitmap of selectivity uniform in [1%, 50%]; p50 / p99 latency per rate."""
+    import torch
+    import qann_b200 as qb
+    n, nlist = (500_000, 2048) if args.small else (5_000_000, 16384)
+    d, m, kf = 128, 64, 10
+    path = CACHE / f"served_{n}x{d}_nl{nlist}_m{m}_kf{kf}.qann"
+    CACHE.mkdir(parents=True, exist_ok=True)
+    x = gaussian_mixture(n, d, 8192, 0.2, seed_rows=0)
+    if not path.exists():
+        t = time.time()
+        ivf = qb.IVFIndex(d, nlist, 32)
+        ivf.enable_pq(m, fast_scan=True)
+        ivf.train(x, seed=1)
+        r = qb.RefineIndex(ivf, kf)
+        r.add(x)
+        r.save(str(path) + ".part")
+        os.replace(str(path) + ".part", path)
+        log(f"built the served index on the GPU in {time.time() - t:.1f} s")
+        del r, ivf
+    index = qb.load(path)
+    nreq = 20_000
+    q = gaussian_mixture(nreq, d, 8192, 0.2, seed_rows=1)
+    rng = np.random.default_rng(2)
+    pool = []
+    for _ in range(16):
+        sel = rng.uniform(0.01, 0.5)
+        bits = rng.random(n) < sel
+        pool.append(bits)
+    rates = (5_000, 10_000, 20_000, 50_000, 100_000, 200_000)
+    out = []
+    same = True
+    with qb.Server(index, slots=4, max_batch=256, mem_budget=4 << 30) as srv:
+        fids = [srv.add_filter(np.packbits(np.concatenate([b, np.zeros((-n) % 64, bool)]), bitorder="little")
+                               .view(np.uint64)) for b in pool]
+        arng = np.random.default_rng(3)
+        ks = arng.choice(np.array([10, 100], np.int32), size=nreq)
+        npb = np.rint(np.exp(arng.uniform(np.log(8), np.log(256), size=nreq))).astype(np.int32)
+        filt = np.where(arng.random(nreq) < 0.3, arng.integers(0, len(fids), nreq), -1)
+        fid = np.array([fids[f] if f >= 0 else -1 for f in filt], np.int32)
+        srv.replay(q[:2000], ks[:2000], np.zeros(2000), nprobes=npb[:2000], filter_ids=fid[:2000])   # warm-up
+        for rate in rates:
+            arrivals = np.cumsum(arng.exponential(1.0 / rate, size=nreq))
+            t = time.perf_counter()
+            ids, _, lat = srv.replay(q, ks, arrivals, nprobes=npb, filter_ids=fid)
+            wall = time.perf_counter() - t
+            lat_ms = np.sort(lat) * 1e3
+            out.append({"offered_qps": rate, "achieved_qps": round(nreq / wall, 1),
+                        "p50_ms": round(float(lat_ms[nreq // 2]), 3),
+                        "p99_ms": round(float(lat_ms[int(0.99 * nreq)]), 3)})
+            log(f"served at {rate}/s: {out[-1]}")
+        # a sample of requests against the same search run alone
+        base = index.base
+        for i in range(0, nreq, nreq // 64):
+            base.nprobe = int(npb[i])
+            allowed = np.flatnonzero(pool[filt[i]]) if filt[i] >= 0 else None
+            si, _ = index.batch_query(q[i:i + 1], int(ks[i]), allowed=allowed)
+            same &= bool(np.array_equal(si[0], ids[i, :ks[i]]))
+        st = srv.stats()
+    # the plain FP32 GPU batch path on the same rows: exact flat search, no tensor cores
+    flat = qb.FlatIndex(d)
+    flat.add(x)
+    qb.set_tensor_filter(0)
+    t = time.perf_counter()
+    flat.batch_query(q[:1000], 10)
+    fp32_qps = 1000 / (time.perf_counter() - t)
+    qb.set_tensor_filter(1)
+    best = max(out, key=lambda r: r["achieved_qps"] if r["p99_ms"] <= 2.0 else 0)
+    print(json.dumps({
+        "metric": "served QPS at p99 <= 2 ms (5M x 128 IVF16384-PQ64x4fs + refine kf10, mixed k / nprobe / filters)",
+        "value": best["achieved_qps"] if best["p99_ms"] <= 2.0 else None, "unit": "queries/s", "n_gpus": 1,
+        "steps": len(rates), "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": f"served_{n}x{d}_nl{nlist}_m{m}_kf{kf}", "requests_per_rate": nreq,
+                   "k": [10, 100], "nprobe": "log-uniform 8..256", "filtered": 0.3, "selectivity": [0.01, 0.5],
+                   "slots": 4, "max_batch": 256},
+        "rates": out, "results_equal_solo_searches": same, "mean_batch": round(st["completed"] / st["batches"], 1),
+        "plain_fp32_gpu_flat_qps": round(fp32_qps, 1)}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -345,7 +595,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the continuous-batching server measurement")
     ap.add_argument("--nprobe", type=int, default=0, help="use this nprobe instead of the recall sweep (profiling)")
+    ap.add_argument("--scan-shape", default="auto", choices=["auto", "global", "staged"],
+                    help="fast-scan kernel shape: autotuned (default) or fixed (profiling)")
+    ap.add_argument("--workload", default="angular", choices=["angular", "flat", "train", "served"],
+                    help="angular: the headline line; flat / train / served: the other configurations")
     args = ap.parse_args()
+    if args.workload != "angular" and args.impl == "qann_b200":
+        import torch
+        torch.cuda.set_device(0)
+        return {"flat": flat_workload, "train": train_workload, "served": served_workload}[args.workload](args)
     cfg = SMALL if args.small else FULL
     if args.impl == "reference":
         return reference_arm(args, cfg)
@@ -369,6 +627,8 @@ def main():
     import qann_b200 as qb
     from qann_b200 import profiling
 
+    if args.scan_shape != "auto":
+        qb.set_scan_options(autotune=False, variant=0 if args.scan_shape == "global" else 1)
     base = mixture(cfg, 0, cfg["n"])
     queries = mixture(cfg, 1 + rank, cfg["nq"])
     index, path = build_or_load(cfg, base, rank, world, barrier)
@@ -395,6 +655,7 @@ def main():
     torch.cuda.synchronize()
     profiling.enable(True)
     profiling.reset()
+    coarse0 = qb.tensor_filter_counts()
     launches0 = profiling.launch_count()
     step_ms = []
     barrier()
@@ -410,7 +671,13 @@ def main():
     torch.cuda.synchronize()
     barrier()
     launches = profiling.launch_count() - launches0
+    coarse1 = qb.tensor_filter_counts()
     profiling.enable(False)
+    cq = coarse1["coarse_queries"] - coarse0["coarse_queries"]
+    coarse = {"path": "f16 tensor-core estimates + exact FP32 recheck" if cq else "exact FP32",
+              "queries": cq, "redone_exactly": coarse1["coarse_redone"] - coarse0["coarse_redone"],
+              "lists_rescored_per_query": round((coarse1["coarse_candidates"] - coarse0["coarse_candidates"]) / cq, 1)
+              if cq else None}
     scan_ms, scan_n = profiling.get("scan")
     kernel_ms = {kname: profiling.get(kname) for kname in profiling.KERNELS}
     total_ms = float(sum(step_ms))
@@ -463,7 +730,7 @@ def main():
                    "parallelism": f"replicas x{world}", "batch_latency_ms": {
                        "p50": round(srt[len(srt) // 2], 4), "p99": round(srt[min(len(srt) - 1, int(0.99 * len(srt)))], 4)},
                    "kernel_ms_total": {kk: round(v[0], 3) for kk, v in kernel_ms.items() if v[1]},
-                   "scan_shape": scan_shape},
+                   "scan_shape": scan_shape, "coarse": coarse},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
                      "kernel": "k_scan", "algorithmic_bytes_per_launch": alg_bytes,

@@ -177,7 +177,11 @@ int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, con
  *   0 = never, 1 = when the work is large enough to pay (default), 2 = whenever
  *   the dimension is supported (<= 128). qg_get_option also reads
  *   "tensor_filter_queries" (queries answered through the filter so far) and
- *   "tensor_filter_redone" (those redone exactly after a candidate overflow). No counterpart in the reference, whose
+ *   "tensor_filter_redone" (those redone exactly after a candidate overflow). The same mode sends an IVF search's
+ *   coarse step (the nprobe nearest lists, reference src/ivf_index.cpp:305-419) through BF16 estimates with an
+ *   error bound and an exact FP32 recheck of the lists that can still be among the nearest; qg_get_option reads
+ *   "tensor_coarse_queries", "tensor_coarse_redone" (queries sent back to the exact path after too many
+ *   near-ties) and "tensor_coarse_candidates" (lists rescored exactly). No counterpart in the reference, whose
  *   exact scores always come from its CPU distance kernels (reference src/flat_index.cpp:33-64).
  * "scan_autotune": 1 (default) times the fast-scan kernel's candidate shapes
  *   (warps per block, lists per LUT group, codes read from global memory or

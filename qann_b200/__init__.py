@@ -98,6 +98,10 @@ def tensor_filter_counts() -> dict:
         v = C.c_int64()
         check(_lib.lib.qg_get_option(f"tensor_filter_{key}".encode(), C.byref(v)))
         out[key] = v.value
+    for key in ("queries", "redone", "candidates"):
+        v = C.c_int64()
+        check(_lib.lib.qg_get_option(f"tensor_coarse_{key}".encode(), C.byref(v)))
+        out[f"coarse_{key}"] = v.value
     return out
 
 

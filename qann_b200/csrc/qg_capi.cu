@@ -541,6 +541,12 @@ int qg_get_option(const char* key, int64_t* value) {
         if (k == "tensor_filter") *value = tensor_filter();
         else if (k == "tensor_filter_queries") *value = queries;
         else if (k == "tensor_filter_redone") *value = redone;
+        else if (k == "tensor_coarse_queries" || k == "tensor_coarse_redone") {
+            int64_t cq = 0, cr = 0;
+            tensor_coarse_counts(&cq, &cr);
+            *value = k == "tensor_coarse_queries" ? cq : cr;
+        }
+        else if (k == "tensor_coarse_candidates") *value = tensor_coarse_candidates();
         else if (k == "scan_autotune") *value = scan_autotune();
         else if (k == "scan_variant") *value = scan_variant();
         else if (k == "scan_tuned_shapes") *value = scan_tuned_shapes();

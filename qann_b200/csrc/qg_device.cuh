@@ -64,6 +64,92 @@ __host__ __device__ __forceinline__ int next_pow2(int n) {
     return p;
 }
 
+// One warp keeps the `keep` smallest of the n distinct keys buf[0, n) in
+// buf[0, keep) (in no particular order) and returns the largest kept key.
+// Radix select, 8 bits at a time from the top: each pass counts the keys
+// that share the prefix chosen so far by their next digit, and takes the
+// digit whose bin holds the keep-th key; it stops once every key of that
+// bin is kept. hist: 256 ints of warp-private shared scratch. n > keep >= 1.
+__device__ __noinline__ static uint64_t warp_select_keep(uint64_t* buf, int n, int keep, int* hist) {
+    const int lane = threadIdx.x & 31;
+    constexpr unsigned kFull = 0xffffffffu;
+    uint64_t prefix = 0, mask = 0;
+    int need = keep;   // keys still to take among those that match the prefix
+    int shift = 56;
+    for (;; shift -= 8) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) hist[8 * lane + j] = 0;
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            const uint64_t k = buf[i];
+            if ((k & mask) == prefix) atomicAdd(&hist[static_cast<int>(k >> shift) & 255], 1);
+        }
+        __syncwarp();
+        int c[8], own = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            c[j] = hist[8 * lane + j];
+            own += c[j];
+        }
+        int incl = own;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int excl = incl - own;
+        const unsigned owner = __ballot_sync(kFull, excl < need && need <= incl);
+        const int ol = __ffs(owner) - 1;
+        int digit = 0, below = 0, cnt = 0;
+        if (lane == ol) {
+            int acc = excl;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (cnt == 0 && acc + c[j] >= need) {
+                    digit = 8 * lane + j;
+                    below = acc;
+                    cnt = c[j];
+                }
+                acc += c[j];
+            }
+        }
+        digit = __shfl_sync(kFull, digit, ol);
+        below = __shfl_sync(kFull, below, ol);
+        cnt = __shfl_sync(kFull, cnt, ol);
+        need -= below;
+        prefix |= static_cast<uint64_t>(digit) << shift;
+        mask |= 0xFFull << shift;
+        __syncwarp();
+        if (cnt == need || shift == 0) break;   // (at shift 0 the bin is one key)
+    }
+    // kept: every key whose bits above `shift` do not exceed the prefix
+    const uint64_t lim = prefix | ((1ull << shift) - 1);
+    int out = 0;
+    uint64_t kmax = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + lane;
+        uint64_t k = 0;
+        bool in = false;
+        if (i < n) {
+            k = buf[i];
+            in = k <= lim;
+        }
+        const unsigned bal = __ballot_sync(kFull, in);
+        __syncwarp();
+        if (in) {
+            buf[out + __popc(bal & ((1u << lane) - 1))] = k;
+            kmax = k > kmax ? k : kmax;
+        }
+        out += __popc(bal);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const uint64_t t = __shfl_xor_sync(kFull, kmax, o);
+        kmax = t > kmax ? t : kmax;
+    }
+    __syncwarp();
+    return kmax;
+}
+
+
 // ---------------------------------------------------------------------------
 // Block reductions
 // ---------------------------------------------------------------------------

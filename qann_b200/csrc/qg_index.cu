@@ -218,6 +218,13 @@ void ensure_device(IVFObj& o, cudaStream_t) {
     v.codes = D.codes.get();
     v.ids = D.ids.get();
     v.deleted = M.idmap.deleted_count() ? D.deleted.get() : nullptr;
+    if (mm_supported(dim)) {
+        prepare_f16_rows(D.centroids.get(), nlist, dim, D.cent_f16, D.cent_sq, D.cent_exp, v.cent_dpad, st);
+        QG_CUDA(cudaStreamSynchronize(st));
+        v.cent_f16 = D.cent_f16.get();
+        v.cent_sq = D.cent_sq.get();
+        v.cent_exp = D.cent_exp.get();
+    }
     o.dev_dirty = false;
 }
 

@@ -21,6 +21,9 @@ struct DeviceIVF {
     DevBuf<uint4> codes;
     DevBuf<uint64_t> deleted;
     DevBuf<int64_t> labels;   // slot -> id when the ids are not the slots
+    DevBuf<uint16_t> cent_f16;   // scaled f16 centroids for the tensor-core coarse step
+    DevBuf<float> cent_sq;
+    DevBuf<int> cent_exp;
     size_t total_sb = 0;
 };
 

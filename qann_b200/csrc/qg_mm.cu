@@ -28,6 +28,7 @@
 
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cmath>
@@ -62,6 +63,9 @@ struct MmArgs {
     uint32_t* cand_row;      // per query, cap entries
     int cap;
     int* err;
+    float* store;            // store mode: the raw products acc(q, row) at store[q * ld + row - n0], no filtering
+    size_t ld;
+    int f16;                 // operands are F16 (else BF16)
 };
 
 size_t filter_smem_bytes(int kblocks) {
@@ -153,7 +157,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t idesc = idesc_bf16_f32(BM, BN);
+            const uint32_t idesc = a.f16 ? idesc_f16_f32(BM, BN) : idesc_bf16_f32(BM, BN);
             int it = 0, aloads = 0, cur_m = -1, ti = 0;
             for (int t = blockIdx.x; t < total && !*abort; t += gridDim.x) {
                 const int mt = t / a.ntiles;
@@ -210,12 +214,21 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_fence_after();
             const int qi = mt * BM + row_in_tile;
             const bool live = qi < a.nq;
-            const float thr = live ? a.thr[qi] : 0.0f;
+            const float thr = live && !a.store ? a.thr[qi] : 0.0f;
             for (int c = 0; c < BN / 2; c += 32) {
                 uint32_t v[32];
                 tmem_ld32(tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(acc * BN + col0 + c),
                           v);
                 const int r0 = a.n0 + nt * BN + col0 + c;   // base row of v[0]
+                if (a.store) {
+                    if (live) {
+                        float* dst = a.store + static_cast<size_t>(qi) * a.ld + (r0 - a.n0);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (r0 + j < a.n1) dst[j] = __uint_as_float(v[j]);
+                    }
+                    continue;
+                }
                 const float xt = r0 + lane < a.n1 ? a.xterm[r0 + lane] : 0.0f;
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
@@ -262,6 +275,38 @@ __global__ void k_mm_prep(const float* __restrict__ x, size_t n, int d, int dpad
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) x2[r] = s;
+}
+
+// Rows to f16 after scaling each by a power of two, 2^e with e = 14 -
+// exponent(max |x_i|), so the largest element lands in [2^13, 2^14) (exact
+// scaling, round to nearest even), zero-padded to dpad; each row's float sum
+// of squares (unscaled) and e. One warp per row.
+__global__ void k_mm_prep16(const float* __restrict__ x, size_t n, int d, int dpad, __half* __restrict__ xh,
+                            float* __restrict__ x2, int* __restrict__ xe) {
+    const size_t r = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= n) return;
+    float s = 0.0f, mx = 0.0f;
+    for (int j = lane; j < d; j += 32) {
+        const float v = x[r * d + j];
+        s = __fmaf_rn(v, v, s);
+        mx = fmaxf(mx, fabsf(v));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    int ex = 0;
+    if (mx > 0.0f) frexpf(mx, &ex);
+    const int e = mx > 0.0f ? 14 - ex : 0;
+    for (int j = lane; j < dpad; j += 32) {
+        const float v = j < d ? ldexpf(x[r * d + j], e) : 0.0f;
+        xh[r * dpad + j] = __float2half_rn(v);
+    }
+    if (lane == 0) {
+        x2[r] = s;
+        xe[r] = e;
+    }
 }
 
 __global__ void k_mm_terms(const float* __restrict__ sq, size_t n, float coef, float* __restrict__ out) {
@@ -342,14 +387,15 @@ EncodeTiled encode_fn() {
     return fn;
 }
 
-// bf16 rows (dpad elements, row stride dpad * 2 bytes) read as boxes of 64 x box_rows, 128-byte swizzle.
-CUtensorMap make_map(const __nv_bfloat16* ptr, size_t rows, int dpad, int box_rows) {
+// bf16 or f16 rows (dpad elements, row stride dpad * 2 bytes) read as boxes of 64 x box_rows, 128-byte swizzle.
+CUtensorMap make_map(const void* ptr, size_t rows, int dpad, int box_rows, bool f16 = false) {
     CUtensorMap m;
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(dpad), static_cast<cuuint64_t>(rows)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(dpad) * 2};
     const cuuint32_t box[2] = {static_cast<cuuint32_t>(KA), static_cast<cuuint32_t>(box_rows)};
     const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), dims,
+    const CUresult r = encode_fn()(&m, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                                   const_cast<void*>(ptr), dims,
                                    strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     require(r == CUDA_SUCCESS, "cuTensorMapEncodeTiled failed", kCudaError);
@@ -472,6 +518,285 @@ static void mm_topk_block(const float* q, size_t nq, const float* rows, const Mm
     require(herr == 0, "tensor-core filter: a pipeline wait timed out", kRuntimeError);
     for (size_t i = 0; i < nq; ++i)
         if (hovf[i]) overflow_q.push_back(static_cast<int>(q_first + i));
+}
+
+
+// ---------------------------------------------------------------------------
+// Coarse assignment through the tensor cores (reference src/ivf_index.cpp:
+// 305-419, which ranks lists by the exact distance, ties by list). The store
+// mode of k_mm_filter gives acc(q, c), the F16 dot product of a query and a
+// centroid (each row scaled by a power of two first, undone exactly after)
+// accumulated in FP32. With e = C (|q|^2 + |c|^2) as in mm_topk (C from
+// f16's unit roundoff 2^-11), each exact score lies in [lb, ub] = [s^ - e,
+// s^ + e] (s^ = |q|^2 + |c|^2 - 2 acc for L2, -acc for inner product, e
+// halved). T, the P-th smallest ub,
+// bounds the P-th exact score from above, so only centroids with lb <= T can
+// be among the P nearest: k_coarse_recheck scores those exactly, in the
+// reference's order, and keeps the P smallest by (score, list), -0 == +0.
+// ---------------------------------------------------------------------------
+namespace {
+
+// The k-th smallest (1-based) of n uint32 keys in shared memory, by one block
+// (radix select, 8 bits a pass). hist: 256 ints of shared scratch.
+__device__ uint32_t block_kth_u32(const uint32_t* keys, int n, int k, int* hist, int* s_pick) {
+    uint32_t prefix = 0, mask = 0;
+    int need = k;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int j = threadIdx.x; j < 256; j += blockDim.x) hist[j] = 0;
+        __syncthreads();
+        for (int base = 0; base < n; base += blockDim.x) {   // (loop trip count is block-uniform)
+            const int i = base + threadIdx.x;
+            const uint32_t key = i < n ? keys[i] : 0u;
+            const bool in = i < n && (key & mask) == prefix;
+            const int bin = in ? static_cast<int>((key >> shift) & 255) : -1;
+            // lanes of a warp that share a bin add once (the first passes put most keys in a few bins)
+            const unsigned same = __match_any_sync(0xffffffffu, bin);
+            if (in && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&hist[bin], __popc(same));
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {   // warp 0: the bin holding the need-th key
+            const int lane = threadIdx.x;
+            int c[8], own = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                c[j] = hist[8 * lane + j];
+                own += c[j];
+            }
+            int incl = own;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int excl = incl - own;
+            if (excl < need && need <= incl) {
+                int acc = excl, digit = 8 * lane + 7;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (acc + c[j] >= need) {
+                        digit = 8 * lane + j;
+                        break;
+                    }
+                    acc += c[j];
+                }
+                s_pick[0] = digit;
+                s_pick[1] = acc;
+            }
+        }
+        __syncthreads();
+        need -= s_pick[1];
+        prefix |= static_cast<uint32_t>(s_pick[0]) << shift;
+        mask |= 0xFFu << shift;
+        __syncthreads();
+    }
+    return prefix;
+}
+
+} // namespace
+
+__global__ void __launch_bounds__(256, 4) k_coarse_recheck(const float* __restrict__ q, const float* __restrict__ q2,
+                                                        const int* __restrict__ qexp, const float* __restrict__ cent,
+                                                        const float* __restrict__ c2, const int* __restrict__ cexp,
+                                                        int nlist, int d, bool ip, float c_up, float c_lo,
+                                                        const float* __restrict__ accm, size_t ld, int P, int cap,
+                                                        uint32_t* __restrict__ probe, float* __restrict__ pdist,
+                                                        int* __restrict__ redo,
+                                                        unsigned long long* __restrict__ ncand) {
+    extern __shared__ __align__(16) uint8_t sm_raw[];
+    const int qi = blockIdx.x;
+    uint64_t* ckey = reinterpret_cast<uint64_t*>(sm_raw);             // cap
+    float* qv = reinterpret_cast<float*>(ckey + cap);                   // d, 16-byte aligned
+    uint32_t* ub = reinterpret_cast<uint32_t*>(qv + ((d + 3) & ~3));    // nlist
+    __shared__ int hist[256], s_pick[2], s_count;
+    const float* arow = accm + static_cast<size_t>(qi) * ld;
+    const float qq = q2[qi];
+    const int qe = qexp[qi];
+    // norms where float squares lose relative accuracy (underflow or near
+    // overflow): the relative bound does not hold, so such a query takes the
+    // exact path and such a list is always rescored
+    auto extreme = [](float x2) { return (x2 > 0.0f && x2 < 0x1p-60f) || !(x2 < 0x1p60f); };
+    if (extreme(qq)) {
+        if (threadIdx.x == 0) redo[qi] = 1;
+        return;
+    }
+    for (int t = threadIdx.x; t < d; t += blockDim.x) qv[t] = q[static_cast<size_t>(qi) * d + t];
+    // upper bounds, rounded up at every step (c_up >= 1 + C for L2, >= C / 2
+    // for inner product; the f16 row scaling is undone exactly by ldexpf).
+    // Four lists per thread and step, read as 16-byte vectors.
+    auto upper = [&](float acc_j, float c2j, int cej) -> uint32_t {
+        const float s = __fadd_ru(qq, c2j);
+        const float a = ldexpf(acc_j, -(qe + cej));
+        const float hi = ip ? __fmaf_ru(c_up, s, -a) : __fmaf_ru(-2.0f, a, __fmul_ru(c_up, s));
+        return extreme(c2j) ? 0xFFFFFFFFu : float_key(hi);
+    };
+    const int n4 = nlist & ~3;
+    for (int j = 4 * threadIdx.x; j < n4; j += 4 * blockDim.x) {
+        const float4 av = *reinterpret_cast<const float4*>(arow + j);
+        const float4 cv = *reinterpret_cast<const float4*>(c2 + j);
+        const int4 ev = *reinterpret_cast<const int4*>(cexp + j);
+        ub[j] = upper(av.x, cv.x, ev.x);
+        ub[j + 1] = upper(av.y, cv.y, ev.y);
+        ub[j + 2] = upper(av.z, cv.z, ev.z);
+        ub[j + 3] = upper(av.w, cv.w, ev.w);
+    }
+    for (int j = n4 + threadIdx.x; j < nlist; j += blockDim.x) ub[j] = upper(arow[j], c2[j], cexp[j]);
+    if (threadIdx.x == 0) s_count = 0;
+    __syncthreads();
+    const uint32_t T = block_kth_u32(ub, nlist, P, hist, s_pick);
+    // candidates: lower bound, rounded down (c_lo <= 1 - C for L2; for inner
+    // product the margin c_up is subtracted from a sum rounded up), <= T
+    auto lower_in = [&](float acc_j, float c2j, int cej) -> bool {
+        const float a = ldexpf(acc_j, -(qe + cej));
+        const float lo = ip ? __fmaf_rd(-c_up, __fadd_ru(qq, c2j), -a)
+                            : __fmaf_rd(-2.0f, a, __fmul_rd(c_lo, __fadd_rd(qq, c2j)));
+        return float_key(lo) <= T || extreme(c2j);
+    };
+    auto push = [&](int j) {
+        const int pos = atomicAdd(&s_count, 1);
+        if (pos < cap) ckey[pos] = static_cast<uint64_t>(j);
+    };
+    for (int j = 4 * threadIdx.x; j < n4; j += 4 * blockDim.x) {
+        const float4 av = *reinterpret_cast<const float4*>(arow + j);
+        const float4 cv = *reinterpret_cast<const float4*>(c2 + j);
+        const int4 ev = *reinterpret_cast<const int4*>(cexp + j);
+        if (lower_in(av.x, cv.x, ev.x)) push(j);
+        if (lower_in(av.y, cv.y, ev.y)) push(j + 1);
+        if (lower_in(av.z, cv.z, ev.z)) push(j + 2);
+        if (lower_in(av.w, cv.w, ev.w)) push(j + 3);
+    }
+    for (int j = n4 + threadIdx.x; j < nlist; j += blockDim.x)
+        if (lower_in(arow[j], c2[j], cexp[j])) push(j);
+    __syncthreads();
+    const int cnt = s_count;
+    if (threadIdx.x == 0) atomicAdd(ncand, static_cast<unsigned long long>(cnt));
+    if (cnt > cap) {   // too many near-ties: this query takes the exact path
+        if (threadIdx.x == 0) redo[qi] = 1;
+        return;
+    }
+    // exact scores, one thread per candidate; each list's score is kept by
+    // list (over its upper bound, no longer needed) for the output
+    float* score_of = reinterpret_cast<float*>(ub);
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+        const int j = static_cast<int>(ckey[i]);
+        const float* row = cent + static_cast<size_t>(j) * d;
+        const float sc = exact_score(qv, row, d, ip);
+        ckey[i] = (static_cast<uint64_t>(float_key_eq0(sc)) << 32) | static_cast<uint32_t>(j);
+        score_of[j] = sc;
+    }
+    __syncthreads();
+    // the P smallest by (score, list), then sorted
+    if (cnt > P) {
+        if (threadIdx.x < 32) warp_select_keep(ckey, cnt, P, hist);
+        __syncthreads();
+    }
+    const int ns = next_pow2(P < 2 ? 2 : P);
+    for (int i = P + threadIdx.x; i < ns; i += blockDim.x) ckey[i] = ~0ull;
+    bitonic_sort_keys(ckey, ns);
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const uint32_t j = static_cast<uint32_t>(ckey[i]);
+        probe[static_cast<size_t>(qi) * P + i] = j;
+        pdist[static_cast<size_t>(qi) * P + i] = score_of[j];
+    }
+}
+
+static size_t coarse_recheck_smem(int nlist, int d, int cap) {
+    return static_cast<size_t>(cap) * 8 + static_cast<size_t>((d + 3) & ~3) * 4 + static_cast<size_t>(nlist) * 4;
+}
+
+static int coarse_cap(int nlist, int P) {
+    return std::min(next_pow2(nlist), std::max(1024, next_pow2(4 * P)));
+}
+
+bool coarse_mm_supported(int nlist, int dim, int P, bool cent_prepared) {
+    return cent_prepared && mm_supported(dim) && P >= 1 && P <= nlist && nlist <= 16384 &&
+           coarse_recheck_smem(nlist, dim, coarse_cap(nlist, P)) <= 200 * 1024;
+}
+
+void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t* probe, float* pdist,
+                      std::vector<int>& redo_q, cudaStream_t st) {
+    redo_q.clear();
+    if (nq == 0) return;
+    const int d = v.dim, nlist = v.nlist;
+    const size_t QB = 65536;   // query blocks bound the score matrix
+    for (size_t q0 = 0; q0 < static_cast<size_t>(nq); q0 += QB) {
+        const int nb = static_cast<int>(std::min(QB, static_cast<size_t>(nq) - q0));
+        DevBuf<uint16_t> qh;
+        DevBuf<float> qsq;
+        DevBuf<int> qexp;
+        int qdpad = 0;
+        prepare_f16_rows(q + q0 * d, nb, d, qh, qsq, qexp, qdpad, st);
+        const size_t ld = (static_cast<size_t>(nlist) + 3) & ~size_t{3};
+        DevBuf<float> accm(static_cast<size_t>(nb) * ld, st);
+        DevBuf<int> redo(nb, st), err(1, st);
+        DevBuf<unsigned long long> ncand(1, st);
+        QG_CUDA(cudaMemsetAsync(ncand.get(), 0, sizeof(unsigned long long), st));
+        QG_CUDA(cudaMemsetAsync(redo.get(), 0, nb * sizeof(int), st));
+        QG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
+        const int kblocks = (qdpad + KA - 1) / KA;
+        const CUtensorMap tmA = make_map(qh.get(), nb, qdpad, BM, true);
+        const CUtensorMap tmB = make_map(v.cent_f16, nlist, v.cent_dpad, BN, true);
+        const size_t smem = std::max<size_t>(filter_smem_bytes(kblocks), 116 * 1024);
+        allow_large_smem<k_mm_filter>();
+        MmArgs a{};
+        a.nq = nb;
+        a.n0 = 0;
+        a.n1 = nlist;
+        a.kblocks = kblocks;
+        a.ksteps = (d + 15) / 16;
+        a.mtiles = static_cast<int>(ceil_div(static_cast<size_t>(nb), BM));
+        a.ntiles = static_cast<int>(ceil_div(static_cast<size_t>(nlist), BN));
+        a.err = err.get();
+        a.store = accm.get();
+        a.ld = ld;
+        a.f16 = 1;
+        {
+            KernelTimer kt("coarse_mm", st);
+            k_mm_filter<<<static_cast<unsigned>(std::min(a.mtiles * a.ntiles, sm_count())), kThreads, smem, st>>>(tmA,
+                                                                                                               tmB, a);
+            QG_LAUNCH_CHECK();
+        }
+        const int cap = coarse_cap(nlist, P);
+        const size_t rsm = coarse_recheck_smem(nlist, d, cap);
+        allow_large_smem<k_coarse_recheck>();
+        // f16 inputs: unit roundoff 2^-11 in place of bf16's 2^-8 (subnormal
+        // rounding of the scaled rows is far below the 2^-14 term)
+        const double C = std::ldexp(1.0, -10) + std::ldexp(1.0, -14) + d * std::ldexp(1.0, -19);
+        // the bound's factors as floats rounded outwards
+        const float c_up = v.ip_metric ? std::nextafter(static_cast<float>(0.5 * C), 1.0f)
+                                       : std::nextafter(static_cast<float>(1.0 + C), 2.0f);
+        const float c_lo = std::nextafter(static_cast<float>(1.0 - C), 0.0f);
+        {
+            KernelTimer kt("coarse_recheck", st);
+            k_coarse_recheck<<<static_cast<unsigned>(nb), 256, rsm, st>>>(
+                q + q0 * d, qsq.get(), qexp.get(), v.centroids, v.cent_sq, v.cent_exp, nlist, d, v.ip_metric, c_up,
+                c_lo, accm.get(), ld, P, cap, probe + q0 * P, pdist + q0 * P, redo.get(), ncand.get());
+            QG_LAUNCH_CHECK();
+        }
+        int herr = 0;
+        unsigned long long hcand = 0;
+        std::vector<int> hredo(nb);
+        QG_CUDA(cudaMemcpyAsync(&hcand, ncand.get(), sizeof(hcand), cudaMemcpyDeviceToHost, st));
+        QG_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+        QG_CUDA(cudaMemcpyAsync(hredo.data(), redo.get(), nb * sizeof(int), cudaMemcpyDeviceToHost, st));
+        QG_CUDA(cudaStreamSynchronize(st));
+        require(herr == 0, "tensor-core coarse step: a pipeline wait timed out", kRuntimeError);
+        count_tensor_coarse_candidates(static_cast<int64_t>(hcand));
+        for (int i = 0; i < nb; ++i)
+            if (hredo[i]) redo_q.push_back(static_cast<int>(q0) + i);
+    }
+}
+
+void prepare_f16_rows(const float* rows, size_t n, int dim, DevBuf<uint16_t>& f16, DevBuf<float>& sq,
+                      DevBuf<int>& exps, int& dpad, cudaStream_t st) {
+    require(mm_supported(dim), "the tensor-core path supports dim <= 128", kUnsupported);
+    dpad = (dim + 7) & ~7;
+    f16.alloc(std::max<size_t>(1, n * dpad), st);
+    sq.alloc(std::max<size_t>(1, n), st);
+    exps.alloc(std::max<size_t>(1, n), st);
+    if (n) {
+        k_mm_prep16<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, st>>>(
+            rows, n, dim, dpad, reinterpret_cast<__half*>(f16.get()), sq.get(), exps.get());
+        QG_LAUNCH_CHECK();
+    }
 }
 
 } // namespace qg

@@ -123,6 +123,29 @@ bool use_tensor_filter(size_t nq, size_t n, int dim, size_t k) {
            (mode == 2 || (nq >= 64 && static_cast<double>(nq) * double(n) * dim >= 2e10));
 }
 
+namespace {
+std::atomic<int64_t> g_coarse_queries{0}, g_coarse_redone{0}, g_coarse_candidates{0};
+}
+
+void count_tensor_coarse_candidates(int64_t n) { g_coarse_candidates += n; }
+int64_t tensor_coarse_candidates() { return g_coarse_candidates.load(); }
+
+void count_tensor_coarse(int64_t queries, int64_t redone) {
+    g_coarse_queries += queries;
+    g_coarse_redone += redone;
+}
+
+void tensor_coarse_counts(int64_t* queries, int64_t* redone) {
+    *queries = g_coarse_queries.load();
+    *redone = g_coarse_redone.load();
+}
+
+bool use_tensor_coarse(size_t nq, int nlist, int dim) {
+    const int mode = g_tensor_filter.load();
+    return mode > 0 && mm_supported(dim) &&
+           (mode == 2 || (nq >= 64 && static_cast<double>(nq) * nlist * dim >= 1e9));
+}
+
 void flat_candidates(const float* q_dev, size_t nq, const float* rows_dev, size_t n, int dim, bool ip, size_t k,
                      const uint64_t* allow_dev, const uint64_t* deny_dev, uint64_t* out_key, uint32_t* out_slot,
                      cudaStream_t st, bool allow_mm, const MmRows* pre) {

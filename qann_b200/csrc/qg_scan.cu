@@ -29,6 +29,7 @@
 #include "qg_device.cuh"
 #include "qg_search.h"
 #include "qg_sm100.cuh"
+#include "qg_train.h"
 
 #include <algorithm>
 #include <atomic>
@@ -186,91 +187,6 @@ __device__ __forceinline__ int upper_index(const uint32_t* pre, int n, uint32_t 
         else hi = mid - 1;
     }
     return lo;
-}
-
-// One warp keeps the `keep` smallest of the n distinct keys buf[0, n) in
-// buf[0, keep) (in no particular order) and returns the largest kept key.
-// Radix select, 8 bits at a time from the top: each pass counts the keys
-// that share the prefix chosen so far by their next digit, and takes the
-// digit whose bin holds the keep-th key; it stops once every key of that
-// bin is kept. hist: 256 ints of warp-private shared scratch. n > keep >= 1.
-__device__ __noinline__ uint64_t warp_select_keep(uint64_t* buf, int n, int keep, int* hist) {
-    const int lane = threadIdx.x & 31;
-    constexpr unsigned kFull = 0xffffffffu;
-    uint64_t prefix = 0, mask = 0;
-    int need = keep;   // keys still to take among those that match the prefix
-    int shift = 56;
-    for (;; shift -= 8) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) hist[8 * lane + j] = 0;
-        __syncwarp();
-        for (int i = lane; i < n; i += 32) {
-            const uint64_t k = buf[i];
-            if ((k & mask) == prefix) atomicAdd(&hist[static_cast<int>(k >> shift) & 255], 1);
-        }
-        __syncwarp();
-        int c[8], own = 0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            c[j] = hist[8 * lane + j];
-            own += c[j];
-        }
-        int incl = own;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(kFull, incl, o);
-            if (lane >= o) incl += t;
-        }
-        const int excl = incl - own;
-        const unsigned owner = __ballot_sync(kFull, excl < need && need <= incl);
-        const int ol = __ffs(owner) - 1;
-        int digit = 0, below = 0, cnt = 0;
-        if (lane == ol) {
-            int acc = excl;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                if (cnt == 0 && acc + c[j] >= need) {
-                    digit = 8 * lane + j;
-                    below = acc;
-                    cnt = c[j];
-                }
-                acc += c[j];
-            }
-        }
-        digit = __shfl_sync(kFull, digit, ol);
-        below = __shfl_sync(kFull, below, ol);
-        cnt = __shfl_sync(kFull, cnt, ol);
-        need -= below;
-        prefix |= static_cast<uint64_t>(digit) << shift;
-        mask |= 0xFFull << shift;
-        __syncwarp();
-        if (cnt == need || shift == 0) break;   // (at shift 0 the bin is one key)
-    }
-    // kept: every key whose bits above `shift` do not exceed the prefix
-    const uint64_t lim = prefix | ((1ull << shift) - 1);
-    int out = 0;
-    uint64_t kmax = 0;
-    for (int base = 0; base < n; base += 32) {
-        const int i = base + lane;
-        uint64_t k = 0;
-        bool in = false;
-        if (i < n) {
-            k = buf[i];
-            in = k <= lim;
-        }
-        const unsigned bal = __ballot_sync(kFull, in);
-        __syncwarp();
-        if (in) {
-            buf[out + __popc(bal & ((1u << lane) - 1))] = k;
-            kmax = k > kmax ? k : kmax;
-        }
-        out += __popc(bal);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        const uint64_t t = __shfl_xor_sync(kFull, kmax, o);
-        kmax = t > kmax ? t : kmax;
-    }
-    __syncwarp();
-    return kmax;
 }
 
 // Shared memory of one block. The LUT ring shares its space with the
@@ -790,13 +706,41 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
         P = filtered_probes(v, s, probe, pdist, nprobe_q, st);
         probes_of = nprobe_q.get();
     } else {
-        // coarse: all pair scores, then the P nearest lists per query
-        DevBuf<float> scores(static_cast<size_t>(nq) * v.nlist, st);
-        pair_scores(s.q, nq, v.centroids, v.nlist, v.dim, v.ip_metric, scores.get(), v.nlist, st);
         probe.alloc(static_cast<size_t>(nq) * P, st);
         pdist.alloc(static_cast<size_t>(nq) * P, st);
-        // (score, list) compared as the reference's heap of (float, uint16_t) pairs does: -0 == +0
-        select_rows(scores.get(), v.nlist, nq, v.nlist, P, probe.get(), pdist.get(), st, nullptr, nullptr, 0, true);
+        // coarse: exact pair scores, then the P nearest lists per query by
+        // (score, list), compared as the reference's heap of (float, uint16_t)
+        // pairs does: -0 == +0 (for queries `sel` of the batch, or all)
+        auto exact_coarse = [&](const float* qs, int n, uint32_t* pr, float* pd) {
+            DevBuf<float> scores(static_cast<size_t>(n) * v.nlist, st);
+            pair_scores(qs, n, v.centroids, v.nlist, v.dim, v.ip_metric, scores.get(), v.nlist, st);
+            select_rows(scores.get(), v.nlist, n, v.nlist, P, pr, pd, st, nullptr, nullptr, 0, true);
+        };
+        if (use_tensor_coarse(nq, v.nlist, v.dim) && coarse_mm_supported(v.nlist, v.dim, P, v.cent_f16 != nullptr)) {
+            std::vector<int> redo;
+            coarse_probes_mm(v, s.q, nq, P, probe.get(), pdist.get(), redo, st);
+            count_tensor_coarse(nq, static_cast<int64_t>(redo.size()));
+            if (!redo.empty()) {
+                // queries with too many near-ties: the exact path, results copied into place
+                const size_t m = redo.size();
+                std::vector<uint32_t> hidx(redo.begin(), redo.end());
+                DevBuf<uint32_t> idx(m, st);
+                QG_CUDA(cudaMemcpyAsync(idx.get(), hidx.data(), m * 4, cudaMemcpyHostToDevice, st));
+                DevBuf<float> qs(m * v.dim, st);
+                gather_rows(s.q, idx.get(), m, v.dim, qs.get(), st);
+                DevBuf<uint32_t> pr(m * P, st);
+                DevBuf<float> pd(m * P, st);
+                exact_coarse(qs.get(), static_cast<int>(m), pr.get(), pd.get());
+                for (size_t j = 0; j < m; ++j) {
+                    QG_CUDA(cudaMemcpyAsync(probe.get() + static_cast<size_t>(redo[j]) * P, pr.get() + j * P, P * 4,
+                                            cudaMemcpyDeviceToDevice, st));
+                    QG_CUDA(cudaMemcpyAsync(pdist.get() + static_cast<size_t>(redo[j]) * P, pd.get() + j * P, P * 4,
+                                            cudaMemcpyDeviceToDevice, st));
+                }
+            }
+        } else {
+            exact_coarse(s.q, nq, probe.get(), pdist.get());
+        }
     }
 
     DevBuf<float> pterm(static_cast<size_t>(nq) * P, st);

@@ -294,7 +294,11 @@ __global__ void k_probe_terms(IvfView v, const float* __restrict__ q, int nq, in
     const int qi = static_cast<int>(i / P);
     const uint32_t list = probe[i];
     float A = pdist[i];
-    if (v.has_resid) A = exact_avx2<true>(q + static_cast<size_t>(qi) * v.dim, v.resid + static_cast<size_t>(list) * v.dim, v.dim);
+    if (v.has_resid) {
+        const float* qa = q + static_cast<size_t>(qi) * v.dim;
+        const float* rc = v.resid + static_cast<size_t>(list) * v.dim;
+        A = (v.dim & 3) == 0 ? exact_avx2_vec<true>(qa, rc, v.dim) : exact_avx2<true>(qa, rc, v.dim);
+    }
     if (v.mode == kModeCosIP) A = __fsub_rn(__fadd_rn(A, 1.0f), v.sqnorm[list]);
     term[i] = A;
 }

@@ -7,6 +7,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace qg {
 
@@ -34,6 +35,11 @@ struct IvfView {
     const uint4* codes = nullptr;       // superblocks, 2 * m_pad uint4 each
     const uint32_t* ids = nullptr;      // 64 slots per superblock, kRemoved for padding
     const uint64_t* deleted = nullptr;  // slot bitmap of deleted vectors, or null
+    const uint16_t* cent_f16 = nullptr;    // f16 copy of the centroids, each row scaled by 2^cent_exp
+                                           // (cent_dpad per row), or null
+    const float* cent_sq = nullptr;        // |centroid|^2 in float
+    const int* cent_exp = nullptr;
+    int cent_dpad = 0;
 };
 
 // Per-query settings of a mixed batch: served requests that each carry their
@@ -107,6 +113,26 @@ int filtered_probes(const IvfView& v, const IvfSearchArgs& s, DevBuf<uint32_t>& 
 // The k' = s.kp best candidates of each query, as sorted (key64, slot) lists
 // (key64 = key(dist) << 32 | push index; 0xFFFF... marks an empty entry).
 void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st);
+// Coarse assignment through the tensor cores (qg_mm.cu): the P nearest lists
+// of each query by exact score, ties by list, from BF16 estimates with an
+// error bound and an exact recheck; queries with too many near-ties are
+// listed in redo_q for the exact path. use_tensor_coarse: whether the batch
+// goes this way (the process-wide tensor-filter mode and the work's size).
+bool coarse_mm_supported(int nlist, int dim, int P, bool cent_prepared);
+bool use_tensor_coarse(size_t nq, int nlist, int dim);
+// Queries whose coarse step went through the tensor cores, and those of them redone exactly.
+void count_tensor_coarse(int64_t queries, int64_t redone);
+void tensor_coarse_counts(int64_t* queries, int64_t* redone);
+// Lists rescored exactly by the tensor-core coarse step so far (its candidates).
+void count_tensor_coarse_candidates(int64_t n);
+int64_t tensor_coarse_candidates();
+void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t* probe, float* pdist,
+                      std::vector<int>& redo_q, cudaStream_t st);
+// Rows scaled by powers of two (2^exps) and rounded to f16 (zero-padded to
+// dpad, a multiple of 8), with their float squared norms (unscaled).
+void prepare_f16_rows(const float* rows, size_t n, int dim, DevBuf<uint16_t>& f16, DevBuf<float>& sq,
+                      DevBuf<int>& exps, int& dpad, cudaStream_t st);
+
 // The scan's shape autotuner: on (1, the default) it times the candidate
 // shapes on the first large search of each problem key; off (0) every search
 // uses the first candidate. The variant restricts the candidates: -1 any, 0

@@ -119,6 +119,13 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
            | (static_cast<uint32_t>(M >> 4) << 24);   // M / 16
 }
 
+// The same with F16 A and B (format code 0).
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N) {
+    return (1u << 4)                                  // D format F32
+           | (static_cast<uint32_t>(N >> 3) << 17)    // N / 8
+           | (static_cast<uint32_t>(M >> 4) << 24);   // M / 16
+}
+
 // D[tmem] (+)= A * B^T for one 16-deep K step; issued by one thread.
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, bool accumulate) {
     const uint32_t no_mask = 0;   // no output lanes disabled

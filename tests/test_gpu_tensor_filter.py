@@ -112,3 +112,65 @@ def test_assignment_in_training_and_adding(tmp_path):
 
     a, b = both_modes(lambda: build(tmp_path / f"m{qb.tensor_filter()}.qann"))
     assert filecmp.cmp(a, b, shallow=False)
+
+
+def coarse_runs(fn):
+    """fn on the exact coarse path and through the tensor cores; the tensor
+    path must have answered the queries."""
+    qb.set_tensor_filter(0)
+    exact = fn()
+    qb.set_tensor_filter(2)
+    before = qb.tensor_filter_counts()
+    fast = fn()
+    after = qb.tensor_filter_counts()
+    assert after["coarse_queries"] > before["coarse_queries"], "the tensor-core coarse step did not run"
+    return exact, fast, after["coarse_redone"] - before["coarse_redone"]
+
+
+@pytest.mark.parametrize("metric", [0, 1, 2])
+@pytest.mark.parametrize("d", [24, 100, 128])
+def test_coarse_identical(metric, d):
+    """IVF search with the coarse step on the tensor cores returns exactly the
+    exact path's results, for nprobe from 1 to most of the lists, also for
+    queries far from every list (their bounds overlap: many lists rescored)."""
+    x = clustered(d, 20000, d, centres=300, sigma=0.2)
+    ivf = qb.IVFIndex(d, 400, 8, metric=qb.Metric(metric))
+    ivf.enable_pq({24: 12, 100: 50, 128: 32}[d], fast_scan=True)
+    ivf.train(x, seed=5)
+    idx = qb.RefineIndex(ivf, 4)
+    idx.add(x)
+    q = clustered(d + 7, 200, d, centres=300, sigma=0.25)
+    far = np.full((3, d), 1000.0, dtype=np.float32)
+    qs = np.vstack([q, far])
+    for nprobe in (1, 16, 200):
+        ivf.nprobe = nprobe
+        for k in (1, 10):
+            exact, fast, _ = coarse_runs(lambda: idx.batch_query(qs, k))
+            assert_same(exact, fast)
+
+
+def test_coarse_overflow_redone_exactly():
+    """More lists within the error bound than the recheck holds (queries far
+    from every list, 2048 lists): those queries go back to the exact path."""
+    d = 32
+    x = clustered(11, 30000, d, centres=1000, sigma=0.2)
+    ivf = qb.IVFIndex(d, 2048, 16)
+    ivf.enable_pq(8, fast_scan=True)
+    ivf.train(x, seed=5)
+    ivf.add(x)
+    qs = np.vstack([clustered(12, 100, d, centres=1000, sigma=0.2), np.full((4, d), 1000.0, dtype=np.float32)])
+    exact, fast, redone = coarse_runs(lambda: ivf.batch_query(qs, 10))
+    assert_same(exact, fast)
+    assert redone >= 4
+
+
+@pytest.mark.parametrize("name", ["l2", "l2_adc", "ip", "cos_ip", "cos_l2", "l2_custom_del"])
+def test_coarse_matches_reference_files(golden, name):
+    """Reference-built indexes and their saved results, coarse step on the tensor cores."""
+    qb.set_tensor_filter(2)
+    for kind in ("ivf", "refine"):
+        idx = qb.load(golden / "gen" / f"{kind}_{name}.qann")
+        q = np.load(golden / "gen" / "queries.npy")
+        ids, d = idx.batch_query(q, 10)
+        np.testing.assert_array_equal(ids, np.load(golden / "gen" / f"{kind}_{name}_ids.npy"))
+        np.testing.assert_array_equal(d, np.load(golden / "gen" / f"{kind}_{name}_dists.npy"))

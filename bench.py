@@ -370,6 +370,65 @@ def device_steps(index, q_dev, nq, k, steps, warmup, flush=None):
     return times, oi, od
 
 
+def small_workload(args):
+    """The reference's own CPU-scale case: base 100,000 x 128 uniform [0, 1)
+    (seeded), squared L2, nlist 256 k-means (seed 1), PQ 64 x 4-bit fast-scan,
+    nprobe 16, RefineIndex k_factor 10, 1,000 queries of the same law, k = 10."""
+    import torch
+    import qann_b200 as qb
+    from qann_b200 import profiling
+    n, d, nq, k = 100_000, 128, 1_000, 10
+    x = np.random.default_rng(0).random((n, d), dtype=np.float32)
+    q = np.random.default_rng(1).random((nq, d), dtype=np.float32)
+    ivf = qb.IVFIndex(d, 256, 16)
+    ivf.enable_pq(64, fast_scan=True)
+    ivf.train(x, seed=1)
+    index = qb.RefineIndex(ivf, 10)
+    index.add(x)
+    dev = torch.device("cuda:0")
+    q_dev = torch.from_numpy(q).to(dev)
+    profiling.enable(True)
+    launches0 = profiling.launch_count()
+    times, oi, _ = device_steps(index, q_dev, nq, k, args.steps, args.warmup)
+    launches = profiling.launch_count() - launches0
+    profiling.enable(False)
+    ids = oi.cpu().numpy()
+    xt = torch.from_numpy(x).to(dev)
+    gt = torch.topk(torch.cdist(q_dev.double(), xt.double()), k, largest=False).indices.cpu().numpy()
+    rec = recall(ids, gt)
+    t = time.perf_counter()
+    e_ids, _ = index.batch_query(q, k)
+    e2e = nq / (time.perf_counter() - t)
+    cpu, same = None, None
+    if not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            path = CACHE / "small_100000x128.qann"
+            CACHE.mkdir(parents=True, exist_ok=True)
+            index.save(path)
+            r = ref.load(path)
+            cores = os.cpu_count() or 1
+            ref.set_num_threads(cores)
+            t = time.perf_counter()
+            r_ids, _ = r.batch_query(q, k)
+            dt = time.perf_counter() - t
+            same = bool(np.array_equal(r_ids, e_ids))
+            cpu = {"value": round(nq / dt, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
+                   "sample": f"all {nq} queries, one batch_query on {cores} threads, the same .qann index"}
+    total = sum(times)
+    print(json.dumps({
+        "metric": "QPS (100k x 128 uniform, IVF256-PQ64x4fs + refine kf10, nprobe 16, k=10)",
+        "value": round(nq * args.steps / (total / 1e3), 1), "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "small_100000x128_nl256_m64_kf10", "nprobe": 16, "recall@10": round(rec, 4),
+                   "results_equal_reference": same},
+        "e2e": {"value": round(e2e, 1), "unit": "queries/s", "h2d_bytes_per_step": nq * d * 4,
+                "d2h_bytes_per_step": nq * k * 12},
+        "gpu_launches": launches, "cpu_baseline": cpu}))
+    return 0
+
+
 def flat_workload(args):
     """Exact flat search as a GEMM: 10,000,000 x 96 float32 (N(0,1) per
     dimension, rows scaled by LogNormal(0, 0.25)), 10,000 queries of the same
@@ -597,13 +656,14 @@ def main():
     ap.add_argument("--nprobe", type=int, default=0, help="use this nprobe instead of the recall sweep (profiling)")
     ap.add_argument("--scan-shape", default="auto", choices=["auto", "global", "staged"],
                     help="fast-scan kernel shape: autotuned (default) or fixed (profiling)")
-    ap.add_argument("--workload", default="angular", choices=["angular", "flat", "train", "served"],
-                    help="angular: the headline line; flat / train / served: the other configurations")
+    ap.add_argument("--workload", default="angular", choices=["angular", "small", "flat", "train", "served"],
+                    help="angular: the headline line; small / flat / train / served: the other configurations")
     args = ap.parse_args()
     if args.workload != "angular" and args.impl == "qann_b200":
         import torch
         torch.cuda.set_device(0)
-        return {"flat": flat_workload, "train": train_workload, "served": served_workload}[args.workload](args)
+        return {"small": small_workload, "flat": flat_workload, "train": train_workload,
+                "served": served_workload}[args.workload](args)
     cfg = SMALL if args.small else FULL
     if args.impl == "reference":
         return reference_arm(args, cfg)

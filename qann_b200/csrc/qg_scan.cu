@@ -41,6 +41,7 @@ namespace qg {
 
 namespace {
 constexpr int kMaxChunk = 256;   // probes per work unit at most
+constexpr int kMinChunk = 8;     // probes per work unit at least, when the query has that many
 constexpr int kSbPerWarp = 4;    // superblocks a warp takes at a time, one per octet
 // Row stride (floats) of the query's table C in shared memory: 80 bytes puts
 // the 16-byte reads of 8 lanes (one row each) on distinct banks.
@@ -757,7 +758,9 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
 
     // chunks: enough blocks to fill the GPU several times over, at most kMaxChunk probes each
     const int sms = s.sm_count > 0 ? s.sm_count : 148;
-    int nchunks = std::clamp(static_cast<int>(ceil_div(static_cast<size_t>(4 * sms), nq)), 1, P);
+    // (and at least kMinChunk probes a chunk, so the merge stays small for small batches)
+    int nchunks = std::clamp(static_cast<int>(ceil_div(static_cast<size_t>(4 * sms), nq)), 1,
+                             std::max(1, P / kMinChunk));
     nchunks = std::max(nchunks, static_cast<int>(ceil_div(P, kMaxChunk)));
     const int pch = static_cast<int>(ceil_div(P, nchunks));
     nchunks = static_cast<int>(ceil_div(P, pch));

@@ -341,30 +341,103 @@ __global__ void k_query_tables(IvfView v, const float* __restrict__ q, float* __
 // Merge: the k' smallest key64 of a query's chunk outputs, sorted. The buffer
 // holds the current best k' and the next batch of entries.
 // ---------------------------------------------------------------------------
+// The k' best of a query's chunk lists (each sorted, ~0 for empty entries):
+// a block-wide radix select of the k'-th smallest valid key, 8 bits a pass
+// from the top and stopping once every key of the chosen bin is kept, then
+// the survivors compacted and sorted. One block per query.
+// ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_merge(const uint64_t* __restrict__ in_key, const uint32_t* __restrict__ in_slot,
-                                               int nchunks, int kp, int capm, uint64_t* __restrict__ out_key,
+                                               int nchunks, int kp, int npow, uint64_t* __restrict__ out_key,
                                                uint32_t* __restrict__ out_slot) {
     extern __shared__ uint8_t sm_raw[];
-    uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);
-    int64_t* val = reinterpret_cast<int64_t*>(key + capm);
+    uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);   // npow
+    int64_t* val = reinterpret_cast<int64_t*>(key + npow);
+    __shared__ int hist[256], s_pick[3], s_valid, s_count;
     const int qi = blockIdx.x;
-    const size_t total = static_cast<size_t>(nchunks) * kp;
+    const int total = nchunks * kp;
     const uint64_t* ik = in_key + static_cast<size_t>(qi) * total;
     const uint32_t* is = in_slot + static_cast<size_t>(qi) * total;
-    for (int i = threadIdx.x; i < kp; i += blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        s_valid = 0;
+        s_count = 0;
+    }
+    __syncthreads();
+    int mine = 0;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) mine += ik[e] != ~0ull;
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+    if (lane == 0) atomicAdd(&s_valid, mine);
+    __syncthreads();
+    uint64_t lim = ~0ull - 1;   // every valid key
+    if (s_valid > kp) {
+        uint64_t prefix = 0, mask = 0;
+        int need = kp, shift = 56;
+        for (;; shift -= 8) {
+            for (int j = threadIdx.x; j < 256; j += blockDim.x) hist[j] = 0;
+            __syncthreads();
+            for (int b0 = 0; b0 < total; b0 += blockDim.x) {   // (trip count is block-uniform)
+                const int e = b0 + threadIdx.x;
+                const uint64_t k = e < total ? ik[e] : ~0ull;
+                const bool in = k != ~0ull && (k & mask) == prefix;
+                const int bin = in ? static_cast<int>((k >> shift) & 255) : -1;
+                const unsigned same = __match_any_sync(0xffffffffu, bin);
+                if (in && lane == __ffs(same) - 1) atomicAdd(&hist[bin], __popc(same));
+            }
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                int c[8], own = 0;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    c[j] = hist[8 * lane + j];
+                    own += c[j];
+                }
+                int incl = own;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int excl = incl - own;
+                if (excl < need && need <= incl) {
+                    int acc = excl;
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        if (acc + c[j] >= need) {
+                            s_pick[0] = 8 * lane + j;
+                            s_pick[1] = acc;
+                            s_pick[2] = c[j];
+                            break;
+                        }
+                        acc += c[j];
+                    }
+                }
+            }
+            __syncthreads();
+            need -= s_pick[1];
+            prefix |= static_cast<uint64_t>(s_pick[0]) << shift;
+            mask |= 0xFFull << shift;
+            const bool done = s_pick[2] == need || shift == 0;
+            __syncthreads();
+            if (done) break;
+        }
+        lim = prefix | ((1ull << shift) - 1);
+    }
+    // the survivors (at most kp), then sorted
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const uint64_t k = ik[e];
+        if (k != ~0ull && k <= lim) {
+            const int pos = atomicAdd(&s_count, 1);
+            if (pos < npow) {
+                key[pos] = k;
+                val[pos] = static_cast<int64_t>(is[e]);
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = min(s_count, npow) + threadIdx.x; i < npow; i += blockDim.x) {
         key[i] = ~0ull;
         val[i] = INT64_MAX;
     }
-    const int batch = capm - kp;
-    for (size_t b0 = 0; b0 < total; b0 += batch) {
-        for (int i = threadIdx.x; i < batch; i += blockDim.x) {
-            const size_t e = b0 + i;
-            const bool ok = e < total && ik[e] != ~0ull;
-            key[kp + i] = ok ? ik[e] : ~0ull;
-            val[kp + i] = ok ? static_cast<int64_t>(is[e]) : INT64_MAX;
-        }
-        bitonic_sort(key, val, capm);
-    }
+    bitonic_sort(key, val, npow);
     for (int i = threadIdx.x; i < kp; i += blockDim.x) {
         out_key[static_cast<size_t>(qi) * kp + i] = key[i];
         out_slot[static_cast<size_t>(qi) * kp + i] = key[i] == ~0ull ? 0xFFFFFFFFu : static_cast<uint32_t>(val[i]);
@@ -576,12 +649,12 @@ void query_tables(const IvfView& v, const float* q, int nq, float* qC, uint4* ql
 void merge_candidates(const uint64_t* in_key, const uint32_t* in_slot, int nq, int nchunks, int kp, uint64_t* out_key,
                       uint32_t* out_slot, cudaStream_t st) {
     if (nq == 0) return;
-    const int capm = next_pow2(2 * kp);
-    const size_t msm = static_cast<size_t>(capm) * 16;
+    const int npow = next_pow2(std::max(2, kp));
+    const size_t msm = static_cast<size_t>(npow) * 16;
     if (msm > 48 * 1024)
         allow_large_smem<k_merge>();
     KernelTimer kt("merge", st);
-    k_merge<<<nq, 256, msm, st>>>(in_key, in_slot, nchunks, kp, capm, out_key, out_slot);
+    k_merge<<<nq, 256, msm, st>>>(in_key, in_slot, nchunks, kp, npow, out_key, out_slot);
     QG_LAUNCH_CHECK();
 }
 

@@ -283,8 +283,8 @@ def reference_arm(args, cfg):
 
 # ---- our arm -------------------------------------------------------------------------------------
 
-def served(index, queries, k, nprobe, batch_ids, rates=(25_000, 50_000, 100_000, 200_000), per_rate=20_000,
-           slots=4, max_batch=256):
+def served(index, queries, k, nprobe, batch_ids, rates=(25_000, 50_000, 100_000, 200_000, 300_000, 400_000),
+           per_rate=20_000, slots=4, max_batch=256):
     """Open-loop Poisson arrivals through the continuous-batching server:
     achieved QPS and p50 / p99 latency (arrival to results) per offered rate;
     every served result must equal the batch path's."""
@@ -311,9 +311,28 @@ def served(index, queries, k, nprobe, batch_ids, rates=(25_000, 50_000, 100_000,
                         "requests": n})
             log(f"served at {rate}/s: {out[-1]}")
         st = srv.stats()
+    ok = [r for r in out if r["p99_ms"] <= 2.0]
+    best = max(ok, key=lambda r: r["achieved_qps"]) if ok else None
     return {"slots": slots, "max_batch": max_batch, "k": k, "nprobe": nprobe, "arrivals": "Poisson, open loop",
             "latency": "arrival to results on the host", "rates": out, "mean_batch": round(st["completed"] / st["batches"], 1),
-            "results_equal_batch_path": same}
+            "results_equal_batch_path": same, "best_qps_at_p99_le_2ms": best["achieved_qps"] if best else None}
+
+
+def plain_fp32_qps(base, queries, k, metric):
+    """The plain FP32 GPU batch path on the same rows: exact flat search with
+    FP32 tiles only (no tensor cores, no index), through the public API."""
+    import qann_b200 as qb
+    flat = qb.FlatIndex(base.shape[1], metric=metric)
+    flat.add(base)
+    qb.set_tensor_filter(0)
+    try:
+        flat.batch_query(queries[:200], k)   # warm-up
+        n = min(2000, queries.shape[0])
+        t = time.perf_counter()
+        flat.batch_query(queries[:n], k)
+        return n / (time.perf_counter() - t)
+    finally:
+        qb.set_tensor_filter(1)
 
 
 def cpu_baseline(cfg, path, queries, nprobe):
@@ -776,7 +795,13 @@ def main():
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
     peak, peak_src = measured_peak("hbm_gbs", 6650.0)
     traffic = scan_traffic()
-    serving = None if args.no_served else served(index, queries, k, nprobe, ids_h)
+    serving = None
+    if not args.no_served:
+        serving = served(index, queries, k, nprobe, ids_h)
+        fp32 = plain_fp32_qps(base, queries, k, qb.Metric.Cosine)
+        serving["plain_fp32_gpu_batch_qps"] = round(fp32, 1)
+        if serving["best_qps_at_p99_le_2ms"]:
+            serving["served_over_plain_fp32"] = round(serving["best_qps_at_p99_le_2ms"] / fp32, 1)
     cpu = None if (args.no_cpu_baseline or world > 1) else cpu_baseline(cfg, path, queries, nprobe)
     srt = sorted(step_ms)
     line = {

@@ -192,7 +192,15 @@ int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, con
  *   "scan_tuned_shapes" (problems tuned so far) and "scan_last_shape" (the
  *   last scan's shape: warps * 1000 + lists per group * 10 + staged). Results are the same under
  *   every shape. No counterpart in the reference, whose scan kernel is fixed
- *   (reference src/fast_scan.cpp:306-338). */
+ *   (reference src/fast_scan.cpp:306-338).
+ * "search_graphs": 1 makes qg_search_device replay device-resident, unfiltered
+ *   searches of an IVF index (or a RefineIndex over one) as CUDA graphs. The
+ *   first call with a given batch size, k, nprobe, k_factor, buffers and stream
+ *   (a non-default stream) runs the search and captures it; later calls launch
+ *   the graph and read its error flags. A change to the index invalidates its
+ *   graphs. 0 (default) runs every search directly. qg_get_option also reads
+ *   "search_graph_replays" and "search_graph_captures". No counterpart in the
+ *   reference, which has no GPU path. */
 int qg_set_option(const char* key, int64_t value);
 int qg_get_option(const char* key, int64_t* value);
 

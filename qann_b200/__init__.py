@@ -116,6 +116,22 @@ def set_scan_options(autotune: bool | None = None, variant: int | None = None) -
         check(_lib.lib.qg_set_option(b"scan_variant", int(variant)))
 
 
+def set_search_graphs(on: bool) -> None:
+    """search_device replays fixed-shape, unfiltered IVF searches as CUDA
+    graphs (captured on the first call with each batch size, k, nprobe and
+    buffers). Off by default; results are identical either way."""
+    check(_lib.lib.qg_set_option(b"search_graphs", int(bool(on))))
+
+
+def search_graph_counts() -> dict:
+    out = {}
+    for key in ("replays", "captures"):
+        v = C.c_int64()
+        check(_lib.lib.qg_get_option(f"search_graph_{key}".encode(), C.byref(v)))
+        out[key] = v.value
+    return out
+
+
 def scan_options() -> dict:
     out = {}
     for key in ("autotune", "variant", "tuned_shapes", "last_shape"):

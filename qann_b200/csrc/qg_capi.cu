@@ -251,7 +251,7 @@ static int search_common(qg_index* h, const float* q, size_t nq, size_t k, const
     r.out_ids = out_ids;
     r.out_d = out_d;
     r.io = io;
-    search(o, r, st);
+    if (!search_graph(o, r, st)) search(o, r, st);
     return QG_OK;
 }
 
@@ -520,6 +520,9 @@ int qg_set_option(const char* key, int64_t value) {
         if (k == "tensor_filter") {
             require(value >= 0 && value <= 2, "tensor_filter must be 0, 1 or 2");
             set_tensor_filter(static_cast<int>(value));
+        } else if (k == "search_graphs") {
+            require(value == 0 || value == 1, "search_graphs must be 0 or 1");
+            set_search_graphs(static_cast<int>(value));
         } else if (k == "scan_autotune") {
             require(value == 0 || value == 1, "scan_autotune must be 0 or 1");
             set_scan_autotune(static_cast<int>(value));
@@ -547,6 +550,12 @@ int qg_get_option(const char* key, int64_t* value) {
             *value = k == "tensor_coarse_queries" ? cq : cr;
         }
         else if (k == "tensor_coarse_candidates") *value = tensor_coarse_candidates();
+        else if (k == "search_graphs") *value = search_graphs();
+        else if (k == "search_graph_replays" || k == "search_graph_captures") {
+            int64_t rp = 0, cp = 0;
+            search_graph_counts(&rp, &cp);
+            *value = k == "search_graph_replays" ? rp : cp;
+        }
         else if (k == "scan_autotune") *value = scan_autotune();
         else if (k == "scan_variant") *value = scan_variant();
         else if (k == "scan_tuned_shapes") *value = scan_tuned_shapes();

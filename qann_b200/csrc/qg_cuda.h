@@ -70,6 +70,8 @@ class KernelTimer {
 public:
     KernelTimer(const char* name, cudaStream_t st) : st_(st) {
         if (!profiler().on.load(std::memory_order_relaxed)) return;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;   // no timers inside a graph capture
+        if (cudaStreamIsCapturing(st_, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
         name_ = name;
         if (cudaEventCreate(&a_) != cudaSuccess || cudaEventCreate(&b_) != cudaSuccess) return;
         cudaEventRecord(a_, st_);

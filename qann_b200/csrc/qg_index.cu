@@ -226,6 +226,7 @@ void ensure_device(IVFObj& o, cudaStream_t) {
         v.cent_exp = D.cent_exp.get();
     }
     o.dev_dirty = false;
+    ++o.dev_gen;
 }
 
 static void upload_rows(DeviceRows& D, const std::vector<float>& rows, const IdMap& map, cudaStream_t st) {
@@ -241,6 +242,7 @@ void ensure_device(FlatObj& o, cudaStream_t) {
     if (!o.dev_dirty) return;
     upload_rows(o.dev, o.model.data, o.model.idmap, resident_stream());
     o.dev_dirty = false;
+    ++o.dev_gen;
 }
 
 void ensure_device(RefineObj& o, cudaStream_t st) {
@@ -249,6 +251,7 @@ void ensure_device(RefineObj& o, cudaStream_t st) {
         if (o.dev_dirty) {
             upload_rows(o.dev, o.data, o.map, resident_stream());
             o.dev_dirty = false;
+            ++o.dev_gen;
         }
     }
     if (o.base->kind == Kind::IVF) ensure_device(static_cast<IVFObj&>(*o.base), st);

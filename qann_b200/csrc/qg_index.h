@@ -9,6 +9,7 @@
 #include <memory>
 #include <mutex>
 #include <shared_mutex>
+#include <vector>
 
 namespace qg {
 
@@ -34,11 +35,33 @@ struct DeviceRows {
     DevBuf<uint64_t> deleted;
 };
 
+// A captured device-resident search (search_graph).
+struct SearchGraph {
+    size_t nq = 0, k = 0, k_factor = 0;
+    int nprobe = 0;
+    const float* q = nullptr;
+    int64_t* ids = nullptr;
+    float* d = nullptr;
+    cudaStream_t st = nullptr;
+    uint64_t gen = 0;                 // device generation of the index (and its base) at capture
+    cudaGraphExec_t exec = nullptr;
+    int* err = nullptr;               // the search's error flags, read after each replay
+    int64_t launches = 0;             // kernels in the graph
+    bool failed = false;              // not capturable: the plain path serves this key
+    ~SearchGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (err) cudaFree(err);
+    }
+};
+
 struct IndexObj {
     Kind kind;
     mutable std::shared_mutex mu;     // shared for queries, exclusive for writes
     std::mutex dev_mu;                // guards (re)building the device copy
     bool dev_dirty = true;
+    uint64_t dev_gen = 0;             // bumped on every rebuild of the device copy
+    std::mutex graph_mu;              // guards `graphs`
+    std::vector<std::unique_ptr<SearchGraph>> graphs;
     bool wrapped = false;             // a RefineIndex wraps this index
     int device = 0;
     explicit IndexObj(Kind k) : kind(k) {}

@@ -614,7 +614,8 @@ __global__ void __launch_bounds__(256, 4) k_coarse_recheck(const float* __restri
     // overflow): the relative bound does not hold, so such a query takes the
     // exact path and such a list is always rescored
     auto extreme = [](float x2) { return (x2 > 0.0f && x2 < 0x1p-60f) || !(x2 < 0x1p60f); };
-    if (extreme(qq)) {
+    const bool all = extreme(qq);   // rescored in full here when there is no exact path to send it to
+    if (all && redo) {
         if (threadIdx.x == 0) redo[qi] = 1;
         return;
     }
@@ -648,7 +649,7 @@ __global__ void __launch_bounds__(256, 4) k_coarse_recheck(const float* __restri
         const float a = ldexpf(acc_j, -(qe + cej));
         const float lo = ip ? __fmaf_rd(-c_up, __fadd_ru(qq, c2j), -a)
                             : __fmaf_rd(-2.0f, a, __fmul_rd(c_lo, __fadd_rd(qq, c2j)));
-        return float_key(lo) <= T || extreme(c2j);
+        return all || float_key(lo) <= T || extreme(c2j);
     };
     auto push = [&](int j) {
         const int pos = atomicAdd(&s_count, 1);
@@ -667,9 +668,9 @@ __global__ void __launch_bounds__(256, 4) k_coarse_recheck(const float* __restri
         if (lower_in(arow[j], c2[j], cexp[j])) push(j);
     __syncthreads();
     const int cnt = s_count;
-    if (threadIdx.x == 0) atomicAdd(ncand, static_cast<unsigned long long>(cnt));
-    if (cnt > cap) {   // too many near-ties: this query takes the exact path
-        if (threadIdx.x == 0) redo[qi] = 1;
+    if (threadIdx.x == 0 && ncand) atomicAdd(ncand, static_cast<unsigned long long>(cnt));
+    if (cnt > cap) {   // too many near-ties: this query takes the exact path (cap >= nlist when redo is null)
+        if (threadIdx.x == 0 && redo) redo[qi] = 1;
         return;
     }
     // exact scores, one thread per candidate; each list's score is kept by
@@ -706,13 +707,15 @@ static int coarse_cap(int nlist, int P) {
     return std::min(next_pow2(nlist), std::max(1024, next_pow2(4 * P)));
 }
 
-bool coarse_mm_supported(int nlist, int dim, int P, bool cent_prepared) {
+bool coarse_mm_supported(int nlist, int dim, int P, bool cent_prepared, bool capture) {
+    const int cap = capture ? next_pow2(nlist) : coarse_cap(nlist, P);
     return cent_prepared && mm_supported(dim) && P >= 1 && P <= nlist && nlist <= 16384 &&
-           coarse_recheck_smem(nlist, dim, coarse_cap(nlist, P)) <= 200 * 1024;
+           coarse_recheck_smem(nlist, dim, cap) <= 200 * 1024;
 }
 
 void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t* probe, float* pdist,
-                      std::vector<int>& redo_q, cudaStream_t st) {
+                      std::vector<int>& redo_q, cudaStream_t st, int* capture_err) {
+    const bool capture = capture_err != nullptr;
     redo_q.clear();
     if (nq == 0) return;
     const int d = v.dim, nlist = v.nlist;
@@ -726,11 +729,16 @@ void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t*
         prepare_f16_rows(q + q0 * d, nb, d, qh, qsq, qexp, qdpad, st);
         const size_t ld = (static_cast<size_t>(nlist) + 3) & ~size_t{3};
         DevBuf<float> accm(static_cast<size_t>(nb) * ld, st);
-        DevBuf<int> redo(nb, st), err(1, st);
-        DevBuf<unsigned long long> ncand(1, st);
-        QG_CUDA(cudaMemsetAsync(ncand.get(), 0, sizeof(unsigned long long), st));
-        QG_CUDA(cudaMemsetAsync(redo.get(), 0, nb * sizeof(int), st));
-        QG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
+        DevBuf<int> redo, err;
+        DevBuf<unsigned long long> ncand;
+        if (!capture) {
+            redo.alloc(nb, st);
+            err.alloc(1, st);
+            ncand.alloc(1, st);
+            QG_CUDA(cudaMemsetAsync(ncand.get(), 0, sizeof(unsigned long long), st));
+            QG_CUDA(cudaMemsetAsync(redo.get(), 0, nb * sizeof(int), st));
+            QG_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
+        }
         const int kblocks = (qdpad + KA - 1) / KA;
         const CUtensorMap tmA = make_map(qh.get(), nb, qdpad, BM, true);
         const CUtensorMap tmB = make_map(v.cent_f16, nlist, v.cent_dpad, BN, true);
@@ -744,7 +752,7 @@ void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t*
         a.ksteps = (d + 15) / 16;
         a.mtiles = static_cast<int>(ceil_div(static_cast<size_t>(nb), BM));
         a.ntiles = static_cast<int>(ceil_div(static_cast<size_t>(nlist), BN));
-        a.err = err.get();
+        a.err = capture ? capture_err : err.get();
         a.store = accm.get();
         a.ld = ld;
         a.f16 = 1;
@@ -754,7 +762,7 @@ void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t*
                                                                                                                tmB, a);
             QG_LAUNCH_CHECK();
         }
-        const int cap = coarse_cap(nlist, P);
+        const int cap = capture ? next_pow2(nlist) : coarse_cap(nlist, P);   // captured: every list fits
         const size_t rsm = coarse_recheck_smem(nlist, d, cap);
         allow_large_smem<k_coarse_recheck>();
         // f16 inputs: unit roundoff 2^-11 in place of bf16's 2^-8 (subnormal
@@ -771,6 +779,7 @@ void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t*
                 c_lo, accm.get(), ld, P, cap, probe + q0 * P, pdist + q0 * P, redo.get(), ncand.get());
             QG_LAUNCH_CHECK();
         }
+        if (capture) continue;   // the flags are read after each replay
         int herr = 0;
         unsigned long long hcand = 0;
         std::vector<int> hredo(nb);

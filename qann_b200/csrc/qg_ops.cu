@@ -214,15 +214,21 @@ namespace {
 struct Prepared {
     DevBuf<float> q;     // prepared queries (normalised for cosine)
     DevBuf<uint64_t> filter;
-    DevBuf<int> err;
+    DevBuf<int> err_own;
+    int* err = nullptr;  // [0] scan overflow, [1] zero cosine row, [2] tensor-core pipeline timeout
 };
 } // namespace
 
 static void prepare(IndexObj& idx, const SearchRequest& r, Prepared& p, cudaStream_t st) {
     const size_t dim = idx.dim();
     const size_t n = r.nq * dim;
-    p.err.alloc(2, st);
-    QG_CUDA(cudaMemsetAsync(p.err.get(), 0, 2 * sizeof(int), st));
+    if (r.err_dev) {
+        p.err = r.err_dev;
+    } else {
+        p.err_own.alloc(3, st);
+        p.err = p.err_own.get();
+    }
+    QG_CUDA(cudaMemsetAsync(p.err, 0, 3 * sizeof(int), st));
     DevBuf<float> raw;
     const float* src = r.q;
     if (r.io == IoSpace::Host) {
@@ -232,7 +238,7 @@ static void prepare(IndexObj& idx, const SearchRequest& r, Prepared& p, cudaStre
     }
     p.q.alloc(n, st);
     if (idx.metric() == Metric::Cosine) {
-        normalize_rows(src, p.q.get(), static_cast<int>(r.nq), static_cast<int>(dim), p.err.get() + 1, st);
+        normalize_rows(src, p.q.get(), static_cast<int>(r.nq), static_cast<int>(dim), p.err + 1, st);
     } else {
         QG_CUDA(cudaMemcpyAsync(p.q.get(), src, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
     }
@@ -268,12 +274,13 @@ static void fill_empty(const SearchRequest& r, cudaStream_t st) {
     }
 }
 
-static void check_err(const DevBuf<int>& err, cudaStream_t st) {
-    int h[2] = {0, 0};
-    QG_CUDA(cudaMemcpyAsync(h, err.get(), sizeof(h), cudaMemcpyDeviceToHost, st));
+static void check_err(const int* err, cudaStream_t st) {
+    int h[3] = {0, 0, 0};
+    QG_CUDA(cudaMemcpyAsync(h, err, sizeof(h), cudaMemcpyDeviceToHost, st));
     QG_CUDA(cudaStreamSynchronize(st));
     if (h[1]) throw Error(kInvalidArgument, "cosine metric needs non-zero vectors");
     if (h[0]) throw Error(kRuntimeError, "fast-scan candidate buffer overflowed (internal error)");
+    if (h[2]) throw Error(kRuntimeError, "tensor-core coarse step: a pipeline wait timed out");
 }
 
 // Filtered probing of an IVF index (reference src/ivf_index.cpp:501-521): at
@@ -342,7 +349,7 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
             QG_CUDA(cudaMemcpyAsync(r.out_ids, out_ids, r.nq * r.k * 8, cudaMemcpyDeviceToHost, st));
             QG_CUDA(cudaMemcpyAsync(r.out_d, out_d, r.nq * r.k * 4, cudaMemcpyDeviceToHost, st));
         }
-        check_err(p.err, st);
+        if (!r.capture) check_err(p.err, st);   // a captured search's caller reads the flags after each replay
     };
 
     if (idx.kind == Kind::IVF) {
@@ -366,8 +373,9 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
         a.kp = kp;
         a.nprobe = r.nprobe > 0 ? r.nprobe : static_cast<int>(o.model.nprobe);
         filter_probing(a, o.model, r.filter, p.filter.get(), r.k);
+        a.capture = r.capture;
         a.sm_count = sm_count_cached();
-        a.d_err = p.err.get();
+        a.d_err = p.err;
         ivf_candidates(o.dev.view, a, ck.get(), cs.get(), st);
         finalize_ivf(ck.get(), cs.get(), a.nq, kp, a.k, o.dev.labels.get(), cosine, out_ids, out_d, st);
         finish(p);
@@ -426,8 +434,9 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
         a.kp = static_cast<int>(kp);
         a.nprobe = r.nprobe > 0 ? r.nprobe : static_cast<int>(b.model.nprobe);
         filter_probing(a, b.model, r.filter, p.filter.get(), kp);
+        a.capture = r.capture;
         a.sm_count = sm_count_cached();
-        a.d_err = p.err.get();
+        a.d_err = p.err;
         ivf_candidates(b.dev.view, a, ck.get(), cs.get(), st);
     } else {
         auto& b = static_cast<FlatObj&>(*o.base);
@@ -437,6 +446,103 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
     refine_candidates(p.q.get(), static_cast<int>(r.nq), dim, o.dev.rows.get(), ck.get(), cs.get(), static_cast<int>(kp),
                       static_cast<int>(r.k), ip, o.dev.labels.get(), cosine, out_ids, out_d, st);
     finish(p);
+}
+
+// ---------------------------------------------------------------------------
+// Device-resident searches replayed as CUDA graphs
+// ---------------------------------------------------------------------------
+namespace {
+std::atomic<int> g_graphs{0};
+std::atomic<int64_t> g_graph_replays{0}, g_graph_captures{0};
+}
+
+void set_search_graphs(int on) { g_graphs.store(on); }
+int search_graphs() { return g_graphs.load(); }
+void search_graph_counts(int64_t* replays, int64_t* captures) {
+    *replays = g_graph_replays.load();
+    *captures = g_graph_captures.load();
+}
+
+bool search_graph(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
+    if (!g_graphs.load() || r.io != IoSpace::Device || r.filter || st == nullptr || r.nq == 0 || r.k == 0) return false;
+    const bool refine = idx.kind == Kind::Refine;
+    IndexObj* base = refine ? static_cast<RefineObj&>(idx).base.get() : &idx;
+    if (base->kind != Kind::IVF) return false;
+    auto& ivf = static_cast<IVFObj&>(*base);
+    if (refine) ensure_device(static_cast<RefineObj&>(idx), st);
+    else ensure_device(ivf, st);
+    if (ivf.model.idmap.live_count() == 0 || (refine && static_cast<RefineObj&>(idx).map.live_count() == 0)) return false;
+    const int nprobe = r.nprobe > 0 ? r.nprobe : static_cast<int>(ivf.model.nprobe);
+    const size_t kf = refine ? static_cast<RefineObj&>(idx).k_factor : 0;
+    const uint64_t gen = idx.dev_gen * 1000003u + (refine ? ivf.dev_gen : 0);
+    std::lock_guard<std::mutex> g(idx.graph_mu);
+    SearchGraph* e = nullptr;
+    for (auto it = idx.graphs.begin(); it != idx.graphs.end();) {
+        SearchGraph& x = **it;
+        if (x.nq == r.nq && x.k == r.k && x.nprobe == nprobe && x.k_factor == kf && x.q == r.q && x.ids == r.out_ids &&
+            x.d == r.out_d && x.st == st) {
+            if (x.gen != gen) {   // the index was rebuilt since the capture
+                it = idx.graphs.erase(it);
+                continue;
+            }
+            e = &x;
+        }
+        ++it;
+    }
+    if (e) {
+        if (e->failed) return false;
+        QG_CUDA(cudaGraphLaunch(e->exec, st));
+        profiler().launches.fetch_add(e->launches, std::memory_order_relaxed);
+        g_graph_replays += 1;
+        int h[3] = {0, 0, 0};
+        QG_CUDA(cudaMemcpyAsync(h, e->err, sizeof(h), cudaMemcpyDeviceToHost, st));
+        QG_CUDA(cudaStreamSynchronize(st));
+        if (h[1]) throw Error(kInvalidArgument, "cosine metric needs non-zero vectors");
+        if (h[0]) throw Error(kRuntimeError, "fast-scan candidate buffer overflowed (internal error)");
+        if (h[2]) throw Error(kRuntimeError, "tensor-core coarse step: a pipeline wait timed out");
+        return true;
+    }
+    // first call with this key: the search itself (results, tuning, one-time setup), then its capture
+    search(idx, r, st);
+    auto ent = std::make_unique<SearchGraph>();
+    ent->nq = r.nq;
+    ent->k = r.k;
+    ent->k_factor = kf;
+    ent->nprobe = nprobe;
+    ent->q = r.q;
+    ent->ids = r.out_ids;
+    ent->d = r.out_d;
+    ent->st = st;
+    ent->gen = gen;
+    QG_CUDA(cudaMalloc(reinterpret_cast<void**>(&ent->err), 3 * sizeof(int)));
+    SearchRequest rc = r;
+    rc.capture = true;
+    rc.err_dev = ent->err;
+    const int64_t launches0 = profiler().launches.load();
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        try {
+            search(idx, rc, st);
+        } catch (...) {
+            ok = false;
+        }
+        ok = cudaStreamEndCapture(st, &graph) == cudaSuccess && ok && graph != nullptr;
+    }
+    if (ok) ok = cudaGraphInstantiate(&ent->exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    // captured launches did not run: they count once per replay instead
+    const int64_t captured = profiler().launches.load() - launches0;
+    profiler().launches.fetch_sub(captured, std::memory_order_relaxed);
+    if (!ok) {
+        (void)cudaGetLastError();   // a capture that failed leaves no sticky error; this key runs uncaptured
+        ent->failed = true;
+    } else {
+        ent->launches = captured;
+        g_graph_captures += 1;
+    }
+    idx.graphs.push_back(std::move(ent));
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -561,7 +667,7 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
     a.pq.wanted = dh.get() + kWanted * nb;
     a.any_filter = any_filter;
     a.sm_count = sm_count_cached();
-    a.d_err = p.err.get();
+    a.d_err = p.err;
     DevBuf<uint64_t> ck(nb * kpmax, st);
     DevBuf<uint32_t> cs(nb * kpmax, st);
     ivf_candidates(ivf->dev.view, a, ck.get(), cs.get(), st);

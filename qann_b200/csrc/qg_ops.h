@@ -22,10 +22,23 @@ struct SearchRequest {
     float* out_d = nullptr;
     IoSpace io = IoSpace::Host;
     int nprobe = 0;                  // > 0: probes instead of the IVF index's nprobe
+    bool capture = false;            // being captured into a CUDA graph: no host reads or waits
+    int* err_dev = nullptr;          // caller-owned error flags (3 ints), read by the caller, or null
 };
 
 // Runs a batch query on `st` and, for host I/O, waits for it.
 void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st);
+
+// A device-resident, unfiltered search of an IVF index (or a RefineIndex over
+// one) replayed as a CUDA graph: the first call with a given batch size, k,
+// nprobe, k_factor, buffers and stream runs the search and captures it; later
+// calls launch the graph. Returns false when the request does not qualify
+// (the caller runs search()). Off unless set_search_graphs(1).
+bool search_graph(IndexObj& idx, const SearchRequest& r, cudaStream_t st);
+void set_search_graphs(int on);
+int search_graphs();
+// Graph replays and captures so far.
+void search_graph_counts(int64_t* replays, int64_t* captures);
 
 // One query of a mixed batch: a served request with its own settings.
 struct MixedQuery {

@@ -717,10 +717,11 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
             pair_scores(qs, n, v.centroids, v.nlist, v.dim, v.ip_metric, scores.get(), v.nlist, st);
             select_rows(scores.get(), v.nlist, n, v.nlist, P, pr, pd, st, nullptr, nullptr, 0, true);
         };
-        if (use_tensor_coarse(nq, v.nlist, v.dim) && coarse_mm_supported(v.nlist, v.dim, P, v.cent_f16 != nullptr)) {
+        if (use_tensor_coarse(nq, v.nlist, v.dim) &&
+            coarse_mm_supported(v.nlist, v.dim, P, v.cent_f16 != nullptr, s.capture)) {
             std::vector<int> redo;
-            coarse_probes_mm(v, s.q, nq, P, probe.get(), pdist.get(), redo, st);
-            count_tensor_coarse(nq, static_cast<int64_t>(redo.size()));
+            coarse_probes_mm(v, s.q, nq, P, probe.get(), pdist.get(), redo, st, s.capture ? s.d_err + 2 : nullptr);
+            if (!s.capture) count_tensor_coarse(nq, static_cast<int64_t>(redo.size()));
             if (!redo.empty()) {
                 // queries with too many near-ties: the exact path, results copied into place
                 const size_t m = redo.size();
@@ -815,7 +816,7 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
         }
     }
     const bool big = static_cast<long long>(nq) * P >= 4 * 148 * 256;
-    if (!tuned && cands.size() > 1 && big) {
+    if (!tuned && cands.size() > 1 && big && !s.capture) {
         shape = tune_scan(cands, a, v, qtab_len, st);
         std::lock_guard<std::mutex> g(g_tune_mu);
         g_tuned[key] = shape;

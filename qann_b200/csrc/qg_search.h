@@ -85,7 +85,8 @@ struct IvfSearchArgs {
     PerQuery pq;                // mixed batches; nprobe above is then the largest nprobe
     bool any_filter = false;    // some query of a mixed batch has a filter
     int sm_count = 0;
-    int* d_err = nullptr;
+    int* d_err = nullptr;       // [0] scan overflow, [2] tensor-core pipeline timeout
+    bool capture = false;       // being captured into a CUDA graph: no host reads, waits or tuning
 };
 
 void normalize_rows(const float* x, float* y, int n, int d, int* d_zero, cudaStream_t st);
@@ -118,7 +119,7 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
 // error bound and an exact recheck; queries with too many near-ties are
 // listed in redo_q for the exact path. use_tensor_coarse: whether the batch
 // goes this way (the process-wide tensor-filter mode and the work's size).
-bool coarse_mm_supported(int nlist, int dim, int P, bool cent_prepared);
+bool coarse_mm_supported(int nlist, int dim, int P, bool cent_prepared, bool capture = false);
 bool use_tensor_coarse(size_t nq, int nlist, int dim);
 // Queries whose coarse step went through the tensor cores, and those of them redone exactly.
 void count_tensor_coarse(int64_t queries, int64_t redone);
@@ -126,8 +127,11 @@ void tensor_coarse_counts(int64_t* queries, int64_t* redone);
 // Lists rescored exactly by the tensor-core coarse step so far (its candidates).
 void count_tensor_coarse_candidates(int64_t n);
 int64_t tensor_coarse_candidates();
+// Under capture (capture_err non-null) nothing is read back: every list fits
+// the recheck, queries with extreme norms rescore every list, and a pipeline
+// timeout is flagged in *capture_err.
 void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t* probe, float* pdist,
-                      std::vector<int>& redo_q, cudaStream_t st);
+                      std::vector<int>& redo_q, cudaStream_t st, int* capture_err = nullptr);
 // Rows scaled by powers of two (2^exps) and rounded to f16 (zero-padded to
 // dpad, a multiple of 8), with their float squared norms (unscaled).
 void prepare_f16_rows(const float* rows, size_t n, int dim, DevBuf<uint16_t>& f16, DevBuf<float>& sq,

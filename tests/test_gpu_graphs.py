@@ -74,3 +74,26 @@ def test_recaptured_after_add(graphs):
     np.testing.assert_array_equal(gi, ei)
     assert gd.tobytes() == ed.tobytes()
     assert after["captures"] - before["captures"] == 1
+
+
+@pytest.mark.parametrize("name", ["l2", "cos_l2"])
+def test_replays_with_tensor_coarse(golden, graphs, name):
+    """The coarse step on the tensor cores inside a captured search (its
+    recheck then holds every list) matches the direct exact path."""
+    qb.set_tensor_filter(2)
+    try:
+        idx = qb.load(golden / "gen" / f"refine_{name}.qann")
+        q = np.load(golden / "gen" / "queries.npy")
+        n, k = 32, 10
+        stream = torch.cuda.Stream()
+        q_dev = torch.from_numpy(np.ascontiguousarray(q[:n])).cuda()
+        ids = torch.empty((n, k), dtype=torch.int64, device="cuda")
+        d = torch.empty((n, k), dtype=torch.float32, device="cuda")
+        for _ in range(3):
+            gi, gd = run_device(idx, q_dev, ids, d, stream)
+        qb.set_tensor_filter(0)
+        ei, ed = idx.batch_query(q[:n], k)
+        np.testing.assert_array_equal(gi, ei)
+        assert gd.tobytes() == ed.tobytes()
+    finally:
+        qb.set_tensor_filter(1)

@@ -626,25 +626,30 @@ int scan_tuned_shapes() {
     return static_cast<int>(g_tuned.size());
 }
 
-// Candidate shapes whose shared memory fits: unstaged ones for two blocks per
-// SM, staged ones for one.
+// Candidate shapes whose shared memory fits: up to three unstaged ones for two
+// blocks per SM (or one, when none fits that), and a staged one.
 static std::vector<ScanShape> scan_shapes(int kp, int m_pad, int qtab_len, int pch, bool shared_lut) {
     static constexpr int kUnstaged[][2] = {{8, 32}, {8, 16}, {4, 32}, {4, 16}, {8, 8}, {4, 8}, {2, 8}, {2, 4}, {1, 4}, {1, 1}};
     static constexpr int kStagedShapes[][2] = {{8, 16}, {8, 8}, {4, 32}, {4, 16}, {4, 8}};
     std::vector<ScanShape> out;
     const int force = g_force.load();
-    auto first_fit = [&](const auto& table, bool staged, size_t limit) {
+    auto fits = [&](const auto& table, bool staged, size_t limit, size_t most) {
+        size_t added = 0;
         for (const auto& sh : table) {
+            if (added == most) break;
             const int lc = shared_lut ? 64 : sh[1];
-            if (scan_layout(kp, m_pad, qtab_len, pch, shared_lut, sh[0], lc, staged).bytes <= limit) {
+            const bool dup = std::any_of(out.begin(), out.end(), [&](const ScanShape& o) {
+                return o.nw == sh[0] && o.lc == lc && o.staged == staged;
+            });
+            if (!dup && scan_layout(kp, m_pad, qtab_len, pch, shared_lut, sh[0], lc, staged).bytes <= limit) {
                 out.push_back({sh[0], lc, staged});
-                return true;
+                ++added;
             }
         }
-        return false;
+        return added > 0;
     };
-    if (force != 1 && !first_fit(kUnstaged, false, 110 * 1024)) first_fit(kUnstaged, false, 226 * 1024);
-    if (force != 0) first_fit(kStagedShapes, true, 226 * 1024);
+    if (force != 1 && !fits(kUnstaged, false, 110 * 1024, 3)) fits(kUnstaged, false, 226 * 1024, 1);
+    if (force != 0) fits(kStagedShapes, true, 226 * 1024, 1);
     return out;
 }
 

@@ -672,9 +672,10 @@ void refine_candidates(const float* q, int nq, int dim, const float* rows, const
                        cudaStream_t st, const int* kp_q, const int* k_q) {
     if (nq == 0 || k == 0) return;
     const int kpow = std::max(2, next_pow2(kp));
-    // candidate rows staged per tile: up to 128 rows within ~96 KB
+    // candidate rows staged per tile: up to 64 rows within ~48 KB, so that
+    // several blocks share an SM and their gathers overlap
     const size_t row_bytes = static_cast<size_t>(dim | 1) * 4;
-    const int tile = static_cast<int>(std::clamp<size_t>((96 * 1024) / row_bytes, 1, 128));
+    const int tile = static_cast<int>(std::clamp<size_t>((48 * 1024) / row_bytes, 1, 64));
     const size_t rsm = static_cast<size_t>(kpow) * 16 + static_cast<size_t>(dim) * 4 + tile * row_bytes;
     require(rsm <= 200 * 1024, "re-rank shared memory exceeds the B200 limit for this k * k_factor and dim",
             kUnsupported);

@@ -98,12 +98,36 @@ int qg_search_bitmap(qg_index* h, const float* q, size_t nq, size_t k, const uin
 int qg_search_device(qg_index* h, const float* q_dev, size_t nq, size_t k, int64_t* out_ids_dev, float* out_dists_dev,
                      void* stream);
 
+/* --- sharded search (no counterpart in the reference, which searches one
+ * in-process index) -------------------------------------------------------------------
+ * Spreads an IVF index's lists over several devices or processes. qg_set(h,
+ * "shards", n) and qg_set(h, "shard", s) on an IVF handle make its device copy
+ * hold only the lists l with l % n == s. The sizes of all lists stay known, so
+ * every shard numbers the probed vectors alike and candidate keys compare
+ * across shards. Each shard computes its candidates:
+ *   qg_candidate_count(h, k, &kp);      k' per query (k, or min(k * k_factor, size))
+ *   qg_search_candidates_device(h, q_dev, nq, k, key_dev, slot_dev, stream);   nq x kp sorted
+ * The shards exchange candidates (an all-gather into [nq][nparts][kp]). Each
+ * then merges and finishes, with the same results as one unsharded search:
+ *   qg_merge_candidates_device(keys, slots, nq, nparts, kp, key_out, slot_out, stream);
+ *   qg_finish_candidates_device(h, q_dev, nq, k, key_out, slot_out, ids_dev, dists_dev, stream);
+ * h may be the IVF handle or a RefineIndex over it (whose raw rows every shard keeps).
+ * Unfiltered queries. A sharded handle refuses qg_search and the server. */
+int qg_candidate_count(qg_index* h, size_t k, size_t* kp);
+int qg_search_candidates_device(qg_index* h, const float* q_dev, size_t nq, size_t k, uint64_t* key_dev,
+                                uint32_t* slot_dev, void* stream);
+int qg_merge_candidates_device(const uint64_t* key_dev, const uint32_t* slot_dev, size_t nq, size_t nparts, size_t kp,
+                               uint64_t* out_key_dev, uint32_t* out_slot_dev, void* stream);
+int qg_finish_candidates_device(qg_index* h, const float* q_dev, size_t nq, size_t k, const uint64_t* key_dev,
+                                const uint32_t* slot_dev, int64_t* out_ids_dev, float* out_dists_dev, void* stream);
+
 /* --- properties ------------------------------------------------------------------
  * keys: "nprobe", "k_factor", "precomputed_tables", "cosine_inner_product",
  * "filter_probe_scaling" (settable; reference ivf_index.hpp:83-118,
  * refine_index.hpp:91-93) and the read-only "dim", "kind", "metric", "nlist",
  * "size", "slots", "custom_ids", "fast_scan", "pq_m", "pq_k", "trained",
- * "rotate", "sq_bits", "wrapped".
+ * "rotate", "sq_bits", "wrapped". Also settable, with no reference
+ * counterpart: "shard" / "shards", the sharded search's list partition.
  */
 int qg_get(qg_index* h, const char* key, int64_t* value);
 int qg_set(qg_index* h, const char* key, int64_t value);

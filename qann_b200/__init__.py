@@ -116,6 +116,14 @@ def set_scan_options(autotune: bool | None = None, variant: int | None = None) -
         check(_lib.lib.qg_set_option(b"scan_variant", int(variant)))
 
 
+def merge_candidates_device(key_ptr: int, slot_ptr: int, nq: int, nparts: int, kp: int, out_key_ptr: int,
+                            out_slot_ptr: int, stream: int = 0) -> None:
+    """The k' smallest keys per query over nparts sorted candidate lists laid
+    out [nq][nparts][kp] (uint64 keys, uint32 slots), sorted."""
+    check(_lib.lib.qg_merge_candidates_device(key_ptr, slot_ptr, nq, nparts, kp, out_key_ptr, out_slot_ptr,
+                                              stream or None))
+
+
 def set_search_graphs(on: bool) -> None:
     """search_device replays fixed-shape, unfiltered IVF searches as CUDA
     graphs (captured on the first call with each batch size, k, nprobe and
@@ -258,6 +266,25 @@ class DenseIndex:
         distances (nq, k) float32 out, on ``stream``."""
         check(_lib.lib.qg_search_device(self._h, q_ptr, nq, k, out_ids_ptr, out_d_ptr, stream or None))
 
+    # -- sharded search (the lists of an IVF index spread over devices) --------------
+    def candidate_count(self, k: int) -> int:
+        """k' candidates per query that search_candidates_device returns."""
+        v = C.c_size_t()
+        check(_lib.lib.qg_candidate_count(self._h, int(k), C.byref(v)))
+        return v.value
+
+    def search_candidates_device(self, q_ptr: int, nq: int, k: int, key_ptr: int, slot_ptr: int,
+                                 stream: int = 0) -> None:
+        """The k' best candidates of each query from this handle's shard of
+        the lists: (nq, k') uint64 keys and uint32 slots, sorted."""
+        check(_lib.lib.qg_search_candidates_device(self._h, q_ptr, nq, k, key_ptr, slot_ptr, stream or None))
+
+    def finish_candidates_device(self, q_ptr: int, nq: int, k: int, key_ptr: int, slot_ptr: int, out_ids_ptr: int,
+                                 out_d_ptr: int, stream: int = 0) -> None:
+        """Results from merged candidates (re-ranked for a RefineIndex)."""
+        check(_lib.lib.qg_finish_candidates_device(self._h, q_ptr, nq, k, key_ptr, slot_ptr, out_ids_ptr, out_d_ptr,
+                                                   stream or None))
+
     def save(self, path) -> None:
         check(_lib.lib.qg_save(self._h, os.fspath(path).encode()))
 
@@ -323,6 +350,12 @@ class IVFIndex(DenseIndex):
     pq_rotate = property(lambda self: bool(self._get("rotate")))
     sq_bits = property(lambda self: self._get("sq_bits"))
     mapped = property(lambda self: False)
+
+    def set_shard(self, shard: int, shards: int) -> None:
+        """Keep on the device only the lists l with l % shards == shard, for
+        the sharded search (qann_b200.sharded); shards=1 holds every list."""
+        self._set("shards", shards)
+        self._set("shard", shard)
 
 
 class RefineIndex(DenseIndex):

@@ -36,6 +36,10 @@ _SIGS = {
     "qg_search": (C.c_int, [_vp, _vp, _sz, _sz, _vp, _sz, _vp, _vp]),
     "qg_search_bitmap": (C.c_int, [_vp, _vp, _sz, _sz, _vp, _sz, _vp, _vp]),
     "qg_search_device": (C.c_int, [_vp, _vp, _sz, _sz, _vp, _vp, _vp]),
+    "qg_candidate_count": (C.c_int, [_vp, _sz, C.POINTER(_sz)]),
+    "qg_search_candidates_device": (C.c_int, [_vp, _vp, _sz, _sz, _vp, _vp, _vp]),
+    "qg_merge_candidates_device": (C.c_int, [_vp, _vp, _sz, _sz, _sz, _vp, _vp, _vp]),
+    "qg_finish_candidates_device": (C.c_int, [_vp, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _vp]),
     "qg_get": (C.c_int, [_vp, C.c_char_p, C.POINTER(_i64)]),
     "qg_set": (C.c_int, [_vp, C.c_char_p, _i64]),
     "qg_ivf_list_sizes": (C.c_int, [_vp, _vp]),

@@ -4,6 +4,7 @@
 
 #include "qg_device.cuh"
 #include "qg_ops.h"
+#include "qg_search.h"
 #include "qg_train.h"
 
 #include <limits>
@@ -291,6 +292,51 @@ int qg_search_device(qg_index* h, const float* q_dev, size_t nq, size_t k, int64
     });
 }
 
+int qg_candidate_count(qg_index* h, size_t k, size_t* kp) {
+    return guarded([&] {
+        require(kp != nullptr, "null argument");
+        IndexObj& o = obj(h);
+        std::shared_lock<std::shared_mutex> lk(o.mu);
+        *kp = candidate_count(o, k);
+    });
+}
+
+int qg_search_candidates_device(qg_index* h, const float* q_dev, size_t nq, size_t k, uint64_t* key_dev,
+                                uint32_t* slot_dev, void* stream) {
+    return guarded([&] {
+        keep_pool_memory();
+        IndexObj& o = obj(h);
+        std::shared_lock<std::shared_mutex> lk(o.mu);
+        std::shared_lock<std::shared_mutex> lb;
+        if (o.kind == Kind::Refine) lb = std::shared_lock<std::shared_mutex>(static_cast<RefineObj&>(o).base->mu);
+        search_candidates(o, q_dev, nq, k, key_dev, slot_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int qg_merge_candidates_device(const uint64_t* key_dev, const uint32_t* slot_dev, size_t nq, size_t nparts, size_t kp,
+                               uint64_t* out_key_dev, uint32_t* out_slot_dev, void* stream) {
+    return guarded([&] {
+        require(nparts >= 1 && kp >= 1 && kp <= 3072, "nparts must be >= 1 and kp in [1, 3072]");
+        keep_pool_memory();
+        merge_candidates(key_dev, slot_dev, static_cast<int>(nq), static_cast<int>(nparts), static_cast<int>(kp),
+                         out_key_dev, out_slot_dev, static_cast<cudaStream_t>(stream));
+        QG_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    });
+}
+
+int qg_finish_candidates_device(qg_index* h, const float* q_dev, size_t nq, size_t k, const uint64_t* key_dev,
+                                const uint32_t* slot_dev, int64_t* out_ids_dev, float* out_dists_dev, void* stream) {
+    return guarded([&] {
+        keep_pool_memory();
+        IndexObj& o = obj(h);
+        std::shared_lock<std::shared_mutex> lk(o.mu);
+        std::shared_lock<std::shared_mutex> lb;
+        if (o.kind == Kind::Refine) lb = std::shared_lock<std::shared_mutex>(static_cast<RefineObj&>(o).base->mu);
+        finish_candidates(o, q_dev, nq, k, key_dev, slot_dev, out_ids_dev, out_dists_dev,
+                          static_cast<cudaStream_t>(stream));
+    });
+}
+
 int qg_get(qg_index* h, const char* key, int64_t* value) {
     return guarded([&] {
         IndexObj& o = obj(h);
@@ -318,6 +364,8 @@ int qg_get(qg_index* h, const char* key, int64_t* value) {
             else if (k == "precomputed_tables") *value = v.precomputed_available();
             else if (k == "cosine_inner_product") *value = M.cosine_ip;
             else if (k == "filter_probe_scaling") *value = M.filter_probe_scaling;
+            else if (k == "shard") *value = v.shard;
+            else if (k == "shards") *value = v.shards;
             else if (k == "fast_scan") *value = M.fast_scan;
             else if (k == "pq_m") *value = static_cast<int64_t>(M.has_pq ? M.pq.m : 0);
             else if (k == "pq_k") *value = static_cast<int64_t>(M.has_pq ? M.pq.K : 0);
@@ -355,6 +403,15 @@ int qg_set(qg_index* h, const char* key, int64_t value) {
             v.dev_dirty = true;
         } else if (k == "filter_probe_scaling") {
             M.filter_probe_scaling = value != 0;
+        } else if (k == "shards") {
+            require(value >= 1 && value <= 4096, "shards must be in [1, 4096]");
+            v.shards = static_cast<int>(value);
+            if (v.shard >= v.shards) v.shard = 0;
+            v.dev_dirty = true;
+        } else if (k == "shard") {
+            require(value >= 0 && value < v.shards, "shard must be in [0, shards)");
+            v.shard = static_cast<int>(value);
+            v.dev_dirty = true;
         } else if (k == "pq_distance") {
             if (M.fast_scan && value == 1) throw Error(kInvalidArgument, "cannot use SDC with fast-scan");
             if (M.metric == Metric::InnerProduct && value == 1)

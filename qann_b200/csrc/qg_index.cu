@@ -164,19 +164,21 @@ void ensure_device(IVFObj& o, cudaStream_t) {
                                                                                  static_cast<int>(M.pq.sub_dim), D.B.get());
         QG_LAUNCH_CHECK();
     }
-    // lists -> superblocks
+    // lists -> superblocks (a shard keeps only its own lists' codes; the sizes stay global)
     std::vector<uint32_t> sizes(nlist), voff(nlist + 1, 0), sb_off(nlist + 1, 0);
+    auto own = [&](int l) { return l % o.shards == o.shard; };
     for (int l = 0; l < nlist; ++l) {
         sizes[l] = static_cast<uint32_t>(M.list_ids[l].size());
-        voff[l + 1] = voff[l] + sizes[l];
-        sb_off[l + 1] = sb_off[l] + static_cast<uint32_t>(ceil_div(sizes[l], kSuperBlock));
+        const uint32_t held = own(l) ? sizes[l] : 0;
+        voff[l + 1] = voff[l] + held;
+        sb_off[l + 1] = sb_off[l] + static_cast<uint32_t>(ceil_div(held, kSuperBlock));
     }
     const size_t n = voff[nlist], total_sb = sb_off[nlist];
     std::vector<uint8_t> codes(n * m);
     std::vector<uint32_t> ids(n);
     std::vector<uint32_t> sb_list(total_sb);
     for (int l = 0; l < nlist; ++l) {
-        if (sizes[l]) {
+        if (sizes[l] && own(l)) {
             std::memcpy(codes.data() + static_cast<size_t>(voff[l]) * m, M.list_codes[l].data(), static_cast<size_t>(sizes[l]) * m);
             std::memcpy(ids.data() + voff[l], M.list_ids[l].data(), sizes[l] * sizeof(uint32_t));
         }

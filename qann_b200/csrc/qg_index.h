@@ -75,6 +75,10 @@ struct IndexObj {
 struct IVFObj : IndexObj {
     IVFModel model;
     DeviceIVF dev;
+    // List sharding: the device copy holds the lists l with l % shards == shard
+    // (codes and slots); list sizes stay global, so push indices (and so
+    // candidate keys) agree across shards. Not saved.
+    int shard = 0, shards = 1;
     IVFObj() : IndexObj(Kind::IVF) {}
     size_t dim() const override { return model.dim; }
     Metric metric() const override { return model.metric; }

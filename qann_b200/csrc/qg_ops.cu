@@ -326,8 +326,17 @@ static void refine_direct(RefineObj& o, const Prepared& p, const SearchRequest& 
                  o.dev.labels.get(), cosine, out_ids, out_d, st);
 }
 
+// A list-sharded IVF device copy holds only some lists: it answers through
+// search_candidates / merge / finish_candidates alone.
+static void require_unsharded(const IndexObj& idx) {
+    const IndexObj* b = idx.kind == Kind::Refine ? static_cast<const RefineObj&>(idx).base.get() : &idx;
+    require(b->kind != Kind::IVF || static_cast<const IVFObj&>(*b).shards == 1,
+            "this index holds one shard of its lists: search it through the sharded search", kLogicError);
+}
+
 void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
     if (r.nq == 0) return;
+    require_unsharded(idx);
     const bool empty_filter = r.filter && r.filter->count == 0;
     if (r.k == 0) return;
     const int dim = static_cast<int>(idx.dim());
@@ -449,6 +458,77 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
+// Sharded search: candidates from this device's lists, merge, finish
+// ---------------------------------------------------------------------------
+static IVFObj& ivf_of(IndexObj& idx) {
+    IndexObj* b = idx.kind == Kind::Refine ? static_cast<RefineObj&>(idx).base.get() : &idx;
+    require(b->kind == Kind::IVF, "the sharded search serves IVF indexes and RefineIndexes over them", kUnsupported);
+    return static_cast<IVFObj&>(*b);
+}
+
+size_t candidate_count(IndexObj& idx, size_t k) {
+    IVFObj& ivf = ivf_of(idx);
+    if (idx.kind != Kind::Refine) return k;
+    auto& o = static_cast<RefineObj&>(idx);
+    (void)ivf;
+    return std::min(k * o.k_factor, o.map.live_count());
+}
+
+void search_candidates(IndexObj& idx, const float* q_dev, size_t nq, size_t k, uint64_t* key, uint32_t* slot,
+                       cudaStream_t st) {
+    if (nq == 0 || k == 0) return;
+    IVFObj& b = ivf_of(idx);
+    const size_t kp = candidate_count(idx, k);
+    require(kp >= 1 && kp <= 3072, "k * k_factor must be in [1, 3072] for the GPU fast-scan", kUnsupported);
+    if (idx.kind == Kind::Refine) ensure_device(static_cast<RefineObj&>(idx), st);
+    else ensure_device(b, st);
+    SearchRequest r;
+    r.q = q_dev;
+    r.nq = nq;
+    r.k = k;
+    r.io = IoSpace::Device;
+    Prepared p;
+    prepare(idx, r, p, st);
+    DevBuf<float> qrot;
+    IvfSearchArgs a;
+    a.q = ivf_queries(b, p, nq, qrot, st);
+    a.nq = static_cast<int>(nq);
+    a.k = static_cast<int>(k);
+    a.kp = static_cast<int>(kp);
+    a.nprobe = static_cast<int>(b.model.nprobe);
+    a.sm_count = sm_count_cached();
+    a.d_err = p.err;
+    ivf_candidates(b.dev.view, a, key, slot, st);
+    check_err(p.err, st);
+}
+
+void finish_candidates(IndexObj& idx, const float* q_dev, size_t nq, size_t k, const uint64_t* key, const uint32_t* slot,
+                       int64_t* out_ids, float* out_d, cudaStream_t st) {
+    if (nq == 0 || k == 0) return;
+    IVFObj& b = ivf_of(idx);
+    const size_t kp = candidate_count(idx, k);
+    const bool cosine = idx.metric() == Metric::Cosine, ip = idx.metric() == Metric::InnerProduct;
+    if (idx.kind == Kind::Refine) ensure_device(static_cast<RefineObj&>(idx), st);
+    else ensure_device(b, st);
+    SearchRequest r;
+    r.q = q_dev;
+    r.nq = nq;
+    r.k = k;
+    r.io = IoSpace::Device;
+    Prepared p;
+    prepare(idx, r, p, st);
+    if (idx.kind == Kind::Refine) {
+        auto& o = static_cast<RefineObj&>(idx);
+        refine_candidates(p.q.get(), static_cast<int>(nq), static_cast<int>(idx.dim()), o.dev.rows.get(), key, slot,
+                          static_cast<int>(kp), static_cast<int>(k), ip, o.dev.labels.get(), cosine, out_ids, out_d, st);
+    } else {
+        finalize_ivf(key, slot, static_cast<int>(nq), static_cast<int>(kp), static_cast<int>(k), b.dev.labels.get(),
+                     cosine, out_ids, out_d, st);
+    }
+    check_err(p.err, st);
+}
+
+// ---------------------------------------------------------------------------
 // Device-resident searches replayed as CUDA graphs
 // ---------------------------------------------------------------------------
 namespace {
@@ -550,6 +630,7 @@ bool search_graph(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs, size_t kmax, int64_t* out_ids,
                   float* out_d, cudaStream_t st) {
+    require_unsharded(idx);
     std::fill(out_ids, out_ids + nq * kmax, int64_t{-1});
     std::fill(out_d, out_d + nq * kmax, std::numeric_limits<float>::infinity());
     if (nq == 0 || kmax == 0) return;

@@ -29,6 +29,17 @@ struct SearchRequest {
 // Runs a batch query on `st` and, for host I/O, waits for it.
 void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st);
 
+// Sharded search of an IVF index (or a RefineIndex over one) whose device
+// copy holds one shard of the lists: the k' candidates per query from this
+// device's lists (sorted (key64, slot) lists, keys comparable across shards),
+// and the results from the merged candidates of every shard. Device buffers;
+// unfiltered queries.
+size_t candidate_count(IndexObj& idx, size_t k);
+void search_candidates(IndexObj& idx, const float* q_dev, size_t nq, size_t k, uint64_t* key, uint32_t* slot,
+                       cudaStream_t st);
+void finish_candidates(IndexObj& idx, const float* q_dev, size_t nq, size_t k, const uint64_t* key, const uint32_t* slot,
+                       int64_t* out_ids, float* out_d, cudaStream_t st);
+
 // A device-resident, unfiltered search of an IVF index (or a RefineIndex over
 // one) replayed as a CUDA graph: the first call with a given batch size, k,
 // nprobe, k_factor, buffers and stream runs the search and captures it; later

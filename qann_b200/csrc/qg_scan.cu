@@ -330,7 +330,8 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
             for (int base = 0; base < np; base += 32) {
                 const int p = base + lane;
                 const uint32_t sz = p < np ? p_size[p] : 0;
-                const uint32_t nsb = (sz + kSuperBlock - 1) / kSuperBlock;
+                // superblocks held on this device (none for another shard's list)
+                const uint32_t nsb = p < np ? v.sb_off[p_list[p] + 1] - p_sboff[p] : 0;
                 uint32_t ip = sz, is = nsb;
                 for (int o = 1; o < 32; o <<= 1) {
                     const uint32_t t1 = __shfl_up_sync(kFull, ip, o), t2 = __shfl_up_sync(kFull, is, o);

@@ -74,6 +74,20 @@ size_t filter_smem_bytes(int kblocks) {
 
 } // namespace
 
+// Tile schedule: each CTA takes a contiguous range of tile indices, walked in
+// groups of kGroupN base tiles; within a group the query tile changes every
+// kGroupN tiles. A base tile thus comes from HBM once and from L2 for every
+// later query tile, and the single-buffered query tile reloads only once
+// per group.
+constexpr int kGroupN = 8;
+__device__ __forceinline__ void tile_coords(int t, int mtiles, int ntiles, int& mt, int& nt) {
+    const int group = t / (mtiles * kGroupN);
+    const int rem = t - group * mtiles * kGroupN;
+    const int gsize = min(kGroupN, ntiles - group * kGroupN);
+    mt = rem / gsize;
+    nt = group * kGroupN + (rem - mt * gsize);
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     k_mm_filter(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, MmArgs a) {
     using namespace sm100;
@@ -116,6 +130,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     const int total = a.mtiles * a.ntiles;
+    const int per = (total + gridDim.x - 1) / gridDim.x;   // this CTA's tiles: [t_begin, t_end)
+    const int t_begin = min(total, blockIdx.x * per), t_end = min(total, t_begin + per);
     auto fail = [&] {
         *abort = 1;
         atomicExch(a.err, 2);
@@ -124,8 +140,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 0) {
         if (lane == 0) {
             int it = 0, aloads = 0, cur_m = -1;
-            for (int t = blockIdx.x; t < total && !*abort; t += gridDim.x) {
-                const int mt = t / a.ntiles, nt = t - mt * a.ntiles;
+            for (int t = t_begin; t < t_end && !*abort; ++t) {
+                int mt, nt;
+                tile_coords(t, a.mtiles, a.ntiles, mt, nt);
                 if (mt != cur_m) {
                     if (aloads > 0 && !mbar_wait(empty_a, (aloads - 1) & 1, abort)) {
                         fail();
@@ -159,8 +176,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) {
             const uint32_t idesc = a.f16 ? idesc_f16_f32(BM, BN) : idesc_bf16_f32(BM, BN);
             int it = 0, aloads = 0, cur_m = -1, ti = 0;
-            for (int t = blockIdx.x; t < total && !*abort; t += gridDim.x) {
-                const int mt = t / a.ntiles;
+            for (int t = t_begin; t < t_end && !*abort; ++t) {
+                int mt, nt;
+                tile_coords(t, a.mtiles, a.ntiles, mt, nt);
+                (void)nt;
                 if (mt != cur_m) {
                     if (cur_m >= 0) mma_commit(empty_a);   // the old query tile is free once its MMAs finish
                     if (!mbar_wait(full_a, aloads & 1, abort)) {
@@ -203,8 +222,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int col0 = (ew >> 2) * (BN / 2);
         const int row_in_tile = quad * 32 + lane;
         int ti = 0;
-        for (int t = blockIdx.x; t < total; t += gridDim.x) {
-            const int mt = t / a.ntiles, nt = t - mt * a.ntiles;
+        for (int t = t_begin; t < t_end; ++t) {
+            int mt, nt;
+            tile_coords(t, a.mtiles, a.ntiles, mt, nt);
             const int acc = ti & 1;
             const bool ok = __all_sync(0xffffffffu, mbar_wait(&tfull[acc], (ti >> 1) & 1, abort));
             if (!ok) {

@@ -680,97 +680,113 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
     if (batch.empty()) return;
     if (ref) ensure_device(*ref, st);
     ensure_device(*ivf, st);
-    const size_t nb = batch.size();
-    std::vector<float> qh(nb * dim);
-    for (size_t j = 0; j < nb; ++j) std::copy_n(q + batch[j] * dim, dim, qh.data() + j * dim);
-    SearchRequest pr;
-    pr.q = qh.data();
-    pr.nq = nb;
-    Prepared p;
-    prepare(idx, pr, p, st);
-
-    // per-query settings, and each distinct filter uploaded once
-    enum { kK, kKp, kNprobe, kMin, kWanted, kFields };
-    std::vector<int> h(kFields * nb);
-    std::vector<const SlotBits*> distinct;
-    std::vector<size_t> which(nb, SIZE_MAX);
-    int npmax = 1, kpmax = 1;
-    bool any_filter = false;
-    for (size_t j = 0; j < nb; ++j) {
-        const MixedQuery& m = qs[batch[j]];
-        const size_t np = std::min<size_t>(m.nprobe > 0 ? static_cast<size_t>(m.nprobe) : M.nprobe, M.nlist);
+    auto kp_of = [&](size_t i) {
+        const MixedQuery& m = qs[i];
         const size_t lv = m.filter ? m.filter->count : live;
-        const size_t kp = ref ? std::min(static_cast<size_t>(m.k) * ref->k_factor, lv) : static_cast<size_t>(m.k);
-        h[kK * nb + j] = m.k;
-        h[kKp * nb + j] = static_cast<int>(kp);
-        h[kNprobe * nb + j] = static_cast<int>(np);
-        if (m.filter) {
-            any_filter = true;
-            h[kMin * nb + j] = static_cast<int>(min_probes_for(M, np, m.filter->count));
-            h[kWanted * nb + j] = static_cast<int>(std::min(kp, m.filter->count));
-            auto it = std::find(distinct.begin(), distinct.end(), m.filter);
-            which[j] = static_cast<size_t>(it - distinct.begin());
-            if (it == distinct.end()) distinct.push_back(m.filter);
+        return ref ? std::min(static_cast<size_t>(m.k) * ref->k_factor, lv) : static_cast<size_t>(m.k);
+    };
+    // One batched search per class of k' (up to 256, above): a few requests
+    // with a large k' would otherwise size every query's candidate lists and
+    // scan trims by theirs.
+    auto run = [&](const std::vector<size_t>& batch) {
+        const size_t nb = batch.size();
+        size_t kmax_g = 1;
+        for (size_t i : batch) kmax_g = std::max(kmax_g, static_cast<size_t>(qs[i].k));
+        std::vector<float> qh(nb * dim);
+        for (size_t j = 0; j < nb; ++j) std::copy_n(q + batch[j] * dim, dim, qh.data() + j * dim);
+        SearchRequest pr;
+        pr.q = qh.data();
+        pr.nq = nb;
+        Prepared p;
+        prepare(idx, pr, p, st);
+
+        // per-query settings, and each distinct filter uploaded once
+        enum { kK, kKp, kNprobe, kMin, kWanted, kFields };
+        std::vector<int> h(kFields * nb);
+        std::vector<const SlotBits*> distinct;
+        std::vector<size_t> which(nb, SIZE_MAX);
+        int npmax = 1, kpmax = 1;
+        bool any_filter = false;
+        for (size_t j = 0; j < nb; ++j) {
+            const MixedQuery& m = qs[batch[j]];
+            const size_t np = std::min<size_t>(m.nprobe > 0 ? static_cast<size_t>(m.nprobe) : M.nprobe, M.nlist);
+            const size_t lv = m.filter ? m.filter->count : live;
+            const size_t kp = ref ? std::min(static_cast<size_t>(m.k) * ref->k_factor, lv) : static_cast<size_t>(m.k);
+            h[kK * nb + j] = m.k;
+            h[kKp * nb + j] = static_cast<int>(kp);
+            h[kNprobe * nb + j] = static_cast<int>(np);
+            if (m.filter) {
+                any_filter = true;
+                h[kMin * nb + j] = static_cast<int>(min_probes_for(M, np, m.filter->count));
+                h[kWanted * nb + j] = static_cast<int>(std::min(kp, m.filter->count));
+                auto it = std::find(distinct.begin(), distinct.end(), m.filter);
+                which[j] = static_cast<size_t>(it - distinct.begin());
+                if (it == distinct.end()) distinct.push_back(m.filter);
+            }
+            npmax = std::max(npmax, static_cast<int>(np));
+            kpmax = std::max(kpmax, static_cast<int>(kp));
         }
-        npmax = std::max(npmax, static_cast<int>(np));
-        kpmax = std::max(kpmax, static_cast<int>(kp));
-    }
-    require(kpmax <= 3072, "k * k_factor above 3072 is not supported by the GPU path", kUnsupported);
-    DevBuf<int> dh(h.size(), st);
-    QG_CUDA(cudaMemcpyAsync(dh.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-    DevBuf<uint64_t> fwords;
-    DevBuf<const uint64_t*> fptr;
-    if (any_filter) {
-        const size_t words = distinct.front()->words.size();
-        for (const SlotBits* f : distinct) require(f->words.size() == words, "filters of one batch differ in size");
-        fwords.alloc(words * distinct.size(), st);
-        for (size_t d = 0; d < distinct.size(); ++d)
-            QG_CUDA(cudaMemcpyAsync(fwords.get() + d * words, distinct[d]->words.data(), words * 8,
-                                    cudaMemcpyHostToDevice, st));
-        std::vector<const uint64_t*> ptr(nb, nullptr);
-        for (size_t j = 0; j < nb; ++j)
-            if (which[j] != SIZE_MAX) ptr[j] = fwords.get() + which[j] * words;
-        fptr.alloc(nb, st);
-        QG_CUDA(cudaMemcpyAsync(fptr.get(), ptr.data(), nb * sizeof(void*), cudaMemcpyHostToDevice, st));
-    }
-    DevBuf<float> qrot;
-    IvfSearchArgs a;
-    a.q = ivf_queries(*ivf, p, nb, qrot, st);
-    a.nq = static_cast<int>(nb);
-    a.k = static_cast<int>(kmax);
-    a.kp = kpmax;
-    a.nprobe = npmax;
-    a.pq.k = dh.get() + kK * nb;
-    a.pq.kp = dh.get() + kKp * nb;
-    a.pq.nprobe = dh.get() + kNprobe * nb;
-    a.pq.filter = any_filter ? fptr.get() : nullptr;
-    a.pq.min_probes = dh.get() + kMin * nb;
-    a.pq.wanted = dh.get() + kWanted * nb;
-    a.any_filter = any_filter;
-    a.sm_count = sm_count_cached();
-    a.d_err = p.err;
-    DevBuf<uint64_t> ck(nb * kpmax, st);
-    DevBuf<uint32_t> cs(nb * kpmax, st);
-    ivf_candidates(ivf->dev.view, a, ck.get(), cs.get(), st);
-    DevBuf<int64_t> oid(nb * kmax, st);
-    DevBuf<float> od(nb * kmax, st);
-    const bool cosine = idx.metric() == Metric::Cosine, ip = idx.metric() == Metric::InnerProduct;
-    if (ref)
-        refine_candidates(p.q.get(), static_cast<int>(nb), static_cast<int>(dim), ref->dev.rows.get(), ck.get(), cs.get(),
-                          kpmax, static_cast<int>(kmax), ip, ref->dev.labels.get(), cosine, oid.get(), od.get(), st,
-                          a.pq.kp, a.pq.k);
-    else
-        finalize_ivf(ck.get(), cs.get(), static_cast<int>(nb), kpmax, static_cast<int>(kmax), ivf->dev.labels.get(), cosine,
-                     oid.get(), od.get(), st, a.pq.k);
-    std::vector<int64_t> hid(nb * kmax);
-    std::vector<float> hd(nb * kmax);
-    QG_CUDA(cudaMemcpyAsync(hid.data(), oid.get(), hid.size() * 8, cudaMemcpyDeviceToHost, st));
-    QG_CUDA(cudaMemcpyAsync(hd.data(), od.get(), hd.size() * 4, cudaMemcpyDeviceToHost, st));
-    check_err(p.err, st);
-    for (size_t j = 0; j < nb; ++j) {
-        std::copy_n(hid.data() + j * kmax, kmax, out_ids + batch[j] * kmax);
-        std::copy_n(hd.data() + j * kmax, kmax, out_d + batch[j] * kmax);
-    }
+        require(kpmax <= 3072, "k * k_factor above 3072 is not supported by the GPU path", kUnsupported);
+        DevBuf<int> dh(h.size(), st);
+        QG_CUDA(cudaMemcpyAsync(dh.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        DevBuf<uint64_t> fwords;
+        DevBuf<const uint64_t*> fptr;
+        if (any_filter) {
+            const size_t words = distinct.front()->words.size();
+            for (const SlotBits* f : distinct) require(f->words.size() == words, "filters of one batch differ in size");
+            fwords.alloc(words * distinct.size(), st);
+            for (size_t d = 0; d < distinct.size(); ++d)
+                QG_CUDA(cudaMemcpyAsync(fwords.get() + d * words, distinct[d]->words.data(), words * 8,
+                                        cudaMemcpyHostToDevice, st));
+            std::vector<const uint64_t*> ptr(nb, nullptr);
+            for (size_t j = 0; j < nb; ++j)
+                if (which[j] != SIZE_MAX) ptr[j] = fwords.get() + which[j] * words;
+            fptr.alloc(nb, st);
+            QG_CUDA(cudaMemcpyAsync(fptr.get(), ptr.data(), nb * sizeof(void*), cudaMemcpyHostToDevice, st));
+        }
+        DevBuf<float> qrot;
+        IvfSearchArgs a;
+        a.q = ivf_queries(*ivf, p, nb, qrot, st);
+        a.nq = static_cast<int>(nb);
+        a.k = static_cast<int>(kmax_g);
+        a.kp = kpmax;
+        a.nprobe = npmax;
+        a.pq.k = dh.get() + kK * nb;
+        a.pq.kp = dh.get() + kKp * nb;
+        a.pq.nprobe = dh.get() + kNprobe * nb;
+        a.pq.filter = any_filter ? fptr.get() : nullptr;
+        a.pq.min_probes = dh.get() + kMin * nb;
+        a.pq.wanted = dh.get() + kWanted * nb;
+        a.any_filter = any_filter;
+        a.sm_count = sm_count_cached();
+        a.d_err = p.err;
+        DevBuf<uint64_t> ck(nb * kpmax, st);
+        DevBuf<uint32_t> cs(nb * kpmax, st);
+        ivf_candidates(ivf->dev.view, a, ck.get(), cs.get(), st);
+        DevBuf<int64_t> oid(nb * kmax_g, st);
+        DevBuf<float> od(nb * kmax_g, st);
+        const bool cosine = idx.metric() == Metric::Cosine, ip = idx.metric() == Metric::InnerProduct;
+        if (ref)
+            refine_candidates(p.q.get(), static_cast<int>(nb), static_cast<int>(dim), ref->dev.rows.get(), ck.get(), cs.get(),
+                              kpmax, static_cast<int>(kmax_g), ip, ref->dev.labels.get(), cosine, oid.get(), od.get(), st,
+                              a.pq.kp, a.pq.k);
+        else
+            finalize_ivf(ck.get(), cs.get(), static_cast<int>(nb), kpmax, static_cast<int>(kmax_g), ivf->dev.labels.get(), cosine,
+                         oid.get(), od.get(), st, a.pq.k);
+        std::vector<int64_t> hid(nb * kmax_g);
+        std::vector<float> hd(nb * kmax_g);
+        QG_CUDA(cudaMemcpyAsync(hid.data(), oid.get(), hid.size() * 8, cudaMemcpyDeviceToHost, st));
+        QG_CUDA(cudaMemcpyAsync(hd.data(), od.get(), hd.size() * 4, cudaMemcpyDeviceToHost, st));
+        check_err(p.err, st);
+        for (size_t j = 0; j < nb; ++j) {
+            std::copy_n(hid.data() + j * kmax_g, kmax_g, out_ids + batch[j] * kmax);
+            std::copy_n(hd.data() + j * kmax_g, kmax_g, out_d + batch[j] * kmax);
+        }
+    };
+    std::vector<size_t> small, large;
+    for (size_t i : batch) (kp_of(i) <= 256 ? small : large).push_back(i);
+    if (!small.empty()) run(small);
+    if (!large.empty()) run(large);
 }
 
 } // namespace qg

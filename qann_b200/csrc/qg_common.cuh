@@ -62,6 +62,11 @@ __host__ __device__ __forceinline__ uint32_t float_key_eq0(float f) {
 //
 // chain(j, L): the FMA chain of accumulator j, lane L.
 // ---------------------------------------------------------------------------
+// Packed FP32 (sm_100): each component of __fadd2_rn / __ffma2_rn rounds as
+// the scalar __fadd_rn / __fmaf_rn does, and x - y is x + (-y) exactly, so
+// pairs of independent chains advance two per instruction with the same bits.
+__device__ __forceinline__ float2 sub2(float2 x, float2 y) { return __fadd2_rn(x, make_float2(-y.x, -y.y)); }
+
 template <bool kL2>
 __device__ __forceinline__ float exact_tail(const float* __restrict__ a, const float* __restrict__ b, int i, int n,
                                             float r) {
@@ -101,25 +106,25 @@ __device__ __forceinline__ float exact_avx2(const float* __restrict__ a, const f
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int lane = L + 4 * h;
-            float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
+            // accumulators 0/1 and 2/3 advance as packed pairs
+            float2 acc01 = make_float2(0.f, 0.f), acc23 = make_float2(0.f, 0.f);
             int i = 0;
             for (; i < n32; i += 32) {
+                const float2 x01 = make_float2(a[i + lane], a[i + 8 + lane]);
+                const float2 x23 = make_float2(a[i + 16 + lane], a[i + 24 + lane]);
+                const float2 y01 = make_float2(b[i + lane], b[i + 8 + lane]);
+                const float2 y23 = make_float2(b[i + 16 + lane], b[i + 24 + lane]);
                 if (kL2) {
-                    const float d0 = __fsub_rn(a[i + lane], b[i + lane]);
-                    const float d1 = __fsub_rn(a[i + 8 + lane], b[i + 8 + lane]);
-                    const float d2 = __fsub_rn(a[i + 16 + lane], b[i + 16 + lane]);
-                    const float d3 = __fsub_rn(a[i + 24 + lane], b[i + 24 + lane]);
-                    acc0 = __fmaf_rn(d0, d0, acc0);
-                    acc1 = __fmaf_rn(d1, d1, acc1);
-                    acc2 = __fmaf_rn(d2, d2, acc2);
-                    acc3 = __fmaf_rn(d3, d3, acc3);
+                    const float2 d01 = sub2(x01, y01), d23 = sub2(x23, y23);
+                    acc01 = __ffma2_rn(d01, d01, acc01);
+                    acc23 = __ffma2_rn(d23, d23, acc23);
                 } else {
-                    acc0 = __fmaf_rn(a[i + lane], b[i + lane], acc0);
-                    acc1 = __fmaf_rn(a[i + 8 + lane], b[i + 8 + lane], acc1);
-                    acc2 = __fmaf_rn(a[i + 16 + lane], b[i + 16 + lane], acc2);
-                    acc3 = __fmaf_rn(a[i + 24 + lane], b[i + 24 + lane], acc3);
+                    acc01 = __ffma2_rn(x01, y01, acc01);
+                    acc23 = __ffma2_rn(x23, y23, acc23);
                 }
             }
+            float acc0 = acc01.x;
+            const float acc1 = acc01.y, acc2 = acc23.x, acc3 = acc23.y;
             for (; i < n8; i += 8) {
                 if (kL2) {
                     const float d = __fsub_rn(a[i + lane], b[i + lane]);
@@ -149,17 +154,22 @@ __device__ __forceinline__ float exact_avx2_vec(const float* __restrict__ a, con
     for (int e = 0; e < 32; ++e) acc[e] = 0.0f;
     const float4* a4 = reinterpret_cast<const float4*>(a);
     const float4* b4 = reinterpret_cast<const float4*>(b);
-    auto step4 = [&](const float4& av, const float4& bv, int base) {
-        const float x[4] = {av.x, av.y, av.z, av.w}, y[4] = {bv.x, bv.y, bv.z, bv.w};
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            if (kL2) {
-                const float d = __fsub_rn(x[u], y[u]);
-                acc[base + u] = __fmaf_rn(d, d, acc[base + u]);
-            } else {
-                acc[base + u] = __fmaf_rn(x[u], y[u], acc[base + u]);
-            }
+    auto step4 = [&](const float4& av, const float4& bv, int base) {   // two chains per packed instruction
+        const float2 x01 = make_float2(av.x, av.y), x23 = make_float2(av.z, av.w);
+        const float2 y01 = make_float2(bv.x, bv.y), y23 = make_float2(bv.z, bv.w);
+        float2 c01 = make_float2(acc[base], acc[base + 1]), c23 = make_float2(acc[base + 2], acc[base + 3]);
+        if (kL2) {
+            const float2 d01 = sub2(x01, y01), d23 = sub2(x23, y23);
+            c01 = __ffma2_rn(d01, d01, c01);
+            c23 = __ffma2_rn(d23, d23, c23);
+        } else {
+            c01 = __ffma2_rn(x01, y01, c01);
+            c23 = __ffma2_rn(x23, y23, c23);
         }
+        acc[base] = c01.x;
+        acc[base + 1] = c01.y;
+        acc[base + 2] = c23.x;
+        acc[base + 3] = c23.y;
     };
     for (int i = 0; i < n32; i += 32) {
         float4 av[8], bv[8];

@@ -359,9 +359,13 @@ __device__ __forceinline__ int sum_limit(uint32_t thr_key, float scale, float of
 __device__ __forceinline__ int sum_limit_fast(uint32_t thr_key, float scale, float offset) {
     if (thr_key == 0xFFFFFFFFu) return 65535;
     const float x = __fmul_rn(__fsub_rn(key_float(thr_key), offset), scale);
-    if (!(x > -4.0f && x < 65540.0f)) return sum_limit(thr_key, scale, offset);
-    int s = max(-1, min(65535, __float2int_rd(x)));
     auto pass = [&](int t) { return float_key(fs_dist(static_cast<uint32_t>(t), scale, offset)) <= thr_key; };
+    // far outside the sum range: distances are monotone in the sum, so one
+    // end decides it (a list whose smallest distance is above the threshold
+    // is the common case once the threshold has tightened)
+    if (!(x > -4.0f)) return pass(0) ? sum_limit(thr_key, scale, offset) : -1;
+    if (!(x < 65540.0f)) return pass(65535) ? 65535 : sum_limit(thr_key, scale, offset);
+    int s = max(-1, min(65535, __float2int_rd(x)));
     for (int it = 0; it < 4; ++it) {
         if (s >= 0 && !pass(s)) {
             --s;

@@ -51,11 +51,18 @@ constexpr int kQtabStride = 20;
 // The 16 entries of LUT rows rounded and packed: round-half-even of
 // (t - min) * scale, as nearbyint / cvtps do, through the 1.5 * 2^23 addend
 // (every value here lies in [0, 64), where float spacing at that magnitude is 1).
+// Two entries per packed FP32 instruction: each component rounds as the scalar
+// __fadd_rn / __fmul_rn does, and t - min is t + (-min) exactly.
 __device__ __forceinline__ uint4 round_row(const float* v, float mn, float scale) {
+    const float2 neg = make_float2(-mn, -mn), sc = make_float2(scale, scale);
+    const float2 magic = make_float2(12582912.0f, 12582912.0f);
     uint32_t b[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j)
-        b[j] = __float_as_uint(__fadd_rn(__fmul_rn(__fsub_rn(v[j], mn), scale), 12582912.0f));
+    for (int j = 0; j < 16; j += 2) {
+        const float2 t = __fadd2_rn(__fmul2_rn(__fadd2_rn(make_float2(v[j], v[j + 1]), neg), sc), magic);
+        b[j] = __float_as_uint(t.x);
+        b[j + 1] = __float_as_uint(t.y);
+    }
     return make_uint4(prmt(prmt(b[0], b[1], 0x0040), prmt(b[2], b[3], 0x0040), 0x5410),
                       prmt(prmt(b[4], b[5], 0x0040), prmt(b[6], b[7], 0x0040), 0x5410),
                       prmt(prmt(b[8], b[9], 0x0040), prmt(b[10], b[11], 0x0040), 0x5410),
@@ -65,9 +72,14 @@ __device__ __forceinline__ uint4 round_row(const float* v, float mn, float scale
 // LUT of one list by one warp. Same arithmetic as quantize_lut; each lane
 // forms its rows twice (for their ranges, then for rounding) rather than
 // holding them in registers across the warp-wide reductions.
+// thr_hi: the block's current threshold key (0xFFFFFFFF: none yet). When even
+// a zero sum's distance is above it, no vector of the list can become a
+// candidate (distances grow with the sum and the threshold only falls), so
+// the LUT entries are left unwritten: the scan never reads them, because its
+// sum limit for such a list is -1.
 template <class RowFn>
 __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* row_min, uint4* lut_out, float& scale_out,
-                                          float& offset_out) {
+                                          float& offset_out, uint32_t thr_hi) {
     const int lane = threadIdx.x & 31;
     float widest = 0.0f;
     auto ranges = [&](int r, const float* v) {
@@ -95,11 +107,13 @@ __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* ro
     const float p2 = __shfl_sync(0xffffffffu, part, 2), p3 = __shfl_sync(0xffffffffu, part, 3);
     const float offset = __fadd_rn(__fadd_rn(p0, p1), __fadd_rn(p2, p3));
     const float scale = widest > 0.0f ? __fdiv_rn(static_cast<float>(kLutMax), widest) : 1.0f;
-    for (int r = lane; r < m; r += 32) {
-        row(r, v0);
-        lut_out[r] = round_row(v0, row_min[r], scale);
+    if (thr_hi == 0xFFFFFFFFu || float_key(fs_dist(0u, scale, offset)) <= thr_hi) {   // (warp-uniform)
+        for (int r = lane; r < m; r += 32) {
+            row(r, v0);
+            lut_out[r] = round_row(v0, row_min[r], scale);
+        }
+        for (int r = m + lane; r < m_pad; r += 32) lut_out[r] = make_uint4(0, 0, 0, 0);
     }
-    for (int r = m + lane; r < m_pad; r += 32) lut_out[r] = make_uint4(0, 0, 0, 0);
     scale_out = scale;
     offset_out = offset;
     __syncwarp();
@@ -108,26 +122,34 @@ __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* ro
 // Mode L2: the LUT of B[list] + C[query] (+ A on row 0), as build_quantize_lut
 // sums them (reference src/fast_scan.cpp:243-254).
 __device__ __noinline__ void warp_lut_l2(const float* __restrict__ B, const float* qtab, float A, int m, int m_pad,
-                                         float* row_min, uint4* lut_out, float* scale_out, float* offset_out) {
+                                         float* row_min, uint4* lut_out, float* scale_out, float* offset_out,
+                                         uint32_t thr_hi) {
     float sc, of;
     warp_lut3(
         [&](int rr, float* o) {
             const float4* b4 = reinterpret_cast<const float4*>(B + rr * 16);
             const float4* c4 = reinterpret_cast<const float4*>(qtab + rr * kQtabStride);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < 4; ++u) {   // packed FP32 adds, rounding per component as __fadd_rn
                 const float4 bb = __ldg(b4 + u), cc = c4[u];
-                o[4 * u + 0] = __fadd_rn(bb.x, cc.x);
-                o[4 * u + 1] = __fadd_rn(bb.y, cc.y);
-                o[4 * u + 2] = __fadd_rn(bb.z, cc.z);
-                o[4 * u + 3] = __fadd_rn(bb.w, cc.w);
+                const float2 lo = __fadd2_rn(make_float2(bb.x, bb.y), make_float2(cc.x, cc.y));
+                const float2 hi = __fadd2_rn(make_float2(bb.z, bb.w), make_float2(cc.z, cc.w));
+                o[4 * u + 0] = lo.x;
+                o[4 * u + 1] = lo.y;
+                o[4 * u + 2] = hi.x;
+                o[4 * u + 3] = hi.y;
             }
             if (rr == 0) {
+                const float2 a2 = make_float2(A, A);
 #pragma unroll
-                for (int jj = 0; jj < 16; ++jj) o[jj] = __fadd_rn(o[jj], A);
+                for (int jj = 0; jj < 16; jj += 2) {
+                    const float2 t = __fadd2_rn(make_float2(o[jj], o[jj + 1]), a2);
+                    o[jj] = t.x;
+                    o[jj + 1] = t.y;
+                }
             }
         },
-        m, m_pad, row_min, lut_out, sc, of);
+        m, m_pad, row_min, lut_out, sc, of, thr_hi);
     *scale_out = sc;
     *offset_out = of;
 }
@@ -137,7 +159,7 @@ __device__ __noinline__ void warp_lut_l2(const float* __restrict__ B, const floa
 // (reference src/ivf_index.cpp:594-610).
 __device__ __noinline__ void warp_lut_adc(const float* __restrict__ ctr, const float* q, const float* __restrict__ pq_t,
                                           int sd, int m, int m_pad, float* row_min, uint4* lut_out, float* scale_out,
-                                          float* offset_out) {
+                                          float* offset_out, uint32_t thr_hi) {
     float sc, of;
     warp_lut3(
         [&](int rr, float* o) {
@@ -152,7 +174,7 @@ __device__ __noinline__ void warp_lut_adc(const float* __restrict__ ctr, const f
                 o[jj] = acc;
             }
         },
-        m, m_pad, row_min, lut_out, sc, of);
+        m, m_pad, row_min, lut_out, sc, of, thr_hi);
     *scale_out = sc;
     *offset_out = of;
 }
@@ -375,12 +397,15 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
                 const uint32_t lj = p_list[p];
                 uint4* out = lut_ring + static_cast<size_t>(h * LC + j) * LS;
                 float sc, of;
+                uint32_t thr_now = 0;   // the same in every lane
+                if (lane == 0) thr_now = static_cast<uint32_t>(*reinterpret_cast<volatile unsigned long long*>(&s_thr) >> 32);
+                thr_now = __shfl_sync(kFull, thr_now, 0);
                 if (v.mode == kModeL2)
                     warp_lut_l2(v.B + static_cast<size_t>(lj) * v.m * 16, qtab, a.pterm[qp + p0 + p], v.m, v.m_pad,
-                                wrmin, out, &sc, &of);
+                                wrmin, out, &sc, &of, thr_now);
                 else
                     warp_lut_adc(v.resid + static_cast<size_t>(lj) * v.dim, qtab, v.pq_t, v.sd, v.m, v.m_pad, wrmin,
-                                 out, &sc, &of);
+                                 out, &sc, &of, thr_now);
                 if (lane == 0) {
                     g_scale[h * LC + j] = sc;
                     g_offset[h * LC + j] = of;
@@ -448,12 +473,16 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
                     }
                     sbl = i - sb_first;
                     sbg = static_cast<size_t>(list_sb) + sbl;
-                    if constexpr (kStaged)
+                    if (smax < 0) {   // no vector of the list can pass (its LUT may be unbuilt)
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) sums[e] = 0;
+                    } else if constexpr (kStaged) {
                         octet_sums_shared(reinterpret_cast<const uint4*>(
                                               cstage + static_cast<size_t>(stage * kSbPerWarp + oct) * sb_bytes),
                                           L, v.m_pad, r, sums);
-                    else
+                    } else {
                         octet_sums(v.codes + sbg * static_cast<size_t>(2 * v.m_pad), L, v.m_pad, r, sums);
+                    }
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
                         const uint32_t pos = sbl * kSuperBlock + 8 * r + e;

@@ -78,7 +78,7 @@ __device__ __forceinline__ uint4 round_row(const float* v, float mn, float scale
 // the LUT entries are left unwritten: the scan never reads them, because its
 // sum limit for such a list is -1.
 template <class RowFn>
-__device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* row_min, uint4* lut_out, float& scale_out,
+__device__ __forceinline__ bool warp_lut3(RowFn row, int m, int m_pad, float* row_min, uint4* lut_out, float& scale_out,
                                           float& offset_out, uint32_t thr_hi) {
     const int lane = threadIdx.x & 31;
     float widest = 0.0f;
@@ -107,7 +107,8 @@ __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* ro
     const float p2 = __shfl_sync(0xffffffffu, part, 2), p3 = __shfl_sync(0xffffffffu, part, 3);
     const float offset = __fadd_rn(__fadd_rn(p0, p1), __fadd_rn(p2, p3));
     const float scale = widest > 0.0f ? __fdiv_rn(static_cast<float>(kLutMax), widest) : 1.0f;
-    if (thr_hi == 0xFFFFFFFFu || float_key(fs_dist(0u, scale, offset)) <= thr_hi) {   // (warp-uniform)
+    const bool live = thr_hi == 0xFFFFFFFFu || float_key(fs_dist(0u, scale, offset)) <= thr_hi;   // (warp-uniform)
+    if (live) {
         for (int r = lane; r < m; r += 32) {
             row(r, v0);
             lut_out[r] = round_row(v0, row_min[r], scale);
@@ -117,15 +118,16 @@ __device__ __forceinline__ void warp_lut3(RowFn row, int m, int m_pad, float* ro
     scale_out = scale;
     offset_out = offset;
     __syncwarp();
+    return live;
 }
 
 // Mode L2: the LUT of B[list] + C[query] (+ A on row 0), as build_quantize_lut
 // sums them (reference src/fast_scan.cpp:243-254).
-__device__ __noinline__ void warp_lut_l2(const float* __restrict__ B, const float* qtab, float A, int m, int m_pad,
+__device__ __noinline__ bool warp_lut_l2(const float* __restrict__ B, const float* qtab, float A, int m, int m_pad,
                                          float* row_min, uint4* lut_out, float* scale_out, float* offset_out,
                                          uint32_t thr_hi) {
     float sc, of;
-    warp_lut3(
+    const bool live = warp_lut3(
         [&](int rr, float* o) {
             const float4* b4 = reinterpret_cast<const float4*>(B + rr * 16);
             const float4* c4 = reinterpret_cast<const float4*>(qtab + rr * kQtabStride);
@@ -152,16 +154,17 @@ __device__ __noinline__ void warp_lut_l2(const float* __restrict__ B, const floa
         m, m_pad, row_min, lut_out, sc, of, thr_hi);
     *scale_out = sc;
     *offset_out = of;
+    return live;
 }
 
 // Mode L2-ADC: the LUT of the residual's ADC table; the residual (q - center)
 // is formed per element inside the table loop, as compute_adc_table reads it
 // (reference src/ivf_index.cpp:594-610).
-__device__ __noinline__ void warp_lut_adc(const float* __restrict__ ctr, const float* q, const float* __restrict__ pq_t,
+__device__ __noinline__ bool warp_lut_adc(const float* __restrict__ ctr, const float* q, const float* __restrict__ pq_t,
                                           int sd, int m, int m_pad, float* row_min, uint4* lut_out, float* scale_out,
                                           float* offset_out, uint32_t thr_hi) {
     float sc, of;
-    warp_lut3(
+    const bool live = warp_lut3(
         [&](int rr, float* o) {
 #pragma unroll
             for (int jj = 0; jj < 16; ++jj) {
@@ -177,6 +180,7 @@ __device__ __noinline__ void warp_lut_adc(const float* __restrict__ ctr, const f
         m, m_pad, row_min, lut_out, sc, of, thr_hi);
     *scale_out = sc;
     *offset_out = of;
+    return live;
 }
 
 // octet_sums over a superblock staged in shared memory.
@@ -374,7 +378,9 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
 
         // LUTs (or scale / offset) of group g into half g & 1. Warps take the
         // lists from a counter, so warps that finish scanning group g - 1 early
-        // build more of them.
+        // build more of them. A list none of whose vectors can beat the block
+        // threshold (even a zero sum's distance is above it) gets scale -1 (real
+        // scales are >= 0) and no LUT; the group's scan skips its superblocks.
         auto build_group = [&](int g) {
             const int h = g & 1, gp0 = g * LC, nc = min(LC, np - gp0);
             if (tid == 0) {
@@ -387,27 +393,30 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
                 j = __shfl_sync(kFull, j, 0);
                 if (j >= nc) break;
                 const int p = gp0 + j;
+                uint32_t thr_now = 0;   // the same in every lane
+                if (lane == 0) thr_now = static_cast<uint32_t>(*reinterpret_cast<volatile unsigned long long*>(&s_thr) >> 32);
+                thr_now = __shfl_sync(kFull, thr_now, 0);
                 if (shared_lut) {
                     if (lane == 0) {
-                        g_scale[h * LC + j] = a.qscale[qi];
-                        g_offset[h * LC + j] = __fadd_rn(a.qoffset[qi], a.pterm[qp + p0 + p]);
+                        const float sc = a.qscale[qi], of = __fadd_rn(a.qoffset[qi], a.pterm[qp + p0 + p]);
+                        const bool live = thr_now == 0xFFFFFFFFu || float_key(fs_dist(0u, sc, of)) <= thr_now;
+                        g_scale[h * LC + j] = live ? sc : -1.0f;
+                        g_offset[h * LC + j] = of;
                     }
                     continue;
                 }
                 const uint32_t lj = p_list[p];
                 uint4* out = lut_ring + static_cast<size_t>(h * LC + j) * LS;
                 float sc, of;
-                uint32_t thr_now = 0;   // the same in every lane
-                if (lane == 0) thr_now = static_cast<uint32_t>(*reinterpret_cast<volatile unsigned long long*>(&s_thr) >> 32);
-                thr_now = __shfl_sync(kFull, thr_now, 0);
+                bool live;
                 if (v.mode == kModeL2)
-                    warp_lut_l2(v.B + static_cast<size_t>(lj) * v.m * 16, qtab, a.pterm[qp + p0 + p], v.m, v.m_pad,
-                                wrmin, out, &sc, &of, thr_now);
+                    live = warp_lut_l2(v.B + static_cast<size_t>(lj) * v.m * 16, qtab, a.pterm[qp + p0 + p], v.m,
+                                       v.m_pad, wrmin, out, &sc, &of, thr_now);
                 else
-                    warp_lut_adc(v.resid + static_cast<size_t>(lj) * v.dim, qtab, v.pq_t, v.sd, v.m, v.m_pad, wrmin,
-                                 out, &sc, &of, thr_now);
+                    live = warp_lut_adc(v.resid + static_cast<size_t>(lj) * v.dim, qtab, v.pq_t, v.sd, v.m, v.m_pad,
+                                        wrmin, out, &sc, &of, thr_now);
                 if (lane == 0) {
-                    g_scale[h * LC + j] = sc;
+                    g_scale[h * LC + j] = live ? sc : -1.0f;
                     g_offset[h * LC + j] = of;
                 }
             }
@@ -419,28 +428,64 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
         for (int g = 0; g < ngroups; ++g) {
             __syncthreads();   // group g's LUTs and the unit's prefix arrays are complete
             const int h = g & 1, gp0 = g * LC, nc = min(LC, np - gp0);
-            const uint32_t sbb = p_sbpre[gp0], sbe = p_sbpre[gp0 + nc];
+            // The group's superblocks without those of skipped lists, numbered
+            // 0..total-1 list after list: list lane (and lane + 32 when LC = 64)
+            // starts at st0 (st1); empty and skipped lists hold ~0u, which no
+            // index reaches. Every warp forms these in its own registers.
+            uint32_t st0 = 0, st1 = 0, total = 0;
+            {
+                uint32_t n0 = 0, n1 = 0;
+                if (lane < nc && !(g_scale[h * LC + lane] < 0.0f))
+                    n0 = p_sbpre[gp0 + lane + 1] - p_sbpre[gp0 + lane];
+                if (lane + 32 < nc && !(g_scale[h * LC + lane + 32] < 0.0f))
+                    n1 = p_sbpre[gp0 + lane + 33] - p_sbpre[gp0 + lane + 32];
+                uint32_t i0 = n0, i1 = n1;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t0 = __shfl_up_sync(kFull, i0, o), t1 = __shfl_up_sync(kFull, i1, o);
+                    if (lane >= o) {
+                        i0 += t0;
+                        i1 += t1;
+                    }
+                }
+                const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
+                total = tot0 + __shfl_sync(kFull, i1, 31);
+                st0 = n0 ? i0 - n0 : ~0u;
+                st1 = n1 ? tot0 + i1 - n1 : ~0u;
+            }
             int cur = -1;   // this octet's current list (index into the unit's probes)
-            uint32_t list_sb = 0, size = 0, push0 = 0, sb_first = 0, thr_hi = 0;
+            uint32_t list_sb = 0, size = 0, push0 = 0, thr_hi = 0;
             float scale = 1.0f, offset = 0.0f;
             int smax = 0;
             const uint4* L = lut_ring;
             // A take: the warp's next kSbPerWarp superblocks of the group, one per
-            // octet: ti (valid while < sbe) and its probe tp. Staged, the octets'
-            // leaders start bulk copies of the taken superblocks into stage `cst`.
-            auto take = [&](uint32_t& ti, int& tp) -> bool {
+            // octet: ti (valid while < total), its probe tp and the index tf of
+            // that list's first superblock. Staged, the octets' leaders start
+            // bulk copies of the taken superblocks into stage `cst`.
+            auto take = [&](uint32_t& ti, int& tp, uint32_t& tf) -> bool {
                 int base = 0;
                 if (lane == 0) base = atomicAdd(&s_next[h], kSbPerWarp);
                 base = __shfl_sync(kFull, base, 0);
-                if (sbb + static_cast<uint32_t>(base) >= sbe) return false;
-                ti = sbb + base + oct;
-                tp = ti < sbe ? gp0 + upper_index(p_sbpre + gp0, nc, ti) : -1;
+                if (static_cast<uint32_t>(base) >= total) return false;
+                ti = base + oct;
+                // the list of each octet's superblock: the last list starting at or before it
+                int jl = 0;
+#pragma unroll
+                for (int o = 0; o < kSbPerWarp; ++o) {
+                    const uint32_t t = base + o;
+                    const unsigned b1 = LC > 32 ? __ballot_sync(kFull, st1 <= t) : 0u;
+                    const unsigned b0 = __ballot_sync(kFull, st0 <= t);
+                    const int j = b1 ? 63 - __clz(b1) : 31 - __clz(b0);
+                    if (o == oct) jl = j;
+                }
+                const uint32_t f0 = __shfl_sync(kFull, st0, jl & 31), f1 = __shfl_sync(kFull, st1, jl & 31);
+                tf = jl < 32 ? f0 : f1;
+                tp = ti < total ? gp0 + jl : -1;
                 if constexpr (kStaged) {
-                    const uint32_t nvalid = min(static_cast<uint32_t>(kSbPerWarp), sbe - (sbb + base));
+                    const uint32_t nvalid = min(static_cast<uint32_t>(kSbPerWarp), total - base);
                     if (lane == 0) sm100::mbar_expect_tx(&cbar[cst], nvalid * sb_bytes);
                     __syncwarp();
                     if (r == 0 && tp >= 0) {
-                        const size_t sbg = static_cast<size_t>(p_sboff[tp]) + (ti - p_sbpre[tp]);
+                        const size_t sbg = static_cast<size_t>(p_sboff[tp]) + (ti - tf);
                         sm100::bulk_load(cstage + static_cast<size_t>(cst * kSbPerWarp + oct) * sb_bytes,
                                          v.codes + sbg * static_cast<size_t>(2 * v.m_pad), sb_bytes, &cbar[cst]);
                     }
@@ -450,7 +495,7 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
             };
             // The sums of take (i, p) and its candidates; codes from `src` (the
             // stage in shared memory, or global memory).
-            auto process = [&](uint32_t i, int p, int stage) {
+            auto process = [&](uint32_t i, int p, uint32_t first, int stage) {
                 const uint64_t thr = *reinterpret_cast<volatile unsigned long long*>(&s_thr);
                 uint32_t sums[8];
                 uint32_t cmask = 0, sbl = 0;
@@ -461,7 +506,6 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
                         list_sb = p_sboff[p];
                         size = p_size[p];
                         push0 = p_push[p];
-                        sb_first = p_sbpre[p];
                         scale = g_scale[h * LC + p - gp0];
                         offset = g_offset[h * LC + p - gp0];
                         L = shared_lut ? lut_ring : lut_ring + static_cast<size_t>(h * LC + p - gp0) * LS;
@@ -471,7 +515,7 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
                         thr_hi = static_cast<uint32_t>(thr >> 32);
                         smax = sum_limit_fast(thr_hi, scale, offset);
                     }
-                    sbl = i - sb_first;
+                    sbl = i - first;
                     sbg = static_cast<size_t>(list_sb) + sbl;
                     if (smax < 0) {   // no vector of the list can pass (its LUT may be unbuilt)
 #pragma unroll
@@ -546,27 +590,28 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
                     }
                 }
             };
-            uint32_t i0 = 0, i1 = 0;
+            uint32_t i0 = 0, i1 = 0, f0 = 0, f1 = 0;
             int q0 = -1, q1 = -1;
             int s0 = cst;
-            bool v0 = take(i0, q0);
+            bool v0 = take(i0, q0, f0);
             while (v0) {
                 if constexpr (kStaged) {
-                    const bool v1 = take(i1, q1);   // the next take's copies overlap this one's sums
+                    const bool v1 = take(i1, q1, f1);   // the next take's copies overlap this one's sums
                     if (!sm100::mbar_wait(&cbar[s0], (cpar >> s0) & 1u, &s_abort)) {
                         s_abort = 1;
                         atomicExch(a.err, 2);
                     }
                     cpar ^= 1u << s0;
-                    process(i0, q0, s0);
+                    process(i0, q0, f0, s0);
                     __syncwarp();   // stage s0 is free again
                     s0 ^= 1;
                     i0 = i1;
                     q0 = q1;
+                    f0 = f1;
                     v0 = v1;
                 } else {
-                    process(i0, q0, 0);
-                    v0 = take(i0, q0);
+                    process(i0, q0, f0, 0);
+                    v0 = take(i0, q0, f0);
                 }
             }
             // out of superblocks of group g: build group g + 1 in the other half

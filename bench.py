@@ -673,7 +673,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the continuous-batching server measurement")
     ap.add_argument("--nprobe", type=int, default=0, help="use this nprobe instead of the recall sweep (profiling)")
-    ap.add_argument("--scan-shape", default="auto", choices=["auto", "global", "staged"],
+    ap.add_argument("--scan-shape", default="auto", choices=["auto", "global", "staged", "dense"],
                     help="fast-scan kernel shape: autotuned (default) or fixed (profiling)")
     ap.add_argument("--workload", default="angular", choices=["angular", "small", "flat", "train", "served"],
                     help="angular: the headline line; small / flat / train / served: the other configurations")
@@ -707,7 +707,7 @@ def main():
     from qann_b200 import profiling
 
     if args.scan_shape != "auto":
-        qb.set_scan_options(autotune=False, variant=0 if args.scan_shape == "global" else 1)
+        qb.set_scan_options(autotune=False, variant={"global": 0, "staged": 1, "dense": 2}[args.scan_shape])
     base = mixture(cfg, 0, cfg["n"])
     queries = mixture(cfg, 1 + rank, cfg["nq"])
     index, path = build_or_load(cfg, base, rank, world, barrier)
@@ -786,7 +786,8 @@ def main():
         return 0
 
     so = qb.scan_options()["last_shape"]
-    scan_shape = {"warps": so // 1000, "lists_per_group": (so % 1000) // 10, "codes": "staged" if so % 10 else "global",
+    scan_shape = {"warps": so // 1000, "lists_per_group": (so % 1000) // 10,
+                  "codes": {0: "global", 1: "staged", 2: "global, dense"}[so % 10],
                   "autotuned": bool(qb.scan_options()["autotune"])}
     rec = recall(got, gt)
     assert np.array_equal(got, ids_h), "device-resident and host-API results differ"

@@ -212,9 +212,11 @@ int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, con
  *   staged through shared memory by bulk copies) on the first large search of
  *   each problem (scoring mode, m, k', nprobe, batch size) and keeps the
  *   fastest; 0 uses the first shape. "scan_variant": -1 (default) any shape,
- *   0 only unstaged, 1 only staged. qg_get_option also reads
- *   "scan_tuned_shapes" (problems tuned so far) and "scan_last_shape" (the
- *   last scan's shape: warps * 1000 + lists per group * 10 + staged). Results are the same under
+ *   0 only unstaged shapes sized for two blocks per SM, 1 only staged, 2 only
+ *   the dense unstaged shapes (registers sized for 3 blocks of 8 warps or 5
+ *   of 4). qg_get_option also reads "scan_tuned_shapes" (problems tuned so
+ *   far) and "scan_last_shape" (the last scan's shape: warps * 1000 + lists
+ *   per group * 10 + 1 staged / 2 dense). Results are the same under
  *   every shape. No counterpart in the reference, whose scan kernel is fixed
  *   (reference src/fast_scan.cpp:306-338).
  * "search_graphs": 1 makes qg_search_device replay device-resident, unfiltered

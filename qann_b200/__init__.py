@@ -108,8 +108,10 @@ def tensor_filter_counts() -> dict:
 def set_scan_options(autotune: bool | None = None, variant: int | None = None) -> None:
     """Fast-scan kernel shapes. autotune: time the candidate shapes on the
     first large search of each problem and keep the fastest (default on).
-    variant: -1 any shape, 0 codes read from global memory, 1 codes staged
-    through shared memory by bulk copies. Results are identical under every shape."""
+    variant: -1 any shape, 0 codes read from global memory (registers sized
+    for two blocks per SM), 1 codes staged through shared memory by bulk
+    copies, 2 codes from global memory with registers sized for more resident
+    warps (3 blocks of 8 warps or 5 of 4). Results are identical under every shape."""
     if autotune is not None:
         check(_lib.lib.qg_set_option(b"scan_autotune", int(bool(autotune))))
     if variant is not None:

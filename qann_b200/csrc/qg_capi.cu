@@ -584,7 +584,7 @@ int qg_set_option(const char* key, int64_t value) {
             require(value == 0 || value == 1, "scan_autotune must be 0 or 1");
             set_scan_autotune(static_cast<int>(value));
         } else if (k == "scan_variant") {
-            require(value >= -1 && value <= 1, "scan_variant must be -1, 0 or 1");
+            require(value >= -1 && value <= 2, "scan_variant must be -1, 0, 1 or 2");
             set_scan_variant(static_cast<int>(value));
         } else {
             throw Error(kInvalidArgument, "unknown option: " + k);

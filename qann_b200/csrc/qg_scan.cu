@@ -259,8 +259,10 @@ __host__ __device__ inline ScanLayout scan_layout(int kp, int m_pad, int qtab_le
     return L;
 }
 
-template <int NW, bool kStaged>
-__global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
+// kMinB: blocks per SM the register budget is sized for (the dense shapes
+// trade registers for more resident warps, which hide the scan's latencies).
+template <int NW, bool kStaged, int kMinB = (kStaged ? 1 : 2)>
+__global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
     extern __shared__ __align__(16) uint8_t sm[];
     constexpr int NT = NW * 32;
     constexpr unsigned kFull = 0xffffffffu;
@@ -659,15 +661,15 @@ __global__ void __launch_bounds__(NW * 32, kStaged ? 1 : 2) k_scan(ScanArgs a) {
     }
 }
 
-template <int NW, bool kStaged>
+template <int NW, bool kStaged, int kMinB = (kStaged ? 1 : 2)>
 static void launch_scan(const ScanArgs& a, size_t smem, cudaStream_t st) {
-    allow_large_smem<k_scan<NW, kStaged>>();
+    allow_large_smem<k_scan<NW, kStaged, kMinB>>();
     int per_sm = 0;
-    QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan<NW, kStaged>, NW * 32, smem));
+    QG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan<NW, kStaged, kMinB>, NW * 32, smem));
     require(per_sm > 0, "fast-scan launch configuration does not fit on the device", kUnsupported);
     const unsigned blocks = static_cast<unsigned>(std::min<long long>(a.nunits, static_cast<long long>(per_sm) * sm_count()));
     KernelTimer kt("scan", st);
-    k_scan<NW, kStaged><<<blocks, NW * 32, smem, st>>>(a);
+    k_scan<NW, kStaged, kMinB><<<blocks, NW * 32, smem, st>>>(a);
     QG_LAUNCH_CHECK();
 }
 
@@ -682,12 +684,13 @@ namespace {
 struct ScanShape {
     int nw = 0, lc = 0;
     bool staged = false;
+    bool dense = false;   // unstaged, registers sized for 3 (8 warps) or 5 (4 warps) blocks per SM
 };
 
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int, int, int>, ScanShape> g_tuned;   // (mode, m_pad, kp, P, log2 nq, variant) -> shape
 std::atomic<int> g_autotune{1};    // 0: the first fitting unstaged shape, 1: tune
-std::atomic<int> g_force{-1};      // -1: any; 0: unstaged only; 1: staged only
+std::atomic<int> g_force{-1};      // -1: any; 0: unstaged (two-block) only; 1: staged only; 2: dense only
 std::atomic<int> g_last_shape{0};  // the last scan's shape: warps * 1000 + lists per group * 10 + staged
 }
 
@@ -702,7 +705,8 @@ int scan_tuned_shapes() {
 }
 
 // Candidate shapes whose shared memory fits: up to three unstaged ones for two
-// blocks per SM (or one, when none fits that), and a staged one.
+// blocks per SM (or one, when none fits that), the dense unstaged ones whose
+// shared memory allows their block count, and a staged one.
 static std::vector<ScanShape> scan_shapes(int kp, int m_pad, int qtab_len, int pch, bool shared_lut) {
     static constexpr int kUnstaged[][2] = {{8, 32}, {8, 16}, {4, 32}, {4, 16}, {8, 8}, {4, 8}, {2, 8}, {2, 4}, {1, 4}, {1, 1}};
     static constexpr int kStagedShapes[][2] = {{8, 16}, {8, 8}, {4, 32}, {4, 16}, {4, 8}};
@@ -714,17 +718,33 @@ static std::vector<ScanShape> scan_shapes(int kp, int m_pad, int qtab_len, int p
             if (added == most) break;
             const int lc = shared_lut ? 64 : sh[1];
             const bool dup = std::any_of(out.begin(), out.end(), [&](const ScanShape& o) {
-                return o.nw == sh[0] && o.lc == lc && o.staged == staged;
+                return o.nw == sh[0] && o.lc == lc && o.staged == staged && !o.dense;
             });
             if (!dup && scan_layout(kp, m_pad, qtab_len, pch, shared_lut, sh[0], lc, staged).bytes <= limit) {
-                out.push_back({sh[0], lc, staged});
+                out.push_back({sh[0], lc, staged, false});
                 ++added;
             }
         }
         return added > 0;
     };
-    if (force != 1 && !fits(kUnstaged, false, 110 * 1024, 3)) fits(kUnstaged, false, 226 * 1024, 1);
-    if (force != 0) fits(kStagedShapes, true, 226 * 1024, 1);
+    if ((force == -1 || force == 0) && !fits(kUnstaged, false, 110 * 1024, 3)) fits(kUnstaged, false, 226 * 1024, 1);
+    if (force == -1 || force == 2) {
+        // dense: 8 warps x 3 blocks or 4 warps x 5 blocks per SM, the widest
+        // LUT group whose shared memory allows that many blocks
+        static constexpr int kDense[][3] = {{8, 3, 32}, {8, 3, 16}, {8, 3, 8}, {4, 5, 16}, {4, 5, 8}};
+        int added8 = 0, added4 = 0;
+        for (const auto& d : kDense) {
+            int& added = d[0] == 8 ? added8 : added4;
+            const int lc = shared_lut ? 64 : d[2];
+            const size_t limit = (227 * 1024) / d[1] - 1024;
+            if (added == 0 && scan_layout(kp, m_pad, qtab_len, pch, shared_lut, d[0], lc, false).bytes <= limit) {
+                out.push_back({d[0], lc, false, true});
+                added = 1;
+            }
+        }
+    }
+    if (force == -1 || force == 1) fits(kStagedShapes, true, 226 * 1024, 1);
+    if (out.empty()) fits(kUnstaged, false, 226 * 1024, 1);   // (a forced kind that fits nowhere)
     return out;
 }
 
@@ -738,6 +758,9 @@ static void run_scan(const ScanShape& sh, ScanArgs a, const IvfView& v, int qtab
             case 8: launch_scan<8, true>(a, smem, st); break;
             default: launch_scan<4, true>(a, smem, st); break;
         }
+    } else if (sh.dense) {
+        if (sh.nw == 8) launch_scan<8, false, 3>(a, smem, st);
+        else launch_scan<4, false, 5>(a, smem, st);
     } else {
         switch (sh.nw) {
             case 8: launch_scan<8, false>(a, smem, st); break;
@@ -901,7 +924,7 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
         std::lock_guard<std::mutex> g(g_tune_mu);
         g_tuned[key] = shape;
     }
-    g_last_shape.store(shape.nw * 1000 + shape.lc * 10 + (shape.staged ? 1 : 0));
+    g_last_shape.store(shape.nw * 1000 + shape.lc * 10 + (shape.staged ? 1 : shape.dense ? 2 : 0));
     run_scan(shape, a, v, qtab_len, st);
     if (!direct) merge_candidates(ckey.get(), cslot.get(), nq, nchunks, kp, out_key, out_slot, st);
 }

@@ -60,12 +60,12 @@ def scan_variant(request):
     qb.set_scan_options(autotune=True, variant=-1)
 
 
-@pytest.mark.parametrize("scan_variant", [0, 1], indirect=True)
+@pytest.mark.parametrize("scan_variant", [0, 1, 2], indirect=True)
 @pytest.mark.parametrize("kind", ["ivf", "refine"])
 @pytest.mark.parametrize("name", GEN)
 def test_scan_shapes_identical(golden, scan_variant, kind, name):
-    """Each fast-scan kernel shape (codes from global memory, or staged through
-    shared memory) returns the reference's results."""
+    """Each fast-scan kernel shape (codes from global memory with two or more
+    blocks per SM, or staged through shared memory) returns the reference's results."""
     idx = qb.load(golden / "gen" / f"{kind}_{name}.qann")
     q = np.load(golden / "gen" / "queries.npy")
     assert qb.scan_options()["variant"] == scan_variant

@@ -556,59 +556,87 @@ static void mm_topk_block(const float* q, size_t nq, const float* rows, const Mm
 // ---------------------------------------------------------------------------
 namespace {
 
-// The k-th smallest (1-based) of n uint32 keys in shared memory, by one block
-// (radix select, 8 bits a pass). hist: 256 ints of shared scratch.
-__device__ uint32_t block_kth_u32(const uint32_t* keys, int n, int k, int* hist, int* s_pick) {
-    uint32_t prefix = 0, mask = 0;
-    int need = k;
-    for (int shift = 24; shift >= 0; shift -= 8) {
-        for (int j = threadIdx.x; j < 256; j += blockDim.x) hist[j] = 0;
-        __syncthreads();
-        for (int base = 0; base < n; base += blockDim.x) {   // (loop trip count is block-uniform)
-            const int i = base + threadIdx.x;
-            const uint32_t key = i < n ? keys[i] : 0u;
-            const bool in = i < n && (key & mask) == prefix;
-            const int bin = in ? static_cast<int>((key >> shift) & 255) : -1;
-            // lanes of a warp that share a bin add once (the first passes put most keys in a few bins)
-            const unsigned same = __match_any_sync(0xffffffffu, bin);
-            if (in && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&hist[bin], __popc(same));
-        }
-        __syncthreads();
-        if (threadIdx.x < 32) {   // warp 0: the bin holding the need-th key
-            const int lane = threadIdx.x;
-            int c[8], own = 0;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                c[j] = hist[8 * lane + j];
-                own += c[j];
-            }
-            int incl = own;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            const int excl = incl - own;
-            if (excl < need && need <= incl) {
-                int acc = excl, digit = 8 * lane + 7;
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    if (acc + c[j] >= need) {
-                        digit = 8 * lane + j;
-                        break;
-                    }
-                    acc += c[j];
-                }
-                s_pick[0] = digit;
-                s_pick[1] = acc;
-            }
-        }
-        __syncthreads();
-        need -= s_pick[1];
-        prefix |= static_cast<uint32_t>(s_pick[0]) << shift;
-        mask |= 0xFFu << shift;
-        __syncthreads();
+// A threshold T at or above the k-th smallest (1-based) of the n uint32 keys
+// in shared memory, by one block. 0xFFFFFFFF marks an unbounded key, above
+// every other. [kmin, kmax] is the range of the nfin bounded keys; they are
+// counted into kCoarseBins equal key intervals, and T is the last key of the
+// first interval whose running count reaches k, so at least k keys are <= T
+// and T lies within one interval of the k-th smallest. (A T above the k-th
+// smallest only admits more candidates to the exact step.) hist: kCoarseBins
+// ints of shared scratch, zero on entry; two barriers.
+constexpr int kCoarseBins = 1024;
+__device__ uint32_t block_threshold_u32(const uint32_t* keys, int n, int k, uint32_t kmin, uint32_t kmax, int nfin,
+                                        int* hist, uint32_t* s_t) {
+    if (nfin < k) return 0xFFFFFFFFu;   // (block-uniform) the k-th smallest is unbounded
+    if (kmax == kmin) return kmin;
+    const uint64_t span = static_cast<uint64_t>(kmax - kmin) + 1;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t key = keys[i];
+        if (key != 0xFFFFFFFFu)
+            atomicAdd(&hist[static_cast<int>(static_cast<uint64_t>(key - kmin) * kCoarseBins / span)], 1);
     }
-    return prefix;
+    __syncthreads();
+    if (threadIdx.x < 32) {   // warp 0: lane l owns bins 32 l .. 32 l + 31
+        const int lane = threadIdx.x;
+        constexpr int kPer = kCoarseBins / 32;
+        int own = 0;
+#pragma unroll 8
+        for (int b = 0; b < kPer; ++b) own += hist[kPer * lane + b];
+        int incl = own;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int excl = incl - own;
+        if (excl < k && k <= incl) {
+            int acc = excl, bin = kPer * lane + kPer - 1;
+            for (int b = 0; b < kPer; ++b) {
+                acc += hist[kPer * lane + b];
+                if (acc >= k) {
+                    bin = kPer * lane + b;
+                    break;
+                }
+            }
+            // keys of bins <= bin: (key - kmin) * kCoarseBins < (bin + 1) * span
+            const uint64_t last = (static_cast<uint64_t>(bin + 1) * span + kCoarseBins - 1) / kCoarseBins - 1;
+            *s_t = static_cast<uint32_t>(min(static_cast<uint64_t>(kmin) + last, static_cast<uint64_t>(kmax)));
+        }
+    }
+    __syncthreads();
+    return *s_t;
+}
+
+// exact_avx2 of one row by the 8 lanes of an aligned lane group: lane L of the
+// group runs AVX2 lane L's four FMA chains (elements i + 8 j + L), the groups'
+// lane sums meet in exact_avx2's tree order through shuffles, and every lane
+// adds the tail. All 32 lanes of the warp call it together. Same bits as
+// exact_avx2<kL2>(a, b, n).
+template <bool kL2>
+__device__ __forceinline__ float exact_avx2_group8(const float* a, const float* __restrict__ b, int n) {
+    const int L = threadIdx.x & 7;
+    const int n32 = n & ~31, n8 = n & ~7;
+    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
+    int i = 0;
+    auto term = [&](int e, float acc) {
+        if (kL2) {
+            const float d = __fsub_rn(a[e], __ldg(b + e));
+            return __fmaf_rn(d, d, acc);
+        }
+        return __fmaf_rn(a[e], __ldg(b + e), acc);
+    };
+    for (; i < n32; i += 32) {
+        acc0 = term(i + L, acc0);
+        acc1 = term(i + 8 + L, acc1);
+        acc2 = term(i + 16 + L, acc2);
+        acc3 = term(i + 24 + L, acc3);
+    }
+    for (; i < n8; i += 8) acc0 = term(i + L, acc0);
+    const float sl = __fadd_rn(__fadd_rn(acc0, acc1), __fadd_rn(acc2, acc3));
+    const float t = __fadd_rn(sl, __shfl_down_sync(0xffffffffu, sl, 4, 8));   // lanes 0..3: s_L + s_{L+4}
+    const float t0 = __shfl_sync(0xffffffffu, t, 0, 8), t1 = __shfl_sync(0xffffffffu, t, 1, 8);
+    const float t2 = __shfl_sync(0xffffffffu, t, 2, 8), t3 = __shfl_sync(0xffffffffu, t, 3, 8);
+    const float r = __fadd_rn(__fadd_rn(t0, t1), __fadd_rn(t2, t3));
+    return exact_tail<kL2>(a, b, n8, n, r);
 }
 
 } // namespace
@@ -626,7 +654,8 @@ __global__ void __launch_bounds__(256, 4) k_coarse_recheck(const float* __restri
     uint64_t* ckey = reinterpret_cast<uint64_t*>(sm_raw);             // cap
     float* qv = reinterpret_cast<float*>(ckey + cap);                   // d, 16-byte aligned
     uint32_t* ub = reinterpret_cast<uint32_t*>(qv + ((d + 3) & ~3));    // nlist
-    __shared__ int hist[256], s_pick[2], s_count;
+    __shared__ int hist[kCoarseBins], s_count, s_wfin[8];
+    __shared__ uint32_t s_wmin[8], s_wmax[8], s_t;
     const float* arow = accm + static_cast<size_t>(qi) * ld;
     const float qq = q2[qi];
     const int qe = qexp[qi];
@@ -640,6 +669,7 @@ __global__ void __launch_bounds__(256, 4) k_coarse_recheck(const float* __restri
         return;
     }
     for (int t = threadIdx.x; t < d; t += blockDim.x) qv[t] = q[static_cast<size_t>(qi) * d + t];
+    for (int t = threadIdx.x; t < kCoarseBins; t += blockDim.x) hist[t] = 0;
     // upper bounds, rounded up at every step (c_up >= 1 + C for L2, >= C / 2
     // for inner product; the f16 row scaling is undone exactly by ldexpf).
     // Four lists per thread and step, read as 16-byte vectors.
@@ -649,20 +679,47 @@ __global__ void __launch_bounds__(256, 4) k_coarse_recheck(const float* __restri
         const float hi = ip ? __fmaf_ru(c_up, s, -a) : __fmaf_ru(-2.0f, a, __fmul_ru(c_up, s));
         return extreme(c2j) ? 0xFFFFFFFFu : float_key(hi);
     };
+    // (and the range and count of the bounded ones, for the threshold)
+    uint32_t kmin = 0xFFFFFFFFu, kmax = 0;
+    int nfin = 0;
+    auto keep = [&](int j, uint32_t u) {
+        ub[j] = u;
+        if (u != 0xFFFFFFFFu) {
+            kmin = min(kmin, u);
+            kmax = max(kmax, u);
+            ++nfin;
+        }
+    };
     const int n4 = nlist & ~3;
     for (int j = 4 * threadIdx.x; j < n4; j += 4 * blockDim.x) {
         const float4 av = *reinterpret_cast<const float4*>(arow + j);
         const float4 cv = *reinterpret_cast<const float4*>(c2 + j);
         const int4 ev = *reinterpret_cast<const int4*>(cexp + j);
-        ub[j] = upper(av.x, cv.x, ev.x);
-        ub[j + 1] = upper(av.y, cv.y, ev.y);
-        ub[j + 2] = upper(av.z, cv.z, ev.z);
-        ub[j + 3] = upper(av.w, cv.w, ev.w);
+        keep(j, upper(av.x, cv.x, ev.x));
+        keep(j + 1, upper(av.y, cv.y, ev.y));
+        keep(j + 2, upper(av.z, cv.z, ev.z));
+        keep(j + 3, upper(av.w, cv.w, ev.w));
     }
-    for (int j = n4 + threadIdx.x; j < nlist; j += blockDim.x) ub[j] = upper(arow[j], c2[j], cexp[j]);
+    for (int j = n4 + threadIdx.x; j < nlist; j += blockDim.x) keep(j, upper(arow[j], c2[j], cexp[j]));
+    for (int o = 16; o > 0; o >>= 1) {
+        kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+        kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+        nfin += __shfl_xor_sync(0xffffffffu, nfin, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_wmin[threadIdx.x >> 5] = kmin;
+        s_wmax[threadIdx.x >> 5] = kmax;
+        s_wfin[threadIdx.x >> 5] = nfin;
+    }
     if (threadIdx.x == 0) s_count = 0;
     __syncthreads();
-    const uint32_t T = block_kth_u32(ub, nlist, P, hist, s_pick);
+    for (int w = 0; w < 8; ++w) {
+        kmin = min(kmin, s_wmin[w]);
+        kmax = max(kmax, s_wmax[w]);
+    }
+    nfin = 0;
+    for (int w = 0; w < 8; ++w) nfin += s_wfin[w];
+    const uint32_t T = block_threshold_u32(ub, nlist, P, kmin, kmax, nfin, hist, &s_t);
     // candidates: lower bound, rounded down (c_lo <= 1 - C for L2; for inner
     // product the margin c_up is subtracted from a sum rounded up), <= T
     auto lower_in = [&](float acc_j, float c2j, int cej) -> bool {
@@ -693,15 +750,23 @@ __global__ void __launch_bounds__(256, 4) k_coarse_recheck(const float* __restri
         if (threadIdx.x == 0 && redo) redo[qi] = 1;
         return;
     }
-    // exact scores, one thread per candidate; each list's score is kept by
-    // list (over its upper bound, no longer needed) for the output
+    // exact scores, one candidate per 8-lane group; each list's score is kept
+    // by list (over its upper bound, no longer needed) for the output
     float* score_of = reinterpret_cast<float*>(ub);
-    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-        const int j = static_cast<int>(ckey[i]);
-        const float* row = cent + static_cast<size_t>(j) * d;
-        const float sc = exact_score(qv, row, d, ip);
-        ckey[i] = (static_cast<uint64_t>(float_key_eq0(sc)) << 32) | static_cast<uint32_t>(j);
-        score_of[j] = sc;
+    {
+        const int ngrp = blockDim.x >> 3, grp = threadIdx.x >> 3;
+        const int rounds = (cnt + ngrp - 1) / ngrp;   // (block-uniform)
+        for (int rd = 0; rd < rounds; ++rd) {
+            const int i = rd * ngrp + grp;
+            const bool act = i < cnt;
+            const int j = act ? static_cast<int>(ckey[i]) : 0;   // idle groups score row 0 unused
+            const float* row = cent + static_cast<size_t>(j) * d;
+            const float sc = ip ? -exact_avx2_group8<false>(qv, row, d) : exact_avx2_group8<true>(qv, row, d);
+            if (act && (threadIdx.x & 7) == 0) {
+                ckey[i] = (static_cast<uint64_t>(float_key_eq0(sc)) << 32) | static_cast<uint32_t>(j);
+                score_of[j] = sc;
+            }
+        }
     }
     __syncthreads();
     // the P smallest by (score, list), then sorted

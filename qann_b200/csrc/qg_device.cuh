@@ -275,7 +275,7 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
     return d;
 }
 
-// Device code layout (built from the file format's blocks, see qg_lists.cu):
+// Device code layout (built from the file format's blocks by pack_superblocks, qg_index.cu):
 // a list is stored in superblocks of 64 vectors. Octet lane r (0..7) owns
 // vectors 8r..8r+7; its word for subspace s holds their codes, vector 8r+i
 // in nibble i. Words are interleaved so each 16-byte load of the 8 lanes is
@@ -297,10 +297,12 @@ __device__ __forceinline__ void octet_step(const uint4& w, const uint4* __restri
         g0 += prmt(L.x, L.y, c) + prmt(L.z, L.w, cx);
         g1 += prmt(L.x, L.y, c >> 16) + prmt(L.z, L.w, cx >> 16);
     }
-    a0 += g0 & 0x00FF00FFu;
-    b0 += (g0 >> 8) & 0x00FF00FFu;
-    a1 += g1 & 0x00FF00FFu;
-    b1 += (g1 >> 8) & 0x00FF00FFu;
+    // bytes 0, 2 and 1, 3 of the byte sums widened into 16-bit fields by one
+    // byte permute each (selector nibble 4 picks a zero byte of the second operand)
+    a0 += prmt(g0, 0u, 0x4240u);
+    b0 += prmt(g0, 0u, 0x4341u);
+    a1 += prmt(g1, 0u, 0x4240u);
+    b1 += prmt(g1, 0u, 0x4341u);
 }
 
 __device__ __forceinline__ void octet_sums(const uint4* __restrict__ sb, const uint4* __restrict__ lut, int m_pad,

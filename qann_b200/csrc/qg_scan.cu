@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
     __shared__ int s_next[2], s_build[2];
     __shared__ unsigned long long s_thr;
     __shared__ int s_wcount[NW];
-    __shared__ uint32_t s_red[NW];
+    __shared__ uint32_t s_red[NW], s_red2[NW];
 
     if (tid == 0) s_abort = 0;
     if (kStaged && lane == 0) {
@@ -424,11 +424,87 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
             }
         };
 
+        // (all threads, after a block barrier; the per-warp histograms serve as one)
+        auto seed_threshold = [&]() {
+            int total = 0;
+            for (int w = 0; w < NW; ++w) total += s_wcount[w];
+            if (total <= kp) return;   // (block-uniform)
+            constexpr int kBins = NW * 256 < 1024 ? NW * 256 : 1024;
+            int* bh = reinterpret_cast<int*>(sm + lay.off_hist);
+            const uint64_t* wb0 = reinterpret_cast<const uint64_t*>(sm + lay.off_wbuf);
+            uint32_t lo = ~0u, hi = 0;
+            for (int w = 0; w < NW; ++w)
+                for (int i = tid; i < s_wcount[w]; i += NT) {
+                    const uint32_t k = static_cast<uint32_t>(wb0[static_cast<size_t>(w) * wcap + i] >> 32);
+                    lo = min(lo, k);
+                    hi = max(hi, k);
+                }
+            for (int t = tid; t < kBins; t += NT) bh[t] = 0;
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = min(lo, __shfl_xor_sync(kFull, lo, o));
+                hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+            }
+            if (lane == 0) {
+                s_red[warp] = lo;
+                s_red2[warp] = hi;
+            }
+            __syncthreads();
+            for (int w = 0; w < NW; ++w) {
+                lo = min(lo, s_red[w]);
+                hi = max(hi, s_red2[w]);
+            }
+            if (lo == hi) {   // (block-uniform)
+                if (tid == 0) atomicMin(&s_thr, (static_cast<unsigned long long>(lo) << 32) | 0xFFFFFFFFull);
+                return;
+            }
+            const uint64_t span = static_cast<uint64_t>(hi - lo) + 1;
+            for (int w = 0; w < NW; ++w)
+                for (int i = tid; i < s_wcount[w]; i += NT) {
+                    const uint32_t k = static_cast<uint32_t>(wb0[static_cast<size_t>(w) * wcap + i] >> 32);
+                    atomicAdd(&bh[static_cast<int>(static_cast<uint64_t>(k - lo) * kBins / span)], 1);
+                }
+            __syncthreads();
+            if (warp == 0) {   // lane l owns bins kPer l .. kPer l + kPer - 1
+                constexpr int kPer = kBins / 32;
+                int own = 0;
+                for (int b = 0; b < kPer; ++b) own += bh[kPer * lane + b];
+                int incl = own;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(kFull, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int excl = incl - own;
+                if (excl < kp && kp <= incl) {
+                    int acc = excl, bin = kPer * lane + kPer - 1;
+                    for (int b = 0; b < kPer; ++b) {
+                        acc += bh[kPer * lane + b];
+                        if (acc >= kp) {
+                            bin = kPer * lane + b;
+                            break;
+                        }
+                    }
+                    // keys of bins <= bin have (k - lo) * kBins < (bin + 1) * span
+                    const uint64_t last = (static_cast<uint64_t>(bin + 1) * span + kBins - 1) / kBins - 1;
+                    const uint32_t T = static_cast<uint32_t>(min(static_cast<uint64_t>(lo) + last, static_cast<uint64_t>(hi)));
+                    atomicMin(&s_thr, (static_cast<unsigned long long>(T) << 32) | 0xFFFFFFFFull);
+                }
+            }
+            __syncthreads();   // warp 0 is done with the histograms before any trim reuses them
+        };
+
         const int ngroups = (np + LC - 1) / LC;
         build_group(0);
         int wcount = 0;   // entries in this warp's buffer (the same in every lane)
         for (int g = 0; g < ngroups; ++g) {
             __syncthreads();   // group g's LUTs and the unit's prefix arrays are complete
+            // After the first group: the warps' buffers together hold the block's
+            // k' best keys so far, so the k'-th smallest of their union bounds the
+            // unit's final k'-th key. Its high half, rounded up to the end of a
+            // histogram interval, lowers the threshold: much tighter than any
+            // single warp's k'-th, so about half as many later takes reach the
+            // candidate path. (Repeating it at later groups cost more barriers
+            // than it saved.)
+            if (NW >= 4 && g == 1) seed_threshold();
             const int h = g & 1, gp0 = g * LC, nc = min(LC, np - gp0);
             // The group's superblocks without those of skipped lists, numbered
             // 0..total-1 list after list: list lane (and lane + 32 when LC = 64)
@@ -616,6 +692,7 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
                     v0 = take(i0, q0, f0);
                 }
             }
+            if (lane == 0) s_wcount[warp] = wcount;   // for the next group's threshold bound
             // out of superblocks of group g: build group g + 1 in the other half
             if (g + 1 < ngroups) build_group(g + 1);
         }

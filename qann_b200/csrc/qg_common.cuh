@@ -195,6 +195,41 @@ __device__ __forceinline__ float exact_avx2_vec(const float* __restrict__ a, con
     return exact_tail<kL2>(a, b, n8, n, r);
 }
 
+// exact_avx2 of one row by the 8 lanes of an aligned lane group: lane L of the
+// group runs AVX2 lane L's four FMA chains (elements i + 8 j + L), the groups'
+// lane sums meet in exact_avx2's tree order through shuffles, and every lane
+// adds the tail. All 32 lanes of the warp call it together. Same bits as
+// exact_avx2<kL2>(a, b, n). kLdg: b is global memory read through the
+// read-only path (else any address space).
+template <bool kL2, bool kLdg>
+__device__ __forceinline__ float exact_avx2_group8(const float* a, const float* __restrict__ b, int n) {
+    const int L = threadIdx.x & 7;
+    const int n32 = n & ~31, n8 = n & ~7;
+    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
+    int i = 0;
+    auto term = [&](int e, float acc) {
+        const float be = kLdg ? __ldg(b + e) : b[e];
+        if (kL2) {
+            const float d = __fsub_rn(a[e], be);
+            return __fmaf_rn(d, d, acc);
+        }
+        return __fmaf_rn(a[e], be, acc);
+    };
+    for (; i < n32; i += 32) {
+        acc0 = term(i + L, acc0);
+        acc1 = term(i + 8 + L, acc1);
+        acc2 = term(i + 16 + L, acc2);
+        acc3 = term(i + 24 + L, acc3);
+    }
+    for (; i < n8; i += 8) acc0 = term(i + L, acc0);
+    const float sl = __fadd_rn(__fadd_rn(acc0, acc1), __fadd_rn(acc2, acc3));
+    const float t = __fadd_rn(sl, __shfl_down_sync(0xffffffffu, sl, 4, 8));   // lanes 0..3: s_L + s_{L+4}
+    const float t0 = __shfl_sync(0xffffffffu, t, 0, 8), t1 = __shfl_sync(0xffffffffu, t, 1, 8);
+    const float t2 = __shfl_sync(0xffffffffu, t, 2, 8), t3 = __shfl_sync(0xffffffffu, t, 3, 8);
+    const float r = __fadd_rn(__fadd_rn(t0, t1), __fadd_rn(t2, t3));
+    return exact_tail<kL2>(a, b, n8, n, r);
+}
+
 // The score the reference's DenseIndex ranks by (reference
 // include/vecengine/index.hpp:269-271): squared L2, or -(a . b) for inner product.
 __device__ __forceinline__ float exact_score(const float* a, const float* b, int n, bool ip) {

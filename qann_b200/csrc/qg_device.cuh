@@ -150,6 +150,25 @@ __device__ __noinline__ static uint64_t warp_select_keep(uint64_t* buf, int n, i
 }
 
 
+// Keeps, in order, the keys of buf[0, n) at or below lim (by one warp, in
+// place) and returns how many there are.
+__device__ __noinline__ static int warp_keep_upto(uint64_t* buf, int n, uint64_t lim) {
+    const int lane = threadIdx.x & 31;
+    constexpr unsigned kFull = 0xffffffffu;
+    int out = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + lane;
+        const uint64_t k = i < n ? buf[i] : ~0ull;
+        const bool in = i < n && k <= lim;
+        const unsigned bal = __ballot_sync(kFull, in);
+        __syncwarp();
+        if (in) buf[out + __popc(bal & ((1u << lane) - 1))] = k;
+        out += __popc(bal);
+    }
+    __syncwarp();
+    return out;
+}
+
 // ---------------------------------------------------------------------------
 // Block reductions
 // ---------------------------------------------------------------------------

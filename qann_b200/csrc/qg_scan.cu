@@ -662,9 +662,17 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
                     wcount += __shfl_sync(kFull, incl, 31);
                     if (wcount > wcap - kSbPerWarp * kSuperBlock && wcount > kp) {
                         __syncwarp();
-                        const uint64_t kth = warp_select_keep(wbuf, min(wcount, wcap), kp, hist);
-                        if (lane == 0) atomicMin(&s_thr, static_cast<unsigned long long>(kth));
-                        wcount = kp;
+                        // keys above the block threshold cannot be among the unit's
+                        // k' best (the block holds k' keys at or below it, the one it
+                        // equals included): drop them first, and select only if more
+                        // than k' remain
+                        const uint64_t lim = *reinterpret_cast<volatile unsigned long long*>(&s_thr);
+                        wcount = warp_keep_upto(wbuf, min(wcount, wcap), lim);
+                        if (wcount > kp) {
+                            const uint64_t kth = warp_select_keep(wbuf, wcount, kp, hist);
+                            if (lane == 0) atomicMin(&s_thr, static_cast<unsigned long long>(kth));
+                            wcount = kp;
+                        }
                     }
                 }
             };

@@ -46,6 +46,7 @@ constexpr int kSbPerWarp = 4;    // superblocks a warp takes at a time, one per 
 // Row stride (floats) of the query's table C in shared memory: 80 bytes puts
 // the 16-byte reads of 8 lanes (one row each) on distinct banks.
 constexpr int kQtabStride = 20;
+constexpr int kFirstGroup = 4;   // lists in the first LUT group (at most LC)
 }
 
 // The 16 entries of LUT rows rounded and packed: round-half-even of
@@ -383,8 +384,13 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
         // build more of them. A list none of whose vectors can beat the block
         // threshold (even a zero sum's distance is above it) gets scale -1 (real
         // scales are >= 0) and no LUT; the group's scan skips its superblocks.
+        // Groups of LC lists, the first one of 4 only: its keys meet no threshold
+        // yet, so the block's bound on the k'-th key after it (below) comes
+        // sooner. (4 was best for 8 x 32, 8 x 16 and 4 x 8 shapes alike.)
+        const int first = min(LC, kFirstGroup);
+        auto group_start = [&](int g) { return g == 0 ? 0 : min(np, first + (g - 1) * LC); };
         auto build_group = [&](int g) {
-            const int h = g & 1, gp0 = g * LC, nc = min(LC, np - gp0);
+            const int h = g & 1, gp0 = group_start(g), nc = group_start(g + 1) - gp0;
             if (tid == 0) {
                 s_next[h] = 0;        // its last user, group g - 2, is done
                 s_build[h ^ 1] = 0;   // group g + 1's; its last user, group g - 1, is done
@@ -492,7 +498,7 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
             __syncthreads();   // warp 0 is done with the histograms before any trim reuses them
         };
 
-        const int ngroups = (np + LC - 1) / LC;
+        const int ngroups = np <= first ? 1 : 1 + (np - first + LC - 1) / LC;
         build_group(0);
         int wcount = 0;   // entries in this warp's buffer (the same in every lane)
         for (int g = 0; g < ngroups; ++g) {
@@ -505,7 +511,7 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
             // candidate path. (Repeating it at later groups cost more barriers
             // than it saved.)
             if (NW >= 4 && g == 1) seed_threshold();
-            const int h = g & 1, gp0 = g * LC, nc = min(LC, np - gp0);
+            const int h = g & 1, gp0 = group_start(g), nc = group_start(g + 1) - gp0;
             // The group's superblocks without those of skipped lists, numbered
             // 0..total-1 list after list: list lane (and lane + 32 when LC = 64)
             // starts at st0 (st1); empty and skipped lists hold ~0u, which no

@@ -503,14 +503,14 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
         int wcount = 0;   // entries in this warp's buffer (the same in every lane)
         for (int g = 0; g < ngroups; ++g) {
             __syncthreads();   // group g's LUTs and the unit's prefix arrays are complete
-            // After the first group: the warps' buffers together hold the block's
-            // k' best keys so far, so the k'-th smallest of their union bounds the
-            // unit's final k'-th key. Its high half, rounded up to the end of a
-            // histogram interval, lowers the threshold: much tighter than any
-            // single warp's k'-th, so about half as many later takes reach the
-            // candidate path. (Repeating it at later groups cost more barriers
-            // than it saved.)
-            if (NW >= 4 && g == 1) seed_threshold();
+            // After the first two groups: the warps' buffers together hold the
+            // block's k' best keys so far, so the k'-th smallest of their union
+            // bounds the unit's final k'-th key. Its high half, rounded up to the
+            // end of a histogram interval, lowers the threshold: much tighter than
+            // any single warp's k'-th, so about half as many later takes reach
+            // the candidate path. (At later groups it cost more barriers than it
+            // saved.)
+            if (NW >= 4 && (g == 1 || g == 2)) seed_threshold();
             const int h = g & 1, gp0 = group_start(g), nc = group_start(g + 1) - gp0;
             // The group's superblocks without those of skipped lists, numbered
             // 0..total-1 list after list: list lane (and lane + 32 when LC = 64)

@@ -332,9 +332,12 @@ def plain_fp32_qps(base, queries, k, metric):
     try:
         flat.batch_query(queries[:200], k)   # warm-up
         n = min(2000, queries.shape[0])
-        t = time.perf_counter()
-        flat.batch_query(queries[:n], k)
-        return n / (time.perf_counter() - t)
+        best = 0.0
+        for _ in range(3):   # the best of three, in the baseline's favour
+            t = time.perf_counter()
+            flat.batch_query(queries[:n], k)
+            best = max(best, n / (time.perf_counter() - t))
+        return best
     finally:
         qb.set_tensor_filter(1)
 

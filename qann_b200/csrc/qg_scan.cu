@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
             for (int rr = tid; rr < v.m_pad; rr += NT) lut_ring[rr] = a.qlut[static_cast<size_t>(qi) * v.m_pad + rr];
         if (tid == 0) {
             s_overflow = 0;
-            s_thr = ~0ull;
+            s_thr = a.qthr ? *reinterpret_cast<volatile unsigned long long*>(a.qthr + qi) : ~0ull;
             s_next[0] = 0;
             s_next[1] = 0;
             s_build[0] = 0;
@@ -460,7 +460,10 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
                 hi = max(hi, s_red2[w]);
             }
             if (lo == hi) {   // (block-uniform)
-                if (tid == 0) atomicMin(&s_thr, (static_cast<unsigned long long>(lo) << 32) | 0xFFFFFFFFull);
+                if (tid == 0) {
+                    atomicMin(&s_thr, (static_cast<unsigned long long>(lo) << 32) | 0xFFFFFFFFull);
+                    if (a.qthr) atomicMin(a.qthr + qi, (static_cast<unsigned long long>(lo) << 32) | 0xFFFFFFFFull);
+                }
                 return;
             }
             const uint64_t span = static_cast<uint64_t>(hi - lo) + 1;
@@ -493,6 +496,7 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
                     const uint64_t last = (static_cast<uint64_t>(bin + 1) * span + kBins - 1) / kBins - 1;
                     const uint32_t T = static_cast<uint32_t>(min(static_cast<uint64_t>(lo) + last, static_cast<uint64_t>(hi)));
                     atomicMin(&s_thr, (static_cast<unsigned long long>(T) << 32) | 0xFFFFFFFFull);
+                    if (a.qthr) atomicMin(a.qthr + qi, (static_cast<unsigned long long>(T) << 32) | 0xFFFFFFFFull);
                 }
             }
             __syncthreads();   // warp 0 is done with the histograms before any trim reuses them
@@ -502,6 +506,8 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
         build_group(0);
         int wcount = 0;   // entries in this warp's buffer (the same in every lane)
         for (int g = 0; g < ngroups; ++g) {
+            if (a.qthr && tid == 0)   // the bound the query's other chunks reached meanwhile
+                atomicMin(&s_thr, *reinterpret_cast<volatile unsigned long long*>(a.qthr + qi));
             __syncthreads();   // group g's LUTs and the unit's prefix arrays are complete
             // After the first two groups: the warps' buffers together hold the
             // block's k' best keys so far, so the k'-th smallest of their union
@@ -676,7 +682,10 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
                         wcount = warp_keep_upto(wbuf, min(wcount, wcap), lim);
                         if (wcount > kp) {
                             const uint64_t kth = warp_select_keep(wbuf, wcount, kp, hist);
-                            if (lane == 0) atomicMin(&s_thr, static_cast<unsigned long long>(kth));
+                            if (lane == 0) {
+                                atomicMin(&s_thr, static_cast<unsigned long long>(kth));
+                                if (a.qthr) atomicMin(a.qthr + qi, static_cast<unsigned long long>(kth));
+                            }
                             wcount = kp;
                         }
                     }
@@ -844,6 +853,8 @@ static void run_scan(const ScanShape& sh, ScanArgs a, const IvfView& v, int qtab
     a.lc = sh.lc;
     const size_t smem = scan_layout(a.kp, v.m_pad, qtab_len, a.pch, shared_lut, sh.nw, sh.lc, sh.staged).bytes;
     QG_CUDA(cudaMemsetAsync(a.work, 0, sizeof(int), st));
+    if (a.qthr)   // (every timed run of the autotuner starts from no bound too)
+        QG_CUDA(cudaMemsetAsync(a.qthr, 0xFF, static_cast<size_t>(a.nunits / a.nchunks) * sizeof(unsigned long long), st));
     if (sh.staged) {
         switch (sh.nw) {
             case 8: launch_scan<8, true>(a, smem, st); break;
@@ -968,9 +979,11 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     const size_t nout = static_cast<size_t>(nq) * nchunks * kp;
     DevBuf<uint64_t> ckey;
     DevBuf<uint32_t> cslot;
+    DevBuf<unsigned long long> qthr;
     if (!direct) {
         ckey.alloc(nout, st);
         cslot.alloc(nout, st);
+        qthr.alloc(nq, st);
     }
     DevBuf<int> work(1, st);
     QG_CUDA(cudaMemsetAsync(work.get(), 0, sizeof(int), st));
@@ -992,6 +1005,7 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     a.kp = kp;
     a.nunits = nq * nchunks;
     a.work = work.get();
+    a.qthr = direct ? nullptr : qthr.get();
     a.out_key = direct ? out_key : ckey.get();
     a.out_slot = direct ? out_slot : cslot.get();
     a.err = s.d_err;

@@ -70,6 +70,9 @@ struct ScanArgs {
     int nunits;              // nq * nchunks work units (query, chunk of pch probes)
     int lc;                  // lists per LUT group
     int* work;               // next unit to take (zero at launch)
+    // per query, shared by its chunks (nchunks > 1; else null): a bound on the
+    // query's k'-th key, all ones at launch; every chunk lowers it and prunes by it
+    unsigned long long* qthr;
     uint64_t* out_key;       // (nq * nchunks) * kp
     uint32_t* out_slot;
     int* err;

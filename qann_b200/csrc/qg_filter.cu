@@ -6,7 +6,8 @@
 // exactly the allowed vectors scanned; so the probe count of each query is the
 // first p >= min_probes whose lists hold >= wanted allowed vectors. Each query
 // may carry its own filter (a mixed batch of served requests); the walk reads
-// only the ids of the lists the query goes on to scan.
+// only the ids of the lists the query goes on to scan: the min_probes nearest
+// ones in parallel, then one list at a time while fewer than `wanted` are seen.
 #include "qg_device.cuh"
 #include "qg_search.h"
 
@@ -30,15 +31,56 @@ __global__ void __launch_bounds__(256) k_rank_lists(const float* __restrict__ sc
     }
 }
 
+// Allowed vectors in the min_probes nearest lists of each filtered query, in
+// parallel: kWalkBlocks blocks per query, a warp per list at a time, the id
+// and bitmap loads of 4 strides of the list in flight together; the blocks'
+// counts meet by atomics in seen[q] (zero at launch).
+constexpr int kWalkBlocks = 16;
+__global__ void __launch_bounds__(256) k_allowed_first(IvfView v, const uint32_t* __restrict__ ranked, int nq,
+                                                       const uint64_t* filter, const uint64_t* const* filters,
+                                                       int min_probes, const int* __restrict__ min_q,
+                                                       unsigned long long* __restrict__ seen) {
+    const int q = blockIdx.x / kWalkBlocks, part = blockIdx.x % kWalkBlocks;
+    const uint64_t* f = filters ? filters[q] : filter;
+    if (q >= nq || !f) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int mp = min(min_q ? min_q[q] : min_probes, v.nlist);
+    const uint32_t* r = ranked + static_cast<size_t>(q) * v.nlist;
+    uint32_t c = 0;
+    for (int i = part * nw + warp; i < mp; i += kWalkBlocks * nw) {
+        const uint32_t l = r[i];
+        const size_t b0 = static_cast<size_t>(v.sb_off[l]) * kSuperBlock;
+        const uint32_t n = v.list_size[l];
+        for (uint32_t j0 = 0; j0 < n; j0 += 128) {
+            uint32_t slot[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t j = j0 + 32 * u + lane;
+                slot[u] = j < n ? v.ids[b0 + j] : 0xFFFFFFFFu;
+            }
+            uint64_t w[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) w[u] = slot[u] != 0xFFFFFFFFu ? f[slot[u] >> 6] : 0ull;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (slot[u] != 0xFFFFFFFFu) c += static_cast<uint32_t>((w[u] >> (slot[u] & 63)) & 1ull);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0 && c) atomicAdd(seen + q, static_cast<unsigned long long>(c));
+}
+
 // warp per query: its probe count. A query with a filter walks its lists
 // nearest first, counting each list's allowed vectors, and stops at the first
 // p >= min_probes with >= wanted seen (the reference stops on its TopK's size,
-// which before the first trim counts exactly the allowed vectors scanned). A
-// query without one probes its own nprobe.
+// which before the first trim counts exactly the allowed vectors scanned). The
+// min_probes nearest lists are counted in parallel beforehand (seen0), so the
+// walk starts there and usually stops at once. A query without a filter
+// probes its own nprobe.
 __global__ void k_probe_walk(IvfView v, const uint32_t* __restrict__ ranked, int nq, const uint64_t* filter,
                              const uint64_t* const* filters, int min_probes, int wanted, const int* __restrict__ min_q,
                              const int* __restrict__ wanted_q, int nprobe, const int* __restrict__ nprobe_q,
-                             int* __restrict__ out) {
+                             const unsigned long long* __restrict__ seen0, int* __restrict__ out) {
     const int q = static_cast<int>((static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (q >= nq) return;
@@ -51,8 +93,8 @@ __global__ void k_probe_walk(IvfView v, const uint32_t* __restrict__ ranked, int
     const int mp = min_q ? min_q[q] : min_probes;
     const long long want = wanted_q ? wanted_q[q] : wanted;
     const uint32_t* r = ranked + static_cast<size_t>(q) * nlist;
-    long long seen = 0;
-    int p = 0;
+    long long seen = static_cast<long long>(seen0[q]);
+    int p = min(mp, nlist);   // lists [0, p) are counted in seen
     for (; p < nlist; ++p) {
         if (p >= mp && seen >= want) break;
         const uint32_t l = r[p];
@@ -98,9 +140,14 @@ int filtered_probes(const IvfView& v, const IvfSearchArgs& s, DevBuf<uint32_t>& 
     }
     scores.release();
     nprobe_q.alloc(nq, st);
+    DevBuf<unsigned long long> seen(nq, st);
+    QG_CUDA(cudaMemsetAsync(seen.get(), 0, nq * sizeof(unsigned long long), st));
+    k_allowed_first<<<static_cast<unsigned>(nq) * kWalkBlocks, 256, 0, st>>>(v, ranked.get(), nq, s.filter, s.pq.filter,
+                                                                              s.min_probes, s.pq.min_probes, seen.get());
+    QG_LAUNCH_CHECK();
     k_probe_walk<<<static_cast<unsigned>(ceil_div(static_cast<size_t>(nq) * 32, 256)), 256, 0, st>>>(
         v, ranked.get(), nq, s.filter, s.pq.filter, s.min_probes, s.wanted, s.pq.min_probes, s.pq.wanted, s.nprobe,
-        s.pq.nprobe, nprobe_q.get());
+        s.pq.nprobe, seen.get(), nprobe_q.get());
     QG_LAUNCH_CHECK();
     std::vector<int> h(nq);
     QG_CUDA(cudaMemcpyAsync(h.data(), nprobe_q.get(), nq * sizeof(int), cudaMemcpyDeviceToHost, st));

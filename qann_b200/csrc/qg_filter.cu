@@ -16,8 +16,10 @@
 
 namespace qg {
 
-// one block per query: every list sorted by (score, list) (float order, -0 == +0)
-__global__ void __launch_bounds__(256) k_rank_lists(const float* __restrict__ scores, int nlist, int npow,
+// one block per query: every list sorted by (score, list) (float order, -0 == +0);
+// 1024 threads, as the sort's stages are barrier-bound and the keys (up to
+// 128 KB) hold the SM to one block anyway
+__global__ void __launch_bounds__(1024) k_rank_lists(const float* __restrict__ scores, int nlist, int npow,
                                                     uint32_t* __restrict__ out_list, float* __restrict__ out_score) {
     extern __shared__ uint64_t keys[];
     const float* row = scores + static_cast<size_t>(blockIdx.x) * nlist;
@@ -135,7 +137,7 @@ int filtered_probes(const IvfView& v, const IvfSearchArgs& s, DevBuf<uint32_t>& 
         allow_large_smem<k_rank_lists>();
     {
         KernelTimer kt("rank_lists", st);
-        k_rank_lists<<<nq, 256, smem, st>>>(scores.get(), nlist, npow, ranked.get(), rscore.get());
+        k_rank_lists<<<nq, 1024, smem, st>>>(scores.get(), nlist, npow, ranked.get(), rscore.get());
         QG_LAUNCH_CHECK();
     }
     scores.release();

@@ -173,7 +173,6 @@ __global__ void __launch_bounds__(256) k_select_rows(const float* __restrict__ s
     __shared__ uint32_t hist[256];
     __shared__ uint32_t s_prefix, s_mask, s_remaining;
     __shared__ uint32_t warp_cnt[2][8];
-    __shared__ uint32_t s_lt, s_eq;
     const float* row = scores + static_cast<size_t>(blockIdx.x) * ld;
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -185,51 +184,83 @@ __global__ void __launch_bounds__(256) k_select_rows(const float* __restrict__ s
         for (int b = tid; b < 256; b += blockDim.x) hist[b] = 0;
         __syncthreads();
         const uint32_t prefix = s_prefix, mask = s_mask;
-        for (int c = tid; c < ncols; c += blockDim.x) {
-            const uint32_t k = col_allowed(allow, deny, col_base + c) ? (eq0 ? float_key_eq0(row[c]) : float_key(row[c]))
-                                                                       : 0xFFFFFFFFu;
-            if ((k & mask) == prefix) atomicAdd(&hist[(k >> shift) & 255u], 1u);
+        for (int c0 = 0; c0 < ncols; c0 += blockDim.x) {   // (trip count block-uniform)
+            const int c = c0 + tid;
+            const uint32_t k = c < ncols && col_allowed(allow, deny, col_base + c)
+                                   ? (eq0 ? float_key_eq0(row[c]) : float_key(row[c]))
+                                   : 0xFFFFFFFFu;
+            const int bin = c < ncols && (k & mask) == prefix ? static_cast<int>((k >> shift) & 255u) : -1;
+            // lanes of a warp that share a bin add once (early passes put most keys in a few bins)
+            const unsigned same = __match_any_sync(0xffffffffu, bin);
+            if (bin >= 0 && (tid & 31) == __ffs(same) - 1) atomicAdd(&hist[bin], static_cast<uint32_t>(__popc(same)));
         }
         __syncthreads();
-        if (tid == 0) {
-            uint32_t rem = s_remaining, b = 0;
-            for (; b < 256; ++b) {
-                if (hist[b] >= rem) break;
-                rem -= hist[b];
+        if (tid < 32) {   // warp 0: the bin holding the remaining-th key, lane l owning bins 8 l .. 8 l + 7
+            const uint32_t rem = s_remaining;
+            uint32_t cb[8], own = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                cb[j] = hist[8 * tid + j];
+                own += cb[j];
             }
-            s_remaining = rem;
-            s_prefix = prefix | (b << shift);
-            s_mask = mask | (255u << shift);
+            uint32_t incl = own;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (tid >= o) incl += t;
+            }
+            const uint32_t excl = incl - own;
+            if (excl < rem && rem <= incl) {
+                uint32_t left = rem - excl, b = 8 * tid + 7;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (cb[j] >= left) {
+                        b = 8 * tid + j;
+                        break;
+                    }
+                    left -= cb[j];
+                }
+                s_remaining = left;
+                s_prefix = prefix | (b << shift);
+                s_mask = mask | (255u << shift);
+            }
         }
         __syncthreads();
     }
     const uint32_t T = s_prefix;
     const uint32_t need_eq = s_remaining;   // ties at T to take, in column order
-    if (tid == 0) {
-        s_lt = 0;
-        s_eq = 0;
+    // the P columns: keys below T, then the first need_eq ties at T in column
+    // order. Each warp owns a contiguous run of columns: it counts its own,
+    // the warps' counts give each one its offsets, and it writes in order.
+    const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
+    const int span = ((ncols + nwarps - 1) / nwarps + 31) & ~31;
+    const int c_begin = min(ncols, warp * span), c_end = min(ncols, c_begin + span);
+    auto key_at = [&](int c) -> uint32_t {
+        return col_allowed(allow, deny, col_base + c) ? (eq0 ? float_key_eq0(row[c]) : float_key(row[c])) : 0xFFFFFFFFu;
+    };
+    uint32_t n_lt = 0, n_eq = 0;
+    for (int c0 = c_begin; c0 < c_end; c0 += 32) {
+        const int c = c0 + lane;
+        const uint32_t k = c < c_end ? key_at(c) : 0xFFFFFFFFu;
+        n_lt += __popc(__ballot_sync(0xffffffffu, c < c_end && k < T));
+        n_eq += __popc(__ballot_sync(0xffffffffu, c < c_end && k == T));
+    }
+    if (lane == 0) {
+        warp_cnt[0][warp] = n_lt;
+        warp_cnt[1][warp] = n_eq;
     }
     __syncthreads();
-    const int warp = tid >> 5, lane = tid & 31;
-    for (int base = 0; base < ncols; base += blockDim.x) {
-        const int c = base + tid;
-        const uint32_t k = c < ncols && col_allowed(allow, deny, col_base + c)
-                               ? (eq0 ? float_key_eq0(row[c]) : float_key(row[c]))
-                               : 0xFFFFFFFFu;
-        const bool lt = c < ncols && k < T;
-        const bool eq = c < ncols && k == T;
+    uint32_t off_lt = 0, off_eq = 0;
+    for (int w = 0; w < warp; ++w) {
+        off_lt += warp_cnt[0][w];
+        off_eq += warp_cnt[1][w];
+    }
+    const uint32_t below = (1u << lane) - 1u;
+    for (int c0 = c_begin; c0 < c_end; c0 += 32) {
+        const int c = c0 + lane;
+        const uint32_t k = c < c_end ? key_at(c) : 0xFFFFFFFFu;
+        const bool lt = c < c_end && k < T;
+        const bool eq = c < c_end && k == T;
         const uint32_t blt = __ballot_sync(0xffffffffu, lt), beq = __ballot_sync(0xffffffffu, eq);
-        if (lane == 0) {
-            warp_cnt[0][warp] = __popc(blt);
-            warp_cnt[1][warp] = __popc(beq);
-        }
-        __syncthreads();
-        uint32_t off_lt = s_lt, off_eq = s_eq;
-        for (int w = 0; w < warp; ++w) {
-            off_lt += warp_cnt[0][w];
-            off_eq += warp_cnt[1][w];
-        }
-        const uint32_t below = (1u << lane) - 1u;
         if (lt) {
             const uint32_t pos = off_lt + __popc(blt & below);
             skey[pos] = static_cast<uint64_t>(k);
@@ -243,17 +274,25 @@ __global__ void __launch_bounds__(256) k_select_rows(const float* __restrict__ s
                 sval[pos] = c;
             }
         }
+        off_lt += __popc(blt);
+        off_eq += __popc(beq);
+    }
+    // in (key, column) order: up to 1,024 of them, each one's rank is the count
+    // of smaller pairs (all distinct) and it goes straight to its place, with
+    // no sorting stages; beyond that a bitonic sort
+    if (P <= 1024) {   // (block-uniform)
         __syncthreads();
-        if (tid == 0) {
-            uint32_t tl = 0, te = 0;
-            for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
-                tl += warp_cnt[0][w];
-                te += warp_cnt[1][w];
-            }
-            s_lt += tl;
-            s_eq += te;
+        for (int i = tid; i < P; i += blockDim.x) {
+            const uint64_t ki = skey[i];
+            const int64_t vi = sval[i];
+            int rank = 0;
+            for (int j = 0; j < P; ++j) rank += pair_less(skey[j], sval[j], ki, vi);
+            const uint32_t col = static_cast<uint32_t>(vi);
+            const bool ok = col_allowed(allow, deny, col_base + col);
+            out_col[static_cast<size_t>(blockIdx.x) * P + rank] = ok ? col : 0xFFFFFFFFu;
+            out_score[static_cast<size_t>(blockIdx.x) * P + rank] = ok ? row[col] : __int_as_float(0x7f800000);
         }
-        __syncthreads();
+        return;
     }
     for (int i = P + tid; i < Pp; i += blockDim.x) {
         skey[i] = ~0ull;

@@ -608,7 +608,7 @@ __device__ uint32_t block_threshold_u32(const uint32_t* keys, int n, int k, uint
 
 } // namespace
 
-__global__ void __launch_bounds__(256, 4) k_coarse_recheck(const float* __restrict__ q, const float* __restrict__ q2,
+__global__ void __launch_bounds__(256, 6) k_coarse_recheck(const float* __restrict__ q, const float* __restrict__ q2,
                                                         const int* __restrict__ qexp, const float* __restrict__ cent,
                                                         const float* __restrict__ c2, const int* __restrict__ cexp,
                                                         int nlist, int d, bool ip, float c_up, float c_lo,

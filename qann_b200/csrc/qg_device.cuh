@@ -352,6 +352,35 @@ __device__ __forceinline__ void octet_sums(const uint4* __restrict__ sb, const u
     sums[7] = b1 >> 16;
 }
 
+// octet_sums for code arrays padded by kCodePad uint4 past their last
+// superblock: the loads two words ahead need no bounds tests (those past the
+// superblock read the next one or the padding, and are never used).
+inline constexpr int kCodePad = 16;
+__device__ __forceinline__ void octet_sums_padded(const uint4* __restrict__ sb, const uint4* __restrict__ lut,
+                                                  int m_pad, int r, uint32_t sums[8]) {
+    uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+    const int nq = m_pad >> 2;
+    const uint4* p = sb + r;
+    uint4 c0 = __ldg(p), c1 = __ldg(p + 8);
+    int q = 0;
+    for (; q + 2 <= nq; q += 2) {
+        const uint4 n0 = __ldg(p + (q + 2) * 8), n1 = __ldg(p + (q + 3) * 8);
+        octet_step(c0, lut + 4 * q, a0, b0, a1, b1);
+        octet_step(c1, lut + 4 * (q + 1), a0, b0, a1, b1);
+        c0 = n0;
+        c1 = n1;
+    }
+    if (q < nq) octet_step(c0, lut + 4 * q, a0, b0, a1, b1);
+    sums[0] = a0 & 0xFFFFu;
+    sums[1] = b0 & 0xFFFFu;
+    sums[2] = a0 >> 16;
+    sums[3] = b0 >> 16;
+    sums[4] = a1 & 0xFFFFu;
+    sums[5] = b1 & 0xFFFFu;
+    sums[6] = a1 >> 16;
+    sums[7] = b1 >> 16;
+}
+
 // Fast-scan distance of an integer sum: sums / scale + offset, an IEEE
 // division then an add (reference src/ivf_index.cpp:496).
 __device__ __forceinline__ float fs_dist(uint32_t sum, float scale, float offset) {

@@ -193,7 +193,7 @@ void ensure_device(IVFObj& o, cudaStream_t) {
     upload(D.sb_off, sb_off, st);
     upload(D.list_size, sizes, st);
     D.total_sb = total_sb;
-    D.codes.alloc(std::max<size_t>(1, total_sb * 2 * m_pad), st);
+    D.codes.alloc(total_sb * 2 * m_pad + kCodePad, st);   // (the scan reads up to kCodePad uint4 past the end)
     D.ids.alloc(std::max<size_t>(1, total_sb * kSuperBlock), st);
     pack_superblocks(dcodes.get(), dids.get(), dvoff.get(), D.sb_off.get(), D.list_size.get(), dsbl.get(), total_sb, m,
                      m_pad, D.codes.get(), D.ids.get(), st);

@@ -615,7 +615,7 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
                                               cstage + static_cast<size_t>(stage * kSbPerWarp + oct) * sb_bytes),
                                           L, v.m_pad, r, sums);
                     } else {
-                        octet_sums(v.codes + sbg * static_cast<size_t>(2 * v.m_pad), L, v.m_pad, r, sums);
+                        octet_sums_padded(v.codes + sbg * static_cast<size_t>(2 * v.m_pad), L, v.m_pad, r, sums);
                     }
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {

@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(128) k_finalize_ivf(const uint64_t* __restrict
 // reading whole rows with coalesced loads, at an odd row stride so that the
 // threads' walks along their own rows fall on distinct banks.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_refine(const float* __restrict__ q, int dim, const float* __restrict__ rows,
+__global__ void __launch_bounds__(128, 8) k_refine(const float* __restrict__ q, int dim, const float* __restrict__ rows,
                                                 const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ slot_in,
                                                 int kp, int k, bool ip, const int64_t* __restrict__ labels, bool cosine,
                                                 int64_t* __restrict__ out_ids, float* __restrict__ out_d,
@@ -542,6 +542,7 @@ __global__ void __launch_bounds__(128) k_refine(const float* __restrict__ q, int
     float* qv = reinterpret_cast<float*>(val + kpow);
     float* trow = qv + dim;
     const int stride = dim | 1;
+    __shared__ uint32_t s_slot[64];   // the tile's slots (tile <= 64)
     const int qi = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     const int kpq = kp_q ? min(kp_q[qi], kp) : kp;   // the query's first kpq candidates by key64
@@ -554,28 +555,35 @@ __global__ void __launch_bounds__(128) k_refine(const float* __restrict__ q, int
     for (int t0 = 0; t0 < kpq; t0 += tile) {
         const int nt = min(tile, kpq - t0);
         __syncthreads();   // the previous tile's rows are consumed
-        // each warp gathers 4 rows at a time, 16 loads per lane in flight
-        for (int c0 = warp; c0 < nt; c0 += 4 * nwarps) {
-            const float* src[4];
-            bool ok[4];
+        // the tile's slots first (0xFFFFFFFF: no candidate), so that the row
+        // loads below do not wait on them batch by batch
+        for (int c = threadIdx.x; c < nt; c += blockDim.x) {
+            const size_t ci = static_cast<size_t>(qi) * kp + t0 + c;
+            s_slot[c] = key_in[ci] != ~0ull ? slot_in[ci] : 0xFFFFFFFFu;
+        }
+        __syncthreads();
+        // each warp gathers 8 rows at a time, 32 loads per lane in flight
+        for (int c0 = warp; c0 < nt; c0 += 8 * nwarps) {
+            const float* src[8];
+            bool ok[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < 8; ++u) {
                 const int c = c0 + u * nwarps;
-                const size_t ci = static_cast<size_t>(qi) * kp + t0 + c;
-                ok[u] = c < nt && key_in[ci] != ~0ull;
-                src[u] = ok[u] ? rows + static_cast<size_t>(slot_in[ci]) * dim : rows;
+                const uint32_t sl = c < nt ? s_slot[c] : 0xFFFFFFFFu;
+                ok[u] = sl != 0xFFFFFFFFu;
+                src[u] = ok[u] ? rows + static_cast<size_t>(sl) * dim : rows;
             }
             for (int e0 = 0; e0 < dim; e0 += 128) {
-                float x[4][4];
+                float x[8][4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+                for (int u = 0; u < 8; ++u)
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         const int e = e0 + lane + 32 * j;
                         x[u][j] = ok[u] && e < dim ? __ldg(src[u] + e) : 0.0f;
                     }
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+                for (int u = 0; u < 8; ++u)
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         const int e = e0 + lane + 32 * j;
@@ -586,15 +594,15 @@ __global__ void __launch_bounds__(128) k_refine(const float* __restrict__ q, int
         __syncthreads();
         for (int c = threadIdx.x; c < nt; c += blockDim.x) {
             const int i = t0 + c;
-            const size_t ci = static_cast<size_t>(qi) * kp + i;
-            if (key_in[ci] == ~0ull) {
+            const uint32_t sl = s_slot[c];
+            if (sl == 0xFFFFFFFFu) {
                 key[i] = ~0ull;
                 val[i] = INT64_MAX;
                 continue;
             }
             const float d = exact_score(qv, trow + c * stride, dim, ip);
             key[i] = float_key_eq0(d);
-            val[i] = slot_in[ci];
+            val[i] = sl;
         }
     }
     bitonic_sort(key, val, kpow);

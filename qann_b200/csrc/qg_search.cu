@@ -326,20 +326,25 @@ void select_rows(const float* scores, size_t ld, int nrows, int ncols, int P, ui
 //   mode IP          : offset term = A = -(q . c)
 //   mode cosine-IP   : base = (A + 1) - |e|^2 (reference src/ivf_index.cpp:577-579)
 // ---------------------------------------------------------------------------
+// One (query, probe) pair per 8-lane group: the exact distance to the list's
+// residual center in exact_avx2's order (each group reads its row as 32-byte
+// segments, so the rows cross L2 once).
 __global__ void k_probe_terms(IvfView v, const float* __restrict__ q, int nq, int P, const uint32_t* __restrict__ probe,
                               const float* __restrict__ pdist, float* __restrict__ term) {
-    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= static_cast<size_t>(nq) * P) return;
+    const size_t n = static_cast<size_t>(nq) * P;
+    const size_t i0 = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
+    const bool in = i0 < n;   // (whole warps call the group scorer together)
+    const size_t i = in ? i0 : 0;
     const int qi = static_cast<int>(i / P);
     const uint32_t list = probe[i];
     float A = pdist[i];
     if (v.has_resid) {
         const float* qa = q + static_cast<size_t>(qi) * v.dim;
         const float* rc = v.resid + static_cast<size_t>(list) * v.dim;
-        A = (v.dim & 3) == 0 ? exact_avx2_vec<true>(qa, rc, v.dim) : exact_avx2<true>(qa, rc, v.dim);
+        A = exact_avx2_group8<true, true>(qa, rc, v.dim);
     }
     if (v.mode == kModeCosIP) A = __fsub_rn(__fadd_rn(A, 1.0f), v.sqnorm[list]);
-    term[i] = A;
+    if (in && (threadIdx.x & 7) == 0) term[i] = A;
 }
 
 // ---------------------------------------------------------------------------
@@ -678,7 +683,8 @@ void probe_terms(const IvfView& v, const float* q, int nq, int P, const uint32_t
                  cudaStream_t st) {
     const size_t n = static_cast<size_t>(nq) * P;
     if (n == 0) return;
-    k_probe_terms<<<static_cast<unsigned>(ceil_div(n, 256)), 256, 0, st>>>(v, q, nq, P, probe, pdist, term);
+    KernelTimer kt("probe_terms", st);
+    k_probe_terms<<<static_cast<unsigned>(ceil_div(n * 8, 256)), 256, 0, st>>>(v, q, nq, P, probe, pdist, term);
     QG_LAUNCH_CHECK();
 }
 

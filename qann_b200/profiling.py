@@ -6,8 +6,8 @@ import ctypes as C
 
 from . import _lib
 
-KERNELS = ("pair_scores", "select_rows", "coarse_mm", "coarse_recheck", "query_tables", "scan", "merge", "refine",
-           "rank_lists", "mm_filter")
+KERNELS = ("pair_scores", "select_rows", "coarse_mm", "coarse_recheck", "probe_terms", "query_tables", "scan", "merge",
+           "refine", "rank_lists", "mm_filter")
 
 
 def enable(on: bool = True) -> None:

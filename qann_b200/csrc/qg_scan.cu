@@ -46,7 +46,7 @@ constexpr int kSbPerWarp = 4;    // superblocks a warp takes at a time, one per 
 // Row stride (floats) of the query's table C in shared memory: 80 bytes puts
 // the 16-byte reads of 8 lanes (one row each) on distinct banks.
 constexpr int kQtabStride = 20;
-constexpr int kFirstGroup = 4;   // lists in the first LUT group (at most LC)
+constexpr int kFirstGroup = 2;   // lists in the first LUT group (at most LC)
 }
 
 // The 16 entries of LUT rows rounded and packed: round-half-even of
@@ -384,9 +384,10 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
         // build more of them. A list none of whose vectors can beat the block
         // threshold (even a zero sum's distance is above it) gets scale -1 (real
         // scales are >= 0) and no LUT; the group's scan skips its superblocks.
-        // Groups of LC lists, the first one of 4 only: its keys meet no threshold
+        // Groups of LC lists, the first one of 2 only: its keys meet no threshold
         // yet, so the block's bound on the k'-th key after it (below) comes
-        // sooner. (4 was best for 8 x 32, 8 x 16 and 4 x 8 shapes alike.)
+        // sooner. (2 to 4 lists measured best for 8 x 32, 8 x 16 and 4 x 8 shapes
+        // alike, 2 by a little.)
         const int first = min(LC, kFirstGroup);
         auto group_start = [&](int g) { return g == 0 ? 0 : min(np, first + (g - 1) * LC); };
         auto build_group = [&](int g) {

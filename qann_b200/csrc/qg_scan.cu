@@ -716,7 +716,7 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
                     v0 = take(i0, q0, f0);
                 }
             }
-            if (lane == 0) s_wcount[warp] = wcount;   // for the next group's threshold bound
+            if (lane == 0) s_wcount[warp] = min(wcount, wcap);   // for the next group's threshold bound
             // out of superblocks of group g: build group g + 1 in the other half
             if (g + 1 < ngroups) build_group(g + 1);
         }

@@ -387,6 +387,13 @@ __device__ __forceinline__ float fs_dist(uint32_t sum, float scale, float offset
     return __fadd_rn(__fdiv_rn(static_cast<float>(sum), scale), offset);
 }
 
+// fs_dist(0, scale, offset) without the division: 0 / scale is +0 for any
+// scale > 0 (+inf included), and the LUT scales are >= 0 (0 / 0 gives the
+// canonical NaN, as here).
+__device__ __forceinline__ float fs_dist0(float scale, float offset) {
+    return scale > 0.0f ? __fadd_rn(0.0f, offset) : __int_as_float(0x7fffffff);
+}
+
 // Largest integer sum whose distance has key <= thr_key, or -1 when none;
 // 65535 when every sum passes. Distances grow monotonically with the sum, so
 // the exact float test `key(dist(S)) <= thr_key` becomes `S <= result`.
@@ -413,7 +420,7 @@ __device__ __forceinline__ int sum_limit_fast(uint32_t thr_key, float scale, flo
     // far outside the sum range: distances are monotone in the sum, so one
     // end decides it (a list whose smallest distance is above the threshold
     // is the common case once the threshold has tightened)
-    if (!(x > -4.0f)) return pass(0) ? sum_limit(thr_key, scale, offset) : -1;
+    if (!(x > -4.0f)) return float_key(fs_dist0(scale, offset)) <= thr_key ? sum_limit(thr_key, scale, offset) : -1;
     if (!(x < 65540.0f)) return pass(65535) ? 65535 : sum_limit(thr_key, scale, offset);
     int s = max(-1, min(65535, __float2int_rd(x)));
     for (int it = 0; it < 4; ++it) {

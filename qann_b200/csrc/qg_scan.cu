@@ -108,7 +108,7 @@ __device__ __forceinline__ bool warp_lut3(RowFn row, int m, int m_pad, float* ro
     const float p2 = __shfl_sync(0xffffffffu, part, 2), p3 = __shfl_sync(0xffffffffu, part, 3);
     const float offset = __fadd_rn(__fadd_rn(p0, p1), __fadd_rn(p2, p3));
     const float scale = widest > 0.0f ? __fdiv_rn(static_cast<float>(kLutMax), widest) : 1.0f;
-    const bool live = thr_hi == 0xFFFFFFFFu || float_key(fs_dist(0u, scale, offset)) <= thr_hi;   // (warp-uniform)
+    const bool live = thr_hi == 0xFFFFFFFFu || float_key(fs_dist0(scale, offset)) <= thr_hi;   // (warp-uniform)
     if (live) {
         for (int r = lane; r < m; r += 32) {
             row(r, v0);
@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
                 if (shared_lut) {
                     if (lane == 0) {
                         const float sc = a.qscale[qi], of = __fadd_rn(a.qoffset[qi], a.pterm[qp + p0 + p]);
-                        const bool live = thr_now == 0xFFFFFFFFu || float_key(fs_dist(0u, sc, of)) <= thr_now;
+                        const bool live = thr_now == 0xFFFFFFFFu || float_key(fs_dist0(sc, of)) <= thr_now;
                         g_scale[h * LC + j] = live ? sc : -1.0f;
                         g_offset[h * LC + j] = of;
                     }

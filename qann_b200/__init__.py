@@ -6,8 +6,9 @@ re-ranking, ``FlatIndex``, their ``train`` / ``add`` / ``batch_query`` /
 ``save`` / ``load``, ``nprobe``, ``k_factor`` and ``allowed`` filters, with
 the same signatures, defaults, errors and ``.qann`` files. Behind it, C++ host
 code drives hand-written sm_100a CUDA kernels through the C ABI in
-``include/qann_gpu.h``; results match the reference's CPU build (see
-DESIGN.md for the exact contract).
+``include/qann_gpu.h``; results match the reference's CPU build: the same
+ids, bit-identical distances and byte-identical ``.qann`` files after
+training and adding.
 
 Differences from qann: ``where=`` metadata filters are evaluated by the
 caller (pass the matching ids as ``allowed``); HNSW, SQ, sparse, hybrid and

@@ -1,7 +1,7 @@
 // `.qann` reader/writer and the slot<->id map for the host-side models.
 //
-// Field order per body follows the reference file format so files are
-// interchangeable with qann (see DESIGN.md "format"):
+// Field order per body follows the reference file format (format version
+// 13), so files move between qann and this library in both directions:
 //   IVF    reference src/ivf_index.cpp:904-974 (save), :976-1122 (load)
 //   Refine reference src/refine_index.cpp:158-213
 //   Flat   reference src/flat_index.cpp:101-133

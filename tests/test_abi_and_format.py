@@ -69,6 +69,23 @@ def test_setters_validate():
         ivf.nprobe = 0
 
 
+def test_scan_options_validate():
+    """Scan shape options (host state only: no kernel runs): each variant -1..2
+    is kept, anything else is refused and leaves the setting as it was."""
+    try:
+        for variant in (-1, 0, 1, 2):
+            qb.set_scan_options(autotune=False, variant=variant)
+            assert qb.scan_options()["variant"] == variant
+            assert qb.scan_options()["autotune"] == 0
+        for bad in (-2, 3):
+            with pytest.raises(ValueError, match="scan_variant"):
+                qb.set_scan_options(variant=bad)
+            assert qb.scan_options()["variant"] == 2
+    finally:
+        qb.set_scan_options(autotune=True, variant=-1)
+    assert qb.scan_options()["variant"] == -1 and qb.scan_options()["autotune"] == 1
+
+
 @pytest.mark.parametrize("name", ["gen/refine_l2.qann", "gen/ivf_cos_ip.qann", "gen/ivf_l2_custom_del.qann",
                                   "gen/refine_l2_custom_del.qann", "gen/refine_cos_l2.qann"])
 def test_resave_is_byte_identical(golden, tmp_path, name):

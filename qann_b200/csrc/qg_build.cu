@@ -261,7 +261,7 @@ static size_t compact_obj(IndexObj& idx, bool keep_ids) {
     if (idx.kind == Kind::Flat) {
         auto& o = static_cast<FlatObj&>(idx);
         if (o.model.idmap.deleted_count() && !o.model.meta.empty())
-            throw Error(kUnsupported, "compacting an index with metadata columns is not supported by this build");
+            throw Error(kUnsupported, "compacting an index with metadata columns is not supported by this library");
         auto remap = o.model.idmap.compact(keep_ids);
         if (remap.empty()) return 0;
         compact_rows(o.model.data, remap, o.model.dim, o.model.idmap.slots());
@@ -271,7 +271,7 @@ static size_t compact_obj(IndexObj& idx, bool keep_ids) {
     if (idx.kind == Kind::IVF) {
         auto& o = static_cast<IVFObj&>(idx);
         if (o.model.idmap.deleted_count() && !o.model.meta.empty())
-            throw Error(kUnsupported, "compacting an index with metadata columns is not supported by this build");
+            throw Error(kUnsupported, "compacting an index with metadata columns is not supported by this library");
         auto remap = o.model.idmap.compact(keep_ids);
         if (remap.empty()) return 0;
         compact_ivf_storage(o.model, remap);
@@ -280,7 +280,7 @@ static size_t compact_obj(IndexObj& idx, bool keep_ids) {
     }
     auto& o = static_cast<RefineObj&>(idx);
     if (o.map.deleted_count() && !o.meta.empty())
-        throw Error(kUnsupported, "compacting an index with metadata columns is not supported by this build");
+        throw Error(kUnsupported, "compacting an index with metadata columns is not supported by this library");
     auto remap = o.map.compact(keep_ids);
     if (remap.empty()) return 0;
     {

@@ -69,6 +69,22 @@ def test_quantize_rounds_half_to_even():
     assert list(lut[17:26]) == [0, 2, 2, 62, 0, 1, 1, 0, 3]
 
 
+@pytest.mark.parametrize("m,sd", [(4, 4), (50, 2), (64, 2)])
+def test_coarse_plus_list_term_plus_inner_table_is_the_residual_adc(m, sd):
+    # reference tests/test_distance.cpp:702-723: per subspace, A (the query-centroid
+    # distance) + B (list term) + C (inner table) equals the ADC table of q - c
+    # within 1e-3 (numpy-drawn codebook, query and centroid here)
+    rng = np.random.default_rng(700 + m)
+    yt = rng.normal(size=(m, sd, 16)).astype(np.float32)
+    q, c = rng.normal(size=(2, m * sd)).astype(np.float32)
+    adc = orc.adc_table(q - c, yt, m, sd).reshape(m, 16)
+    inner = orc.inner_table(q, yt, m, sd).reshape(m, 16)
+    lt = orc.list_term(c, yt, m, sd).reshape(m, 16)
+    for s in range(m):
+        a = orc.l2(q[s * sd:(s + 1) * sd], c[s * sd:(s + 1) * sd])
+        np.testing.assert_allclose(a + lt[s] + inner[s], adc[s], rtol=0, atol=1e-3)
+
+
 @pytest.mark.parametrize("m", [2, 6, 16, 64, 196, 256, 480, 1024])
 def test_mask_at_limits(m):
     # reference tests/test_fast_scan.cpp:416-439 (inputs drawn by numpy here)

@@ -613,6 +613,7 @@ def served_workload(args):
     index = qb.load(path)
     nreq = 20_000
     q = gaussian_mixture(nreq, d, 8192, 0.2, seed_rows=1)
+    batch = batch_scan_roofline(index, q[:10_000], m, (32, 256), max(3, args.steps // 10), max(3, args.warmup))
     rng = np.random.default_rng(2)
     pool = []
     for _ in range(16):
@@ -668,8 +669,63 @@ def served_workload(args):
                    "k": [10, 100], "nprobe": "log-uniform 8..256", "filtered": 0.3, "selectivity": [0.01, 0.5],
                    "slots": 4, "max_batch": 256},
         "rates": out, "results_equal_solo_searches": same, "mean_batch": round(st["completed"] / st["batches"], 1),
-        "plain_fp32_gpu_flat_qps": round(fp32_qps, 1)}))
+        "plain_fp32_gpu_flat_qps": round(fp32_qps, 1), "batch_scan": batch}))
     return 0
+
+
+def batch_scan_roofline(index, queries, m, nprobes, steps, warmup):
+    """Device-resident batches of the served index at fixed nprobe, k 10: QPS
+    and the scan's algorithmic code bytes per second against the HBM peak.
+    The codes (n x m / 2 bytes: 160 MB at 5M x 64) exceed the 126 MB L2, so
+    this is the scan's HBM-bound case; the L2 is flushed between steps."""
+    import torch
+    from qann_b200 import profiling
+    dev = torch.device("cuda:0")
+    nq, k = queries.shape[0], 10
+    q_dev = torch.from_numpy(queries).to(dev)
+    ids = torch.empty((nq, k), dtype=torch.int64, device=dev)
+    dists = torch.empty((nq, k), dtype=torch.float32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    peak, peak_src = measured_peak("hbm_gbs", 6650.0)
+    base = index.base
+    old = base.nprobe
+    out = []
+    for p in nprobes:
+        base.nprobe = p
+        for _ in range(warmup):
+            index.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), dists.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        profiling.enable(True)
+        profiling.reset()
+        step_ms = []
+        for _ in range(steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            index.search_device(q_dev.data_ptr(), nq, k, ids.data_ptr(), dists.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+        scan_ms, scan_n = profiling.get("scan")
+        profiling.enable(False)
+        per_launch = scan_ms / max(1, scan_n)
+        alg = algorithmic_scan_bytes({"m": m}, index, queries, p, dev)
+        achieved = alg / (per_launch / 1e3) / 1e9
+        out.append({"nprobe": p, "nq": nq, "k": k, "qps": round(nq * steps / (sum(step_ms) / 1e3), 1),
+                    "scan_launch_ms": round(per_launch, 4), "algorithmic_bytes_per_launch": alg,
+                    "achieved_gbs": round(achieved, 1), "peak_gbs": peak, "frac": round(achieved / peak, 4),
+                    "peak_source": peak_src, "scan_shape": qb_last_shape()})
+        log(f"batch scan at nprobe {p}: {out[-1]}")
+    base.nprobe = old
+    return out
+
+
+def qb_last_shape():
+    import qann_b200 as qb
+    so = qb.scan_options()["last_shape"]
+    return {"warps": so // 1000, "lists_per_group": (so % 1000) // 10,
+            "codes": {0: "global", 1: "staged", 2: "global, dense"}.get(so % 10)}
 
 
 def main():

@@ -613,7 +613,20 @@ def served_workload(args):
     index = qb.load(path)
     nreq = 20_000
     q = gaussian_mixture(nreq, d, 8192, 0.2, seed_rows=1)
-    batch = batch_scan_roofline(index, q[:10_000], m, (32, 256), max(3, args.steps // 10), max(3, args.warmup))
+    if args.scan_shape != "auto":
+        qb.set_scan_options(autotune=False, variant={"global": 0, "staged": 1, "dense": 2}[args.scan_shape])
+    batch = batch_scan_roofline(index, q[:10_000], m, (args.nprobe,) if args.nprobe else (32, 256),
+                                max(3, args.steps // 10), max(3, args.warmup))
+    if args.no_served:   # the batch measurement alone
+        print(json.dumps({
+            "metric": "batch QPS of the served index (5M x 128 IVF16384-PQ64x4fs + refine kf10, k 10)",
+            "value": batch[-1]["qps"], "unit": "queries/s", "n_gpus": 1, "steps": max(3, args.steps // 10),
+            "warmup": max(3, args.warmup), "ms_per_step": round(10_000 / batch[-1]["qps"] * 1e3, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": f"served_{n}x{d}_nl{nlist}_m{m}_kf{kf}", "nq": 10_000, "k": 10,
+                       "nprobe": batch[-1]["nprobe"], "l2": "flushed between steps (256 MB write)"},
+            "batch_scan": batch}))
+        return 0
     rng = np.random.default_rng(2)
     pool = []
     for _ in range(16):

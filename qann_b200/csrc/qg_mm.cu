@@ -243,9 +243,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (a.store) {
                     if (live) {
                         float* dst = a.store + static_cast<size_t>(qi) * a.ld + (r0 - a.n0);
+                        if (r0 + 32 <= a.n1 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+                            // a whole 32-column run: 16-byte stores, a quarter of the store instructions
 #pragma unroll
-                        for (int j = 0; j < 32; ++j)
-                            if (r0 + j < a.n1) dst[j] = __uint_as_float(v[j]);
+                            for (int j = 0; j < 32; j += 4)
+                                *reinterpret_cast<float4*>(dst + j) =
+                                    make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                                                __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                if (r0 + j < a.n1) dst[j] = __uint_as_float(v[j]);
+                        }
                     }
                     continue;
                 }

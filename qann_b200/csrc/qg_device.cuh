@@ -435,4 +435,28 @@ __device__ __forceinline__ int sum_limit_fast(uint32_t thr_key, float scale, flo
     return sum_limit(thr_key, scale, offset);
 }
 
+// nbins nearly equal intervals over the keys lo .. lo + span - 1, found by a
+// multiply-high instead of a 64-bit division per key. With span > nbins,
+// mul = floor(2^32 nbins / span) < 2^32 and bin(x) = floor((x - lo) mul / 2^32)
+// <= floor(nbins (span - 1) / span) < nbins; otherwise every key has its own
+// interval (mul = 0). last(b), the largest key whose interval is <= b, is
+// lo + ceil((b + 1) 2^32 / mul) - 1 (x mul < (b + 1) 2^32), so a threshold
+// taken there is at or above every key counted in intervals 0 .. b.
+struct KeyBins {
+    uint32_t lo, mul;
+    __device__ __forceinline__ KeyBins(uint32_t lo_, uint64_t span, int nbins)
+        : lo(lo_),
+          mul(span > static_cast<uint64_t>(nbins)
+                  ? static_cast<uint32_t>((static_cast<uint64_t>(nbins) << 32) / span)
+                  : 0u) {}
+    __device__ __forceinline__ int bin(uint32_t key) const {
+        const uint32_t x = key - lo;
+        return static_cast<int>(mul ? __umulhi(x, mul) : x);
+    }
+    __device__ __forceinline__ uint64_t last(int b) const {
+        return static_cast<uint64_t>(lo) +
+               (mul ? ((static_cast<uint64_t>(b + 1) << 32) + mul - 1) / mul - 1 : static_cast<uint64_t>(b));
+    }
+};
+
 } // namespace qg

@@ -568,7 +568,7 @@ namespace {
 // A threshold T at or above the k-th smallest (1-based) of the n uint32 keys
 // in shared memory, by one block. 0xFFFFFFFF marks an unbounded key, above
 // every other. [kmin, kmax] is the range of the nfin bounded keys; they are
-// counted into kCoarseBins equal key intervals, and T is the last key of the
+// counted into kCoarseBins nearly equal key intervals (KeyBins), and T is the last key of the
 // first interval whose running count reaches k, so at least k keys are <= T
 // and T lies within one interval of the k-th smallest. (A T above the k-th
 // smallest only admits more candidates to the exact step.) hist: kCoarseBins
@@ -578,11 +578,10 @@ __device__ uint32_t block_threshold_u32(const uint32_t* keys, int n, int k, uint
                                         int* hist, uint32_t* s_t) {
     if (nfin < k) return 0xFFFFFFFFu;   // (block-uniform) the k-th smallest is unbounded
     if (kmax == kmin) return kmin;
-    const uint64_t span = static_cast<uint64_t>(kmax - kmin) + 1;
+    const KeyBins kb(kmin, static_cast<uint64_t>(kmax - kmin) + 1, kCoarseBins);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const uint32_t key = keys[i];
-        if (key != 0xFFFFFFFFu)
-            atomicAdd(&hist[static_cast<int>(static_cast<uint64_t>(key - kmin) * kCoarseBins / span)], 1);
+        if (key != 0xFFFFFFFFu) atomicAdd(&hist[kb.bin(key)], 1);
     }
     __syncthreads();
     if (threadIdx.x < 32) {   // warp 0: lane l owns bins 32 l .. 32 l + 31
@@ -606,9 +605,8 @@ __device__ uint32_t block_threshold_u32(const uint32_t* keys, int n, int k, uint
                     break;
                 }
             }
-            // keys of bins <= bin: (key - kmin) * kCoarseBins < (bin + 1) * span
-            const uint64_t last = (static_cast<uint64_t>(bin + 1) * span + kCoarseBins - 1) / kCoarseBins - 1;
-            *s_t = static_cast<uint32_t>(min(static_cast<uint64_t>(kmin) + last, static_cast<uint64_t>(kmax)));
+            // every key counted in bins <= bin is <= kb.last(bin)
+            *s_t = static_cast<uint32_t>(min(kb.last(bin), static_cast<uint64_t>(kmax)));
         }
     }
     __syncthreads();

@@ -467,11 +467,11 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
                 }
                 return;
             }
-            const uint64_t span = static_cast<uint64_t>(hi - lo) + 1;
+            const KeyBins kb(lo, static_cast<uint64_t>(hi - lo) + 1, kBins);
             for (int w = 0; w < NW; ++w)
                 for (int i = tid; i < s_wcount[w]; i += NT) {
                     const uint32_t k = static_cast<uint32_t>(wb0[static_cast<size_t>(w) * wcap + i] >> 32);
-                    atomicAdd(&bh[static_cast<int>(static_cast<uint64_t>(k - lo) * kBins / span)], 1);
+                    atomicAdd(&bh[kb.bin(k)], 1);
                 }
             __syncthreads();
             if (warp == 0) {   // lane l owns bins kPer l .. kPer l + kPer - 1
@@ -493,9 +493,8 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
                             break;
                         }
                     }
-                    // keys of bins <= bin have (k - lo) * kBins < (bin + 1) * span
-                    const uint64_t last = (static_cast<uint64_t>(bin + 1) * span + kBins - 1) / kBins - 1;
-                    const uint32_t T = static_cast<uint32_t>(min(static_cast<uint64_t>(lo) + last, static_cast<uint64_t>(hi)));
+                    // every key counted in bins <= bin is <= kb.last(bin)
+                    const uint32_t T = static_cast<uint32_t>(min(kb.last(bin), static_cast<uint64_t>(hi)));
                     atomicMin(&s_thr, (static_cast<unsigned long long>(T) << 32) | 0xFFFFFFFFull);
                     if (a.qthr) atomicMin(a.qthr + qi, (static_cast<unsigned long long>(T) << 32) | 0xFFFFFFFFull);
                 }

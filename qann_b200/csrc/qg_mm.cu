@@ -615,6 +615,13 @@ __device__ uint32_t block_threshold_u32(const uint32_t* keys, int n, int k, uint
 
 } // namespace
 
+// x * 2^e rounded to nearest, which is what ldexpf returns: one multiply by
+// 2^e when that is a normal float (the product is then the correctly rounded
+// x * 2^e), ldexpf itself otherwise.
+__device__ __forceinline__ float scale_pow2(float x, int e) {
+    return (e >= -126 && e <= 127) ? __fmul_rn(x, __int_as_float((e + 127) << 23)) : ldexpf(x, e);
+}
+
 __global__ void __launch_bounds__(256, 6) k_coarse_recheck(const float* __restrict__ q, const float* __restrict__ q2,
                                                         const int* __restrict__ qexp, const float* __restrict__ cent,
                                                         const float* __restrict__ c2, const int* __restrict__ cexp,
@@ -645,11 +652,11 @@ __global__ void __launch_bounds__(256, 6) k_coarse_recheck(const float* __restri
     for (int t = threadIdx.x; t < d; t += blockDim.x) qv[t] = q[static_cast<size_t>(qi) * d + t];
     for (int t = threadIdx.x; t < kCoarseBins; t += blockDim.x) hist[t] = 0;
     // upper bounds, rounded up at every step (c_up >= 1 + C for L2, >= C / 2
-    // for inner product; the f16 row scaling is undone exactly by ldexpf).
+    // for inner product; the f16 row scaling is undone exactly by scale_pow2).
     // Four lists per thread and step, read as 16-byte vectors.
     auto upper = [&](float acc_j, float c2j, int cej) -> uint32_t {
         const float s = __fadd_ru(qq, c2j);
-        const float a = ldexpf(acc_j, -(qe + cej));
+        const float a = scale_pow2(acc_j, -(qe + cej));
         const float hi = ip ? __fmaf_ru(c_up, s, -a) : __fmaf_ru(-2.0f, a, __fmul_ru(c_up, s));
         return extreme(c2j) ? 0xFFFFFFFFu : float_key(hi);
     };
@@ -697,7 +704,7 @@ __global__ void __launch_bounds__(256, 6) k_coarse_recheck(const float* __restri
     // candidates: lower bound, rounded down (c_lo <= 1 - C for L2; for inner
     // product the margin c_up is subtracted from a sum rounded up), <= T
     auto lower_in = [&](float acc_j, float c2j, int cej) -> bool {
-        const float a = ldexpf(acc_j, -(qe + cej));
+        const float a = scale_pow2(acc_j, -(qe + cej));
         const float lo = ip ? __fmaf_rd(-c_up, __fadd_ru(qq, c2j), -a)
                             : __fmaf_rd(-2.0f, a, __fmul_rd(c_lo, __fadd_rd(qq, c2j)));
         return all || float_key(lo) <= T || extreme(c2j);

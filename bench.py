@@ -673,9 +673,15 @@ def served_workload(args):
     fp32_qps = 1000 / (time.perf_counter() - t)
     qb.set_tensor_filter(1)
     best = max(out, key=lambda r: r["achieved_qps"] if r["p99_ms"] <= 2.0 else 0)
+    # sustained: the highest offered rate the server keeps up with (achieved >= 98 % of offered)
+    kept = [r for r in out if r["achieved_qps"] >= 0.98 * r["offered_qps"]]
+    sus = max(kept, key=lambda r: r["achieved_qps"]) if kept else None
     print(json.dumps({
-        "metric": "served QPS at p99 <= 2 ms (5M x 128 IVF16384-PQ64x4fs + refine kf10, mixed k / nprobe / filters)",
-        "value": best["achieved_qps"] if best["p99_ms"] <= 2.0 else None, "unit": "queries/s", "n_gpus": 1,
+        "metric": "served stream: highest sustained QPS (achieved >= 98% of offered) with p50/p99 per offered rate "
+                  "(5M x 128 IVF16384-PQ64x4fs + refine kf10, mixed k / nprobe / filters)",
+        "value": sus["achieved_qps"] if sus else None, "unit": "queries/s", "n_gpus": 1,
+        "p50_ms_at_value": sus["p50_ms"] if sus else None, "p99_ms_at_value": sus["p99_ms"] if sus else None,
+        "qps_at_p99_le_2ms": best["achieved_qps"] if best["p99_ms"] <= 2.0 else None,
         "steps": len(rates), "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": f"served_{n}x{d}_nl{nlist}_m{m}_kf{kf}", "requests_per_rate": nreq,

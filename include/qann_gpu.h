@@ -165,7 +165,8 @@ int64_t qg_launch_count(void);
  *   vectors with plain codes (n x m bytes, one code per byte) and one LUT index
  *   per group of 64 vectors; the same values fast_scan_block computes
  *   (reference src/fast_scan.cpp:256-262). LUTs are nluts x m x 16 bytes,
- *   16-byte aligned.
+ *   16-byte aligned. Waits for its work; a LUT index lut_of[i] >= nluts is
+ *   caught on the device and returned as QG_INVALID_ARGUMENT.
  * qg_exact_scores_dev: out[i * nb + j] = squared L2 (ip = 0) or -(a . b) (ip = 1)
  *   in the reference's AVX2 accumulation order (reference src/distance.cpp:66-96, :138-151).
  */
@@ -188,7 +189,9 @@ int qg_exact_scores_dev(const float* a_dev, size_t na, const float* b_dev, size_
  * (about 1 million vectors at m = 64; larger n returns QG_INVALID_ARGUMENT).
  * The first call on a device looks the array up (cudaGetSymbolAddress): make
  * it before any stream capture. Calls share the array, so calls that overlap
- * on the GPU race; work is queued on `stream` and not waited for.
+ * on the GPU race. Like qg_fast_scan_dev, the call waits for its work on
+ * `stream`: a LUT index lut_of[i] >= nluts is caught on the device and
+ * returned as QG_INVALID_ARGUMENT.
  * No counterpart in the reference, which runs on the CPU only. */
 int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, const uint8_t* codes_dev,
                              const uint32_t* lut_of_dev, size_t n, uint16_t* sums_dev, void* stream);

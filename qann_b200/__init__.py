@@ -198,7 +198,9 @@ class DenseIndex:
     def add(self, data, ids=None, *, metadata=None):
         """Adds an (n, dim) array; returns the vectors' int64 ids."""
         if metadata is not None:
-            raise NotImplementedError("metadata columns are not supported by qann_b200; filter with allowed=")
+            raise NotImplementedError(
+                "metadata columns are not kept by qann_b200: keep them beside the index, evaluate filters on the "
+                "host into a slot bitmap and query with batch_query_bitmap(query, k, words), or pass allowed= ids")
         x = _f32_rows(data, self.dim())
         n = x.shape[0]
         idarr = None if ids is None else _ids(ids)
@@ -225,7 +227,10 @@ class DenseIndex:
         """k nearest neighbours of each row: (ids int64 (nq, k), distances
         float32 (nq, k)), padded with -1 / inf."""
         if where is not None:
-            raise NotImplementedError("where= needs metadata evaluation; pass the matching ids as allowed=")
+            raise NotImplementedError(
+                "where= needs the metadata store, which qann_b200 does not keep: evaluate the expression on the "
+                "host into a slot bitmap (uint64 words, bit s allows slot s) and call batch_query_bitmap(query, k, "
+                "words), or pass the matching ids as allowed=")
         q = _f32_rows(query, self.dim(), "query")
         k = int(k)
         if k < 0:

@@ -24,6 +24,11 @@
 // stream capture. All calls share the one array and it keeps the last call's
 // contents: each call rewrites every part it reads, and calls that overlap on
 // the GPU (on different streams, or from different host threads) race on it.
+//
+// Every LUT index lut_of[sb] is checked against nluts on the device; the call
+// waits for its work (as qg_fast_scan_dev does) and returns
+// QG_INVALID_ARGUMENT naming the first superblock whose index is out of
+// range. Inputs are refused before any product of their sizes can wrap.
 #include "../../include/qann_gpu.h"
 
 #include "qg_device.cuh"
@@ -63,29 +68,40 @@ unsigned char* scratch_on_current_device() {
 
 inline size_t round256(size_t b) { return (b + 255) & ~size_t{255}; }
 
-// one list of n vectors: offsets {0, n}, superblock offsets {0, nsb}, size n
+// one list of n vectors: offsets {0, n}, superblock offsets {0, nsb}, size n;
+// word 5 receives the first superblock whose LUT index is out of range
 __global__ void k_noalloc_header(uint32_t* meta, uint32_t n, uint32_t nsb) {
     meta[0] = 0;
     meta[1] = n;
     meta[2] = 0;
     meta[3] = nsb;
     meta[4] = n;
+    meta[5] = 0xFFFFFFFFu;
 }
 
 // octet per superblock, the LUT rows of lut_of[sb] copied to shared memory
-// with zero rows up to m_pad
+// with zero rows up to m_pad; an index of nluts or more is not followed (the
+// superblock's sums stay unwritten and the lowest such superblock goes to *bad)
 __global__ void k_noalloc_sums(const uint4* __restrict__ codes, size_t nsb, const uint4* __restrict__ luts, int m,
-                               int m_pad, const uint32_t* __restrict__ lut_of, size_t n, uint16_t* __restrict__ sums) {
+                               int m_pad, const uint32_t* __restrict__ lut_of, size_t nluts, size_t n,
+                               uint16_t* __restrict__ sums, uint32_t* bad) {
     extern __shared__ uint4 lut_sm[];
     const int oct = threadIdx.x >> 3, r = threadIdx.x & 7;
     const size_t sb = static_cast<size_t>(blockIdx.x) * (blockDim.x >> 3) + oct;
     uint4* L = lut_sm + static_cast<size_t>(oct) * m_pad;
-    if (sb < nsb) {
-        const uint4* src = luts + static_cast<size_t>(lut_of[sb]) * m;
-        for (int row = r; row < m_pad; row += 8) L[row] = row < m ? src[row] : make_uint4(0, 0, 0, 0);
+    bool skip = sb >= nsb;
+    if (!skip) {
+        const uint32_t li = lut_of[sb];   // the same for the octet's 8 lanes
+        if (li >= nluts) {
+            if (r == 0) atomicMin(bad, static_cast<uint32_t>(sb));
+            skip = true;
+        } else {
+            const uint4* src = luts + static_cast<size_t>(li) * m;
+            for (int row = r; row < m_pad; row += 8) L[row] = row < m ? src[row] : make_uint4(0, 0, 0, 0);
+        }
     }
     __syncwarp();
-    if (sb >= nsb) return;
+    if (skip) return;
     uint32_t s[8];
     octet_sums(codes + sb * static_cast<size_t>(2 * m_pad), L, m_pad, r, s);
 #pragma unroll
@@ -106,14 +122,22 @@ extern "C" int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, si
         require(m >= 1 && m <= kFsMaxSubspaces, "m must be in [1, 1024]");
         require(nluts >= 1, "need at least one LUT");
         require(reinterpret_cast<uintptr_t>(lut_dev) % 16 == 0, "the LUT buffer must be 16-byte aligned");
+        if (n > kNoAllocScratchBytes)   // at least a byte of scratch per vector; also keeps n in 32 bits
+            throw Error(kInvalidArgument, "qg_fast_scan_noalloc_dev: " + std::to_string(n) +
+                                              " vectors exceed the static scratch (use qg_fast_scan_dev)");
         const int mi = static_cast<int>(m), m_pad = (mi + 3) & ~3;
         const size_t nsb = ceil_div(n, kSuperBlock);
-        const size_t need = kHeaderBytes + round256(nsb * sizeof(uint32_t)) + nsb * 32 * static_cast<size_t>(m_pad);
-        if (need > kNoAllocScratchBytes)
+        // bound the superblock count before any product, so that no size
+        // wraps around: each superblock takes 32 * m_pad bytes of the scratch
+        const size_t max_sb = kNoAllocScratchBytes / (32 * static_cast<size_t>(m_pad));
+        const size_t need = nsb > max_sb ? 0
+                                         : kHeaderBytes + round256(nsb * sizeof(uint32_t)) +
+                                               nsb * 32 * static_cast<size_t>(m_pad);
+        if (nsb > max_sb || need > kNoAllocScratchBytes)
             throw Error(kInvalidArgument, "qg_fast_scan_noalloc_dev: " + std::to_string(n) + " vectors of m = " +
-                                              std::to_string(m) + " need " + std::to_string(need) +
-                                              " bytes of scratch; the static scratch holds " +
-                                              std::to_string(kNoAllocScratchBytes) + " (use qg_fast_scan_dev)");
+                                              std::to_string(m) + " need more than the " +
+                                              std::to_string(kNoAllocScratchBytes) +
+                                              " bytes of the static scratch (use qg_fast_scan_dev)");
         if (n == 0) return QG_OK;
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         unsigned char* base = scratch_on_current_device();
@@ -130,8 +154,15 @@ extern "C" int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, si
         if (smem > 48 * 1024)
             allow_large_smem<k_noalloc_sums>();
         k_noalloc_sums<<<static_cast<unsigned>(ceil_div(nsb, opb)), 8 * opb, smem, st>>>(
-            packed, nsb, reinterpret_cast<const uint4*>(lut_dev), mi, m_pad, lut_of_dev, n, sums_dev);
+            packed, nsb, reinterpret_cast<const uint4*>(lut_dev), mi, m_pad, lut_of_dev, nluts, n, sums_dev,
+            meta + 5);
         QG_LAUNCH_CHECK();
+        // the index check's verdict, copied to a host word (no allocation)
+        uint32_t bad = 0;
+        QG_CUDA(cudaMemcpyAsync(&bad, meta + 5, sizeof(bad), cudaMemcpyDeviceToHost, st));
+        QG_CUDA(cudaStreamSynchronize(st));
+        require(bad == 0xFFFFFFFFu,
+                "lut_of[" + std::to_string(bad) + "] is not below nluts = " + std::to_string(nluts));
         return QG_OK;
     } catch (const Error& e) {
         set_last_error(e.what());

@@ -42,6 +42,7 @@ struct ServeRequest {
     double t_arrive = 0, t_done = 0;
     size_t bytes = 0;
     int status = -1;   // -1 while pending, then a QG_* status
+    bool claimed = false;   // a thread is waiting on it
     std::string err;
     std::vector<int64_t> ids;
     std::vector<float> d;
@@ -72,13 +73,17 @@ public:
         }
         cv_in_.notify_all();
         for (auto& t : workers_) t.join();
-        std::lock_guard<std::mutex> g(mu_);
+        std::unique_lock<std::mutex> lk(mu_);
         for (auto& [id, r] : reqs_)
             if (r->status < 0) {
                 r->status = QG_RUNTIME_ERROR;
                 r->err = "server stopped";
             }
         cv_out_.notify_all();
+        // threads still inside wait() hold references to mu_ and cv_out_:
+        // let every one of them take its request and leave before the
+        // members are destroyed
+        cv_out_.wait(lk, [&] { return waiters_ == 0; });
     }
 
     size_t dim() const { return idx_->dim(); }
@@ -119,14 +124,22 @@ public:
     }
 
     // Waits for a request and takes its results (k entries each).
+    // One thread waits per ticket. The request is owned by the map until
+    // then; no iterator is held across the wait, because submit() may
+    // rehash the map while this thread sleeps.
     void wait(uint64_t id, int64_t* ids, float* d, double* latency_us) {
         std::unique_lock<std::mutex> lk(mu_);
         auto it = reqs_.find(id);
         require(it != reqs_.end(), "unknown ticket");
         ServeRequest* r = it->second.get();
+        require(!r->claimed, "another thread is already waiting on this ticket");
+        r->claimed = true;
+        ++waiters_;
         cv_out_.wait(lk, [&] { return r->status >= 0; });
-        std::unique_ptr<ServeRequest> own = std::move(it->second);
-        reqs_.erase(it);
+        auto jt = reqs_.find(id);
+        std::unique_ptr<ServeRequest> own = std::move(jt->second);
+        reqs_.erase(jt);
+        if (--waiters_ == 0 && stop_) cv_out_.notify_all();
         lk.unlock();
         if (own->status != QG_OK) throw Error(own->status, own->err);
         if (ids) std::copy(own->ids.begin(), own->ids.end(), ids);
@@ -247,6 +260,7 @@ private:
     std::vector<std::shared_ptr<const SlotBits>> filters_;
     uint64_t next_ = 1;
     size_t in_flight_ = 0, peak_ = 0;
+    int waiters_ = 0;   // threads inside wait()
     int64_t completed_ = 0, batches_ = 0;
     bool stop_ = false;
     std::vector<std::thread> workers_;

@@ -52,19 +52,29 @@ void quantize_luts(const float* B, const float* C, const float* A, size_t n, siz
 }
 
 // Sums of superblocks: octet per superblock, its LUT (by lut_of[sb]) copied
-// to shared memory with zero rows up to m_pad.
+// to shared memory with zero rows up to m_pad. A LUT index of nluts or more
+// is not followed: the superblock's sums are left unwritten and the lowest
+// such superblock is recorded in *bad (which starts at 0xFFFFFFFF).
 __global__ void k_scan_sums(const uint4* __restrict__ codes, size_t nsb, const uint4* __restrict__ luts, int m,
-                            int m_pad, const uint32_t* __restrict__ lut_of, size_t n, uint16_t* __restrict__ sums) {
+                            int m_pad, const uint32_t* __restrict__ lut_of, size_t nluts, size_t n,
+                            uint16_t* __restrict__ sums, uint32_t* bad) {
     extern __shared__ uint4 lut_sm[];   // one LUT per octet of the block
     const int oct = threadIdx.x >> 3, r = threadIdx.x & 7;
     const size_t sb = static_cast<size_t>(blockIdx.x) * (blockDim.x >> 3) + oct;
     uint4* L = lut_sm + static_cast<size_t>(oct) * m_pad;
-    if (sb < nsb) {
-        const uint4* src = luts + static_cast<size_t>(lut_of[sb]) * m;
-        for (int row = r; row < m_pad; row += 8) L[row] = row < m ? src[row] : make_uint4(0, 0, 0, 0);
+    bool skip = sb >= nsb;
+    if (!skip) {
+        const uint32_t li = lut_of[sb];   // the same for the octet's 8 lanes
+        if (li >= nluts) {
+            if (r == 0) atomicMin(bad, static_cast<uint32_t>(sb));
+            skip = true;
+        } else {
+            const uint4* src = luts + static_cast<size_t>(li) * m;
+            for (int row = r; row < m_pad; row += 8) L[row] = row < m ? src[row] : make_uint4(0, 0, 0, 0);
+        }
     }
     __syncwarp();
-    if (sb >= nsb) return;
+    if (skip) return;
     uint32_t s[8];
     octet_sums(codes + sb * static_cast<size_t>(2 * m_pad), L, m_pad, r, s);
 #pragma unroll
@@ -79,17 +89,16 @@ void fast_scan_sums(const uint8_t* lut, size_t nluts, size_t m, const uint8_t* c
     require(m >= 1 && m <= kFsMaxSubspaces, "m must be in [1, 1024]");
     require(nluts >= 1, "need at least one LUT");
     require(reinterpret_cast<uintptr_t>(lut) % 16 == 0, "the LUT buffer must be 16-byte aligned");
+    require(n <= 0xFFFFFFFFu, "n must fit in 32 bits");
     if (n == 0) return;
     const int mi = static_cast<int>(m), m_pad = (mi + 3) & ~3;
     const size_t nsb = ceil_div(n, kSuperBlock);
-    // one list holding all n vectors
-    const uint32_t h_voff[2] = {0, static_cast<uint32_t>(n)};
-    const uint32_t h_sboff[2] = {0, static_cast<uint32_t>(nsb)};
-    const uint32_t h_size = static_cast<uint32_t>(n);
-    DevBuf<uint32_t> meta(5, st), sbl(nsb, st);
-    QG_CUDA(cudaMemcpyAsync(meta.get(), h_voff, 8, cudaMemcpyHostToDevice, st));
-    QG_CUDA(cudaMemcpyAsync(meta.get() + 2, h_sboff, 8, cudaMemcpyHostToDevice, st));
-    QG_CUDA(cudaMemcpyAsync(meta.get() + 4, &h_size, 4, cudaMemcpyHostToDevice, st));
+    // one list holding all n vectors; word 5 receives the first superblock
+    // whose LUT index is out of range
+    const uint32_t h_meta[6] = {0, static_cast<uint32_t>(n), 0, static_cast<uint32_t>(nsb), static_cast<uint32_t>(n),
+                                0xFFFFFFFFu};
+    DevBuf<uint32_t> meta(6, st), sbl(nsb, st);
+    QG_CUDA(cudaMemcpyAsync(meta.get(), h_meta, sizeof(h_meta), cudaMemcpyHostToDevice, st));
     QG_CUDA(cudaMemsetAsync(sbl.get(), 0, nsb * 4, st));
     DevBuf<uint4> packed(nsb * 2 * m_pad, st);
     pack_superblocks(codes, nullptr, meta.get(), meta.get() + 2, meta.get() + 4, sbl.get(), nsb, mi, m_pad, packed.get(),
@@ -100,9 +109,12 @@ void fast_scan_sums(const uint8_t* lut, size_t nluts, size_t m, const uint8_t* c
     if (smem > 48 * 1024)
         allow_large_smem<k_scan_sums>();
     k_scan_sums<<<static_cast<unsigned>(ceil_div(nsb, OPB)), 8 * OPB, smem, st>>>(
-        packed.get(), nsb, reinterpret_cast<const uint4*>(lut), mi, m_pad, lut_of, n, sums);
+        packed.get(), nsb, reinterpret_cast<const uint4*>(lut), mi, m_pad, lut_of, nluts, n, sums, meta.get() + 5);
     QG_LAUNCH_CHECK();
+    uint32_t bad = 0;
+    QG_CUDA(cudaMemcpyAsync(&bad, meta.get() + 5, 4, cudaMemcpyDeviceToHost, st));
     QG_CUDA(cudaStreamSynchronize(st));
+    require(bad == 0xFFFFFFFFu, "lut_of[" + std::to_string(bad) + "] is not below nluts = " + std::to_string(nluts));
 }
 
 } // namespace qg

@@ -11,6 +11,7 @@ copies) and ``oracle/_ref/libqann_ref.so`` (``make -C oracle``).
 """
 from __future__ import annotations
 
+import os
 import pathlib
 import shutil
 import sys
@@ -23,7 +24,7 @@ sys.path.insert(0, str(ROOT))
 from oracle import ref  # noqa: E402
 
 HERE = pathlib.Path(__file__).resolve().parent
-REF_DATA = pathlib.Path("/root/reference/tests/data")
+REF_DATA = pathlib.Path(os.environ.get("QANN_REFERENCE", "/root/reference")) / "tests" / "data"
 
 # (index file, queries file) of the reference fixtures on the dense search path
 REF_CASES = [

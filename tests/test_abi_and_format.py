@@ -124,3 +124,16 @@ def test_reference_reads_our_files(ref, golden, tmp_path):
     q = np.load(golden / "gen" / "queries.npy")
     ids, _ = r.batch_query(q, 10)
     np.testing.assert_array_equal(ids, np.load(golden / "gen" / "refine_cos_ip_ids.npy"))
+
+
+def test_where_and_metadata_point_to_the_bitmap_entry_point():
+    """where= and add(metadata=) need the reference's metadata store, which
+    this library leaves to the caller; the errors name the bitmap query that
+    takes the evaluated filter instead (no GPU needed: both are refused
+    before any device work)."""
+    import qann_b200 as qb
+    idx = qb.IVFIndex(8, 100, 2)
+    with pytest.raises(NotImplementedError, match="batch_query_bitmap"):
+        idx.batch_query(np.zeros((1, 8), np.float32), 1, where={"a": 1})
+    with pytest.raises(NotImplementedError, match="batch_query_bitmap"):
+        idx.add(np.zeros((1, 8), np.float32), metadata=[{"a": 1}])

@@ -167,3 +167,41 @@ def test_index_first_searched_by_a_server_outlives_its_workers(built):
     other = qb.load(built[1]["ivf"])
     ids, _ = other.batch_query(q, 5)
     assert (ids >= 0).all()
+
+
+def test_many_threads_submit_while_others_wait(built):
+    """Sixteen threads keep several tickets open each while the others
+    submit, so the server's request map rehashes many times while threads
+    sleep in result(); every result must still be the request's own."""
+    idx = qb.load(built[0]["ivf"])
+    ivf = idx
+    n_threads, per_thread, window = 16, 96, 6
+    q, ks, nprobes = _mix(21, n_threads * per_thread)
+    results = {}
+    errors = []
+    with qb.Server(idx, slots=3, max_batch=16) as srv:
+        def client(part):
+            try:
+                open_ = []
+                for i in range(part, n_threads * per_thread, n_threads):
+                    open_.append((i, srv.submit(q[i], int(ks[i]), nprobe=int(nprobes[i]))))
+                    if len(open_) == window:
+                        j, t = open_.pop(0)
+                        results[j] = srv.result(t)
+                for j, t in open_:
+                    results[j] = srv.result(t)
+            except Exception as e:   # reported below, on the main thread
+                errors.append(e)
+        threads = [threading.Thread(target=client, args=(p,)) for p in range(n_threads)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        st = srv.stats()
+    assert not errors, errors[:3]
+    assert len(results) == n_threads * per_thread and st["completed"] == len(results)
+    for i in range(0, len(results), 37):
+        ai, ad = _alone(idx, ivf, q[i], ks[i], nprobes[i], None)
+        ids, d, _ = results[i]
+        np.testing.assert_array_equal(ids, ai[0])
+        assert d.tobytes() == ad[0].tobytes()

@@ -49,7 +49,14 @@ def _reset_pool_high_water():
     from cuda.bindings import runtime as rt
     err, pool = rt.cudaDeviceGetDefaultMemPool(torch.cuda.current_device())
     assert err == rt.cudaError_t.cudaSuccess
-    err, = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh, rt.cuuint64_t(0))
+    from cuda.bindings import driver as drv
+    attr = rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh
+    for value in (drv.cuuint64_t(0), 0):   # the binding's value type differs between releases
+        try:
+            err, = rt.cudaMemPoolSetAttribute(pool, attr, value)
+            break
+        except TypeError:
+            continue
     assert err == rt.cudaError_t.cudaSuccess
 
 

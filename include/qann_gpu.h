@@ -222,6 +222,15 @@ int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, con
  *   per group * 10 + 1 staged / 2 dense). Results are the same under
  *   every shape. No counterpart in the reference, whose scan kernel is fixed
  *   (reference src/fast_scan.cpp:306-338).
+ * "tensor_scan": the fast-scan of large unfiltered IVF batches with per-list
+ *   L2 tables on the tensor cores, list-major: each list's vectors as one-hot
+ *   rows times the rounded LUTs of every query probing it, a tcgen05 int8 GEMM
+ *   whose integer sums equal the lookups' (reference src/fast_scan.cpp:306-338
+ *   computes them one query and block at a time). 0 = never, 1 = when the
+ *   batch probes each list from enough queries (default), 2 = whenever it
+ *   applies. Results are the same in every mode. qg_get_option also reads
+ *   "tensor_scan_calls" and "tensor_scan_redone" (queries whose candidates
+ *   overflowed and were rescanned query-major).
  * "search_graphs": 1 makes qg_search_device replay device-resident, unfiltered
  *   searches of an IVF index (or a RefineIndex over one) as CUDA graphs. The
  *   first call with a given batch size, k, nprobe, k_factor, buffers and stream

@@ -143,6 +143,25 @@ def search_graph_counts() -> dict:
     return out
 
 
+def set_tensor_scan(mode: int) -> None:
+    """The fast-scan on the tensor cores (list-major, int8 MMA over one-hot
+    codes and rounded LUTs) for large unfiltered batches with per-list L2
+    tables: 0 never, 1 when the batch is large enough to pay (default), 2
+    whenever it applies. Results are identical in every mode."""
+    check(_lib.lib.qg_set_option(b"tensor_scan", int(mode)))
+
+
+def tensor_scan_counts() -> dict:
+    """Searches that went through the tensor-core scan, and queries of them
+    redone by the query-major scan because their candidates overflowed."""
+    out = {}
+    for key in ("calls", "redone"):
+        v = C.c_int64()
+        check(_lib.lib.qg_get_option(f"tensor_scan_{key}".encode(), C.byref(v)))
+        out[key] = v.value
+    return out
+
+
 def scan_options() -> dict:
     out = {}
     for key in ("autotune", "variant", "tuned_shapes", "last_shape"):

@@ -586,6 +586,9 @@ int qg_set_option(const char* key, int64_t value) {
         } else if (k == "scan_variant") {
             require(value >= -1 && value <= 2, "scan_variant must be -1, 0, 1 or 2");
             set_scan_variant(static_cast<int>(value));
+        } else if (k == "tensor_scan") {
+            require(value >= 0 && value <= 2, "tensor_scan must be 0, 1 or 2");
+            set_tensor_scan(static_cast<int>(value));
         } else {
             throw Error(kInvalidArgument, "unknown option: " + k);
         }
@@ -617,6 +620,12 @@ int qg_get_option(const char* key, int64_t* value) {
         else if (k == "scan_variant") *value = scan_variant();
         else if (k == "scan_tuned_shapes") *value = scan_tuned_shapes();
         else if (k == "scan_last_shape") *value = scan_last_shape();
+        else if (k == "tensor_scan") *value = tensor_scan();
+        else if (k == "tensor_scan_calls" || k == "tensor_scan_redone") {
+            int64_t c = 0, r = 0;
+            tensor_scan_counts(&c, &r);
+            *value = k == "tensor_scan_calls" ? c : r;
+        }
         else throw Error(kInvalidArgument, "unknown option: " + k);
     });
 }

@@ -294,6 +294,27 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
     return d;
 }
 
+// The 16 entries of LUT rows rounded and packed: round-half-even of
+// (t - min) * scale, as nearbyint / cvtps do, through the 1.5 * 2^23 addend
+// (every value here lies in [0, 64), where float spacing at that magnitude is 1).
+// Two entries per packed FP32 instruction: each component rounds as the scalar
+// __fadd_rn / __fmul_rn does, and t - min is t + (-min) exactly.
+__device__ __forceinline__ uint4 round_row(const float* v, float mn, float scale) {
+    const float2 neg = make_float2(-mn, -mn), sc = make_float2(scale, scale);
+    const float2 magic = make_float2(12582912.0f, 12582912.0f);
+    uint32_t b[16];
+#pragma unroll
+    for (int j = 0; j < 16; j += 2) {
+        const float2 t = __fadd2_rn(__fmul2_rn(__fadd2_rn(make_float2(v[j], v[j + 1]), neg), sc), magic);
+        b[j] = __float_as_uint(t.x);
+        b[j + 1] = __float_as_uint(t.y);
+    }
+    return make_uint4(prmt(prmt(b[0], b[1], 0x0040), prmt(b[2], b[3], 0x0040), 0x5410),
+                      prmt(prmt(b[4], b[5], 0x0040), prmt(b[6], b[7], 0x0040), 0x5410),
+                      prmt(prmt(b[8], b[9], 0x0040), prmt(b[10], b[11], 0x0040), 0x5410),
+                      prmt(prmt(b[12], b[13], 0x0040), prmt(b[14], b[15], 0x0040), 0x5410));
+}
+
 // Device code layout (built from the file format's blocks by pack_superblocks, qg_index.cu):
 // a list is stored in superblocks of 64 vectors. Octet lane r (0..7) owns
 // vectors 8r..8r+7; its word for subspace s holds their codes, vector 8r+i

@@ -49,27 +49,6 @@ constexpr int kQtabStride = 20;
 constexpr int kFirstGroup = 2;   // lists in the first LUT group (at most LC)
 }
 
-// The 16 entries of LUT rows rounded and packed: round-half-even of
-// (t - min) * scale, as nearbyint / cvtps do, through the 1.5 * 2^23 addend
-// (every value here lies in [0, 64), where float spacing at that magnitude is 1).
-// Two entries per packed FP32 instruction: each component rounds as the scalar
-// __fadd_rn / __fmul_rn does, and t - min is t + (-min) exactly.
-__device__ __forceinline__ uint4 round_row(const float* v, float mn, float scale) {
-    const float2 neg = make_float2(-mn, -mn), sc = make_float2(scale, scale);
-    const float2 magic = make_float2(12582912.0f, 12582912.0f);
-    uint32_t b[16];
-#pragma unroll
-    for (int j = 0; j < 16; j += 2) {
-        const float2 t = __fadd2_rn(__fmul2_rn(__fadd2_rn(make_float2(v[j], v[j + 1]), neg), sc), magic);
-        b[j] = __float_as_uint(t.x);
-        b[j + 1] = __float_as_uint(t.y);
-    }
-    return make_uint4(prmt(prmt(b[0], b[1], 0x0040), prmt(b[2], b[3], 0x0040), 0x5410),
-                      prmt(prmt(b[4], b[5], 0x0040), prmt(b[6], b[7], 0x0040), 0x5410),
-                      prmt(prmt(b[8], b[9], 0x0040), prmt(b[10], b[11], 0x0040), 0x5410),
-                      prmt(prmt(b[12], b[13], 0x0040), prmt(b[14], b[15], 0x0040), 0x5410));
-}
-
 // LUT of one list by one warp. Same arithmetic as quantize_lut; each lane
 // forms its rows twice (for their ranges, then for rounding) rather than
 // holding them in registers across the warp-wide reductions.
@@ -899,6 +878,90 @@ static ScanShape tune_scan(const std::vector<ScanShape>& cands, const ScanArgs& 
     return best;
 }
 
+// The query-major scan (k_scan) of nq queries: probe / pterm rows of
+// `stride` entries, each query scanning its first probes_of[q] (or Pn) of
+// them, at most Pn; tables qC (mode L2) or qlut / qscale / qoffset (IP
+// modes), raw queries q (mode L2-ADC). Outputs each query's k' best keys and
+// slots, sorted.
+static void scan_query_major(const IvfView& v, const IvfSearchArgs& s, int nq, int stride, int Pn,
+                             const uint32_t* probe, const float* pterm, const float* qC, const uint4* qlut,
+                             const float* qscale, const float* qoffset, const float* q, const int* probes_of,
+                             uint64_t* out_key, uint32_t* out_slot, cudaStream_t st) {
+    const int kp = s.kp;
+    if (nq == 0) return;
+    // chunks: enough blocks to fill the GPU several times over, at most kMaxChunk probes each
+    const int sms = s.sm_count > 0 ? s.sm_count : 148;
+    const int P = Pn;
+    // (and at least kMinChunk probes a chunk, so the merge stays small for small batches)
+    int nchunks = std::clamp(static_cast<int>(ceil_div(static_cast<size_t>(4 * sms), nq)), 1,
+                             std::max(1, P / kMinChunk));
+    nchunks = std::max(nchunks, static_cast<int>(ceil_div(P, kMaxChunk)));
+    const int pch = static_cast<int>(ceil_div(P, nchunks));
+    nchunks = static_cast<int>(ceil_div(P, pch));
+    const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
+    const int qtab_len = v.mode == kModeL2 ? v.m * kQtabStride : (v.mode == kModeL2Adc ? v.dim : 0);
+    const std::vector<ScanShape> cands = scan_shapes(kp, v.m_pad, qtab_len, pch, shared_lut);
+    require(!cands.empty(), "fast-scan shared memory exceeds the B200 limit for this m / k * k_factor", kUnsupported);
+
+    const bool direct = nchunks == 1;
+    const size_t nout = static_cast<size_t>(nq) * nchunks * kp;
+    DevBuf<uint64_t> ckey;
+    DevBuf<uint32_t> cslot;
+    DevBuf<unsigned long long> qthr;
+    if (!direct) {
+        ckey.alloc(nout, st);
+        cslot.alloc(nout, st);
+        qthr.alloc(nq, st);
+    }
+    DevBuf<int> work(1, st);
+    QG_CUDA(cudaMemsetAsync(work.get(), 0, sizeof(int), st));
+    ScanArgs a{};
+    a.v = v;
+    a.q = q;
+    a.probe = probe;
+    a.pterm = pterm;
+    a.qC = qC;
+    a.qlut = qlut;
+    a.qscale = qscale;
+    a.qoffset = qoffset;
+    a.filter = s.filter;
+    a.filters = s.pq.filter;
+    a.nprobe_q = probes_of;
+    a.P = stride;
+    a.pch = pch;
+    a.nchunks = nchunks;
+    a.kp = kp;
+    a.nunits = nq * nchunks;
+    a.work = work.get();
+    a.qthr = direct ? nullptr : qthr.get();
+    a.out_key = direct ? out_key : ckey.get();
+    a.out_slot = direct ? out_slot : cslot.get();
+    a.err = s.d_err;
+    // the shape: tuned once per problem key on a search large enough to fill
+    // the GPU several times over, else the first candidate
+    const int nq_bucket = 31 - __builtin_clz(static_cast<unsigned>(std::max(1, nq)));
+    const auto key = std::make_tuple(v.mode, v.m_pad, kp, P, nq_bucket, g_force.load());
+    ScanShape shape = cands.front();
+    bool tuned = !g_autotune.load();
+    if (!tuned) {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        const auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            shape = it->second;
+            tuned = true;
+        }
+    }
+    const bool big = static_cast<long long>(nq) * P >= 4 * 148 * 256;
+    if (!tuned && cands.size() > 1 && big && !s.capture) {
+        shape = tune_scan(cands, a, v, qtab_len, st);
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        g_tuned[key] = shape;
+    }
+    g_last_shape.store(shape.nw * 1000 + shape.lc * 10 + (shape.staged ? 1 : shape.dense ? 2 : 0));
+    run_scan(shape, a, v, qtab_len, st);
+    if (!direct) merge_candidates(ckey.get(), cslot.get(), nq, nchunks, kp, out_key, out_slot, st);
+}
+
 void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st) {
     const int nq = s.nq, kp = s.kp;
     if (nq == 0) return;
@@ -962,76 +1025,50 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     }
     if (v.mode != kModeL2Adc) query_tables(v, s.q, nq, qC.get(), qlut.get(), qscale.get(), qoffset.get(), st);
 
-    // chunks: enough blocks to fill the GPU several times over, at most kMaxChunk probes each
-    const int sms = s.sm_count > 0 ? s.sm_count : 148;
-    // (and at least kMinChunk probes a chunk, so the merge stays small for small batches)
-    int nchunks = std::clamp(static_cast<int>(ceil_div(static_cast<size_t>(4 * sms), nq)), 1,
-                             std::max(1, P / kMinChunk));
-    nchunks = std::max(nchunks, static_cast<int>(ceil_div(P, kMaxChunk)));
-    const int pch = static_cast<int>(ceil_div(P, nchunks));
-    nchunks = static_cast<int>(ceil_div(P, pch));
-    const bool shared_lut = v.mode == kModeIP || v.mode == kModeCosIP;
-    const int qtab_len = v.mode == kModeL2 ? v.m * kQtabStride : (v.mode == kModeL2Adc ? v.dim : 0);
-    const std::vector<ScanShape> cands = scan_shapes(kp, v.m_pad, qtab_len, pch, shared_lut);
-    require(!cands.empty(), "fast-scan shared memory exceeds the B200 limit for this m / k * k_factor", kUnsupported);
-
-    const bool direct = nchunks == 1;
-    const size_t nout = static_cast<size_t>(nq) * nchunks * kp;
-    DevBuf<uint64_t> ckey;
-    DevBuf<uint32_t> cslot;
-    DevBuf<unsigned long long> qthr;
-    if (!direct) {
-        ckey.alloc(nout, st);
-        cslot.alloc(nout, st);
-        qthr.alloc(nq, st);
-    }
-    DevBuf<int> work(1, st);
-    QG_CUDA(cudaMemsetAsync(work.get(), 0, sizeof(int), st));
-    ScanArgs a{};
-    a.v = v;
-    a.q = s.q;
-    a.probe = probe.get();
-    a.pterm = pterm.get();
-    a.qC = qC.get();
-    a.qlut = qlut.get();
-    a.qscale = qscale.get();
-    a.qoffset = qoffset.get();
-    a.filter = s.filter;
-    a.filters = s.pq.filter;
-    a.nprobe_q = probes_of;
-    a.P = P;
-    a.pch = pch;
-    a.nchunks = nchunks;
-    a.kp = kp;
-    a.nunits = nq * nchunks;
-    a.work = work.get();
-    a.qthr = direct ? nullptr : qthr.get();
-    a.out_key = direct ? out_key : ckey.get();
-    a.out_slot = direct ? out_slot : cslot.get();
-    a.err = s.d_err;
-    // the shape: tuned once per problem key on a search large enough to fill
-    // the GPU several times over, else the first candidate
-    const int nq_bucket = 31 - __builtin_clz(static_cast<unsigned>(std::max(1, nq)));
-    const auto key = std::make_tuple(v.mode, v.m_pad, kp, P, nq_bucket, g_force.load());
-    ScanShape shape = cands.front();
-    bool tuned = !g_autotune.load();
-    if (!tuned) {
-        std::lock_guard<std::mutex> g(g_tune_mu);
-        const auto it = g_tuned.find(key);
-        if (it != g_tuned.end()) {
-            shape = it->second;
-            tuned = true;
+    const bool per_query = s.pq.k || s.pq.kp || s.pq.nprobe;
+    if (tensor_scan_applies(v, s, P, per_query)) {
+        // wave 0: the first F probes of every query, query-major; wave 1 on the tensor cores
+        const int F = tensor_scan_first(P);
+        DevBuf<int> first(nq, st);
+        fill_i32(first.get(), nq, F, st);
+        DevBuf<uint64_t> key0(static_cast<size_t>(nq) * kp, st);
+        DevBuf<uint32_t> slot0(static_cast<size_t>(nq) * kp, st);
+        scan_query_major(v, s, nq, P, F, probe.get(), pterm.get(), qC.get(), qlut.get(), qscale.get(), qoffset.get(),
+                         s.q, first.get(), key0.get(), slot0.get(), st);
+        std::vector<int> redo;
+        tensor_scan_candidates(v, nq, P, kp, probe.get(), pterm.get(), qC.get(), key0.get(), out_key, out_slot, redo,
+                               s.d_err, st);
+        if (!redo.empty()) {
+            // queries whose candidates overflowed: the query-major scan over all their probes
+            const size_t r = redo.size();
+            std::vector<uint32_t> hidx(redo.begin(), redo.end());
+            DevBuf<uint32_t> idx(r, st);
+            QG_CUDA(cudaMemcpyAsync(idx.get(), hidx.data(), r * 4, cudaMemcpyHostToDevice, st));
+            DevBuf<uint32_t> pr(r * P, st);
+            DevBuf<float> pt(r * P, st), qc(r * v.m * 16, st);
+            gather_rows(reinterpret_cast<const float*>(probe.get()), idx.get(), r, P, reinterpret_cast<float*>(pr.get()),
+                        st);
+            gather_rows(pterm.get(), idx.get(), r, P, pt.get(), st);
+            gather_rows(qC.get(), idx.get(), r, v.m * 16, qc.get(), st);
+            DevBuf<uint64_t> rk(r * kp, st);
+            DevBuf<uint32_t> rs(r * kp, st);
+            IvfSearchArgs sr = s;   // (an unfiltered batch of uniform settings, re-indexed)
+            sr.pq = PerQuery{};
+            sr.nq = static_cast<int>(r);
+            scan_query_major(v, sr, static_cast<int>(r), P, P, pr.get(), pt.get(), qc.get(), nullptr, nullptr, nullptr,
+                             nullptr, nullptr, rk.get(), rs.get(), st);
+            for (size_t j = 0; j < r; ++j) {
+                QG_CUDA(cudaMemcpyAsync(out_key + static_cast<size_t>(redo[j]) * kp, rk.get() + j * kp, kp * 8,
+                                        cudaMemcpyDeviceToDevice, st));
+                QG_CUDA(cudaMemcpyAsync(out_slot + static_cast<size_t>(redo[j]) * kp, rs.get() + j * kp, kp * 4,
+                                        cudaMemcpyDeviceToDevice, st));
+            }
+            QG_CUDA(cudaStreamSynchronize(st));   // the index buffers above outlive their copies
         }
+        return;
     }
-    const bool big = static_cast<long long>(nq) * P >= 4 * 148 * 256;
-    if (!tuned && cands.size() > 1 && big && !s.capture) {
-        shape = tune_scan(cands, a, v, qtab_len, st);
-        std::lock_guard<std::mutex> g(g_tune_mu);
-        g_tuned[key] = shape;
-    }
-    g_last_shape.store(shape.nw * 1000 + shape.lc * 10 + (shape.staged ? 1 : shape.dense ? 2 : 0));
-    run_scan(shape, a, v, qtab_len, st);
-    if (!direct) merge_candidates(ckey.get(), cslot.get(), nq, nchunks, kp, out_key, out_slot, st);
+    scan_query_major(v, s, nq, P, P, probe.get(), pterm.get(), qC.get(), qlut.get(), qscale.get(), qoffset.get(), s.q,
+                     probes_of, out_key, out_slot, st);
 }
 
 } // namespace qg

@@ -163,4 +163,20 @@ void finalize_ivf(const uint64_t* key, const uint32_t* slot, int nq, int kp, int
 void refine_candidates(const float* q, int nq, int dim, const float* rows, const uint64_t* key, const uint32_t* slot,
                        int kp, int k, bool ip, const int64_t* labels, bool cosine, int64_t* out_ids, float* out_d,
                        cudaStream_t st, const int* kp_q = nullptr, const int* k_q = nullptr);
+// The fast-scan on the tensor cores (qg_tscan.cu), list-major, for large
+// unfiltered batches of per-list L2 tables. Mode 0 never, 1 when the batch
+// is large enough to pay (default), 2 whenever it applies.
+void set_tensor_scan(int mode);
+int tensor_scan();
+void tensor_scan_counts(int64_t* calls, int64_t* redone);
+bool tensor_scan_applies(const IvfView& v, const IvfSearchArgs& s, int P, bool per_query);
+int tensor_scan_first(int P);   // probes per query that wave 0 scans query-major
+void fill_i32(int* a, int n, int value, cudaStream_t st);
+// Wave 1 and the final cut: key0 holds wave 0's k' best keys per query
+// (sorted, from its first tensor_scan_first(P) probes). Fills out_key /
+// out_slot except for the queries listed in redo_q, whose candidates
+// overflowed (the caller redoes them).
+void tensor_scan_candidates(const IvfView& v, int nq, int P, int kp, const uint32_t* probe, const float* pterm,
+                            const float* qC, const uint64_t* key0, uint64_t* out_key, uint32_t* out_slot,
+                            std::vector<int>& redo_q, int* d_err, cudaStream_t st);
 } // namespace qg

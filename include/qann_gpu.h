@@ -143,6 +143,16 @@ int qg_ivf_centroids(qg_index* h, float* out_centroids);
  */
 int qg_save(qg_index* h, const char* path);
 int qg_load(const char* path, qg_index** out, int* kind);
+/* qg_load_mapped replaces qann.load(path, mmap=True) (reference
+ * src/index_factory.cpp:120-141, include/vecengine/vector_store.hpp:21-110):
+ * the file is mapped read-only and a RefineIndex's raw rows (format 10 and
+ * later, 64 KB aligned in the file) stay in the mapping, read in place by the
+ * re-rank through host-mapped memory rather than copied into HBM, so rows
+ * larger than the GPU's memory can be served. An add or compact copies them
+ * into memory first; qg_get(h, "rows_mapped") reads 2 while the re-rank reads
+ * the mapping, 1 while the rows are mapped but copied to HBM (the driver
+ * refused the registration), 0 otherwise. Results are the same either way. */
+int qg_load_mapped(const char* path, qg_index** out, int* kind);
 
 /* --- profiling (no counterpart in the reference, which times sections with
  * compile-time timers, reference src/profile.hpp) --------------------------------

@@ -400,6 +400,9 @@ class RefineIndex(DenseIndex):
         self._base = base
 
     k_factor = property(lambda self: self._get("k_factor"), lambda self, v: self._set("k_factor", v))
+    # 2: raw rows read in place from the mapped file by the re-rank; 1: mapped
+    # but copied to GPU memory; 0: in memory (see load(mmap=True))
+    rows_mapped = property(lambda self: self._get("rows_mapped"))
     mapped = property(lambda self: False)
 
     @property
@@ -415,11 +418,15 @@ class RefineIndex(DenseIndex):
 
 def load(path, *, mmap=False):
     """Loads an index saved by qann or by this package (.qann format 1..13);
-    returns FlatIndex, IVFIndex or RefineIndex. mmap is accepted for API
-    compatibility: the device holds the whole index either way."""
+    returns FlatIndex, IVFIndex or RefineIndex. With mmap=True the file is
+    mapped read-only and a RefineIndex's raw rows stay in it: the re-rank
+    reads them in place over the host link instead of from a copy in GPU
+    memory, so rows larger than the GPU's memory can be served (an add or
+    compact copies them into memory first). Results are the same either way."""
     h = C.c_void_p()
     kind = C.c_int()
-    check(_lib.lib.qg_load(os.fspath(path).encode(), C.byref(h), C.byref(kind)))
+    fn = _lib.lib.qg_load_mapped if mmap else _lib.lib.qg_load
+    check(fn(os.fspath(path).encode(), C.byref(h), C.byref(kind)))
     if kind.value == 1:
         return FlatIndex(0, _handle=h.value)
     if kind.value == 2:

@@ -46,6 +46,7 @@ _SIGS = {
     "qg_ivf_centroids": (C.c_int, [_vp, _vp]),
     "qg_save": (C.c_int, [_vp, C.c_char_p]),
     "qg_load": (C.c_int, [C.c_char_p, _H, C.POINTER(C.c_int)]),
+    "qg_load_mapped": (C.c_int, [C.c_char_p, _H, C.POINTER(C.c_int)]),
     "qg_profile_enable": (C.c_int, [C.c_int]),
     "qg_profile_reset": (C.c_int, []),
     "qg_profile_get": (C.c_int, [C.c_char_p, C.POINTER(C.c_double), C.POINTER(_i64)]),

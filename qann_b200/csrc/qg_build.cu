@@ -211,6 +211,7 @@ void add(IndexObj& idx, const float* x, size_t n, const int64_t* ids, int64_t* o
     } else {
         auto& o = static_cast<RefineObj&>(idx);
         o.map.check(n, ids);
+        o.materialize();   // rows of a mapped file move to memory before they change
         DevBuf<float> dev;
         std::vector<float> rows = prepare_rows(o.metric(), x, n, dim, dev, st);
         if (o.base->kind == Kind::IVF) {
@@ -281,6 +282,7 @@ static size_t compact_obj(IndexObj& idx, bool keep_ids) {
     auto& o = static_cast<RefineObj&>(idx);
     if (o.map.deleted_count() && !o.meta.empty())
         throw Error(kUnsupported, "compacting an index with metadata columns is not supported by this library");
+    if (o.map.deleted_count()) o.materialize();   // (before the slot count changes)
     auto remap = o.map.compact(keep_ids);
     if (remap.empty()) return 0;
     {

@@ -355,6 +355,16 @@ int qg_get(qg_index* h, const char* key, int64_t* value) {
         } else if (k == "base_kind") {
             require(o.kind == Kind::Refine, "not a RefineIndex");
             *value = static_cast<int64_t>(static_cast<RefineObj&>(o).base->kind);
+        } else if (k == "rows_mapped") {
+            // 1: the raw rows are read in place from the mapped file (load with
+            // mmap); 2: and the re-rank reads them there through host-mapped
+            // memory rather than from a copy in HBM
+            if (o.kind != Kind::Refine) {
+                *value = 0;
+            } else {
+                const auto& r = static_cast<RefineObj&>(o);
+                *value = r.mapped ? (r.dev.ext ? 2 : 1) : 0;
+            }
         } else {
             require(o.kind == Kind::IVF, "unknown property '" + k + "' for this index");
             const IVFObj& v = static_cast<IVFObj&>(o);
@@ -467,7 +477,7 @@ int qg_save(qg_index* h, const char* path) {
             }
             w.pod<uint64_t>(r.map.slots() * r.dim());
             w.pad(64 * 1024);
-            w.bytes(r.data.data(), r.data.size() * sizeof(float));
+            w.bytes(r.rows_host(), r.rows_len() * sizeof(float));
             r.map.save(w);
             r.meta.write(w);
         }
@@ -475,10 +485,12 @@ int qg_save(qg_index* h, const char* path) {
     });
 }
 
-int qg_load(const char* path, qg_index** out, int* kind) {
-    return guarded([&] {
-        const std::vector<char> bytes = read_file(path);
-        Reader r{bytes.data(), bytes.size()};
+namespace {
+
+// Reads an index from `bytes` (the whole file); with `file`, a RefineIndex
+// keeps its raw rows inside that mapping.
+void load_from(const char* data, size_t size, std::shared_ptr<const MappedFile> file, qg_index** out, int* kind) {
+        Reader r{data, size};
         uint32_t version = 0;
         const Kind k = read_header(r, &version);
         std::shared_ptr<IndexObj> o;
@@ -491,7 +503,7 @@ int qg_load(const char* path, qg_index** out, int* kind) {
             f->model = std::move(*FlatModel::load_body(r, version));
             o = f;
         } else {
-            auto m = RefineModel::load_body(r, version);
+            auto m = RefineModel::load_body(r, version, file != nullptr);
             auto ro = std::make_shared<RefineObj>();
             if (m->base_kind == Kind::IVF) {
                 auto v = std::make_shared<IVFObj>();
@@ -507,11 +519,32 @@ int qg_load(const char* path, qg_index** out, int* kind) {
             ro->data = std::move(m->data);
             ro->map = std::move(m->idmap);
             ro->meta = std::move(m->meta);
+            if (m->mapped) {
+                ro->mapped = m->mapped;
+                ro->file = file;
+            }
             o = ro;
         }
         if (r.pos != r.size) throw Error(kRuntimeError, "corrupt file: unexpected data after the index");
         *kind = static_cast<int>(k);
         *out = wrap(o);
+}
+
+} // namespace
+
+int qg_load(const char* path, qg_index** out, int* kind) {
+    return guarded([&] {
+        require(path && out && kind, "null argument");
+        const std::vector<char> bytes = read_file(path);
+        load_from(bytes.data(), bytes.size(), nullptr, out, kind);
+    });
+}
+
+int qg_load_mapped(const char* path, qg_index** out, int* kind) {
+    return guarded([&] {
+        require(path && out && kind, "null argument");
+        std::shared_ptr<const MappedFile> f = MappedFile::open(path);
+        load_from(f->data, f->size, f, out, kind);
     });
 }
 

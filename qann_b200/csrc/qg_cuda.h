@@ -77,8 +77,11 @@ public:
         cudaEventRecord(a_, st_);
         armed_ = true;
     }
-    ~KernelTimer() {
+    ~KernelTimer() { stop(); }
+    // ends the bracket early (a section of several launches)
+    void stop() {
         if (!armed_) return;
+        armed_ = false;
         cudaEventRecord(b_, st_);
         std::lock_guard<std::mutex> g(profiler().mu);
         profiler().pending.push_back({name_, a_, b_});

@@ -15,6 +15,11 @@
 #include <numeric>
 #include <unordered_set>
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 namespace qg {
 
 [[noreturn]] void Reader::throw_corrupt(const std::string& what) { throw Error(kRuntimeError, "corrupt file: " + what); }
@@ -277,6 +282,32 @@ Kind read_header(Reader& r, uint32_t* version) {
                                       " (HNSW, sparse, hybrid or codebook) is not on the GPU search path");
     *version = v;
     return static_cast<Kind>(k);
+}
+
+std::shared_ptr<const MappedFile> MappedFile::open(const std::string& path) {
+    const int fd = ::open(path.c_str(), O_RDONLY | O_CLOEXEC);
+    if (fd < 0) throw Error(kRuntimeError, "cannot open " + path + " for reading");
+    struct stat sb {};
+    if (::fstat(fd, &sb) != 0) {
+        ::close(fd);
+        throw Error(kRuntimeError, "cannot stat " + path);
+    }
+    auto f = std::make_shared<MappedFile>();
+    f->size = static_cast<size_t>(sb.st_size);
+    if (f->size) {
+        void* p = ::mmap(nullptr, f->size, PROT_READ, MAP_SHARED, fd, 0);
+        if (p == MAP_FAILED) {
+            ::close(fd);
+            throw Error(kRuntimeError, "cannot map " + path);
+        }
+        f->data = static_cast<const char*>(p);
+    }
+    ::close(fd);   // the mapping keeps the file
+    return f;
+}
+
+MappedFile::~MappedFile() {
+    if (data) ::munmap(const_cast<char*>(data), size);
 }
 
 std::vector<char> read_file(const std::string& path) {
@@ -554,7 +585,7 @@ void RefineModel::save_body(Writer& w) const {
     meta.write(w);
 }
 
-std::unique_ptr<RefineModel> RefineModel::load_body(Reader& r, uint32_t version) {
+std::unique_ptr<RefineModel> RefineModel::load_body(Reader& r, uint32_t version, bool map_rows) {
     auto m = std::make_unique<RefineModel>();
     m->k_factor = r.pod<uint64_t>();
     const auto count = r.pod<uint64_t>();
@@ -583,8 +614,14 @@ std::unique_ptr<RefineModel> RefineModel::load_body(Reader& r, uint32_t version)
     const auto len = r.pod<uint64_t>();
     if (len != count * dim) Reader::throw_corrupt("unexpected number of vectors");
     if (version >= 10) r.pad(kRowAlign);
-    m->data.resize(len);
-    r.bytes(m->data.data(), len * sizeof(float));
+    if (map_rows && version >= 10 && reinterpret_cast<uintptr_t>(r.data + r.pos) % 16 == 0) {
+        r.need(len * sizeof(float));
+        m->mapped = reinterpret_cast<const float*>(r.data + r.pos);
+        r.pos += len * sizeof(float);
+    } else {
+        m->data.resize(len);
+        r.bytes(m->data.data(), len * sizeof(float));
+    }
     if (version >= 2) m->idmap = IdMap::load(r, count, version);
     else m->idmap.add(count, nullptr);
     if (version >= 9) m->meta = MetaBlob::read(r, count);

@@ -180,16 +180,28 @@ struct FlatModel {
     static std::unique_ptr<FlatModel> load_body(Reader& r, uint32_t version);
 };
 
+// A whole file mapped read-only (reference include/vecengine/vector_store.hpp:21-49),
+// unmapped when the last owner lets go.
+struct MappedFile {
+    const char* data = nullptr;
+    size_t size = 0;
+    static std::shared_ptr<const MappedFile> open(const std::string& path);
+    ~MappedFile();
+};
+
 struct RefineModel {
     uint64_t k_factor = 10;
     Kind base_kind = Kind::IVF;
     std::shared_ptr<IVFModel> ivf;     // one of ivf / flat is the base
     std::shared_ptr<FlatModel> flat;
     std::vector<float> data;           // raw rows, slots * dim
+    const float* mapped = nullptr;     // load_body(map_rows): the rows inside the reader's buffer instead of `data`
     IdMap idmap;
     MetaBlob meta;
     void save_body(Writer& w) const;
-    static std::unique_ptr<RefineModel> load_body(Reader& r, uint32_t version);
+    // map_rows: leave the raw rows in the reader's buffer (format 10 and
+    // later keep them 64 KB aligned there) and point `mapped` at them
+    static std::unique_ptr<RefineModel> load_body(Reader& r, uint32_t version, bool map_rows = false);
 };
 
 void write_header(Writer& w, Kind kind);

@@ -7,6 +7,8 @@
 #include <numeric>
 #include <thread>
 
+#include <unistd.h>
+
 namespace qg {
 
 // ---------------------------------------------------------------------------
@@ -247,11 +249,63 @@ void ensure_device(FlatObj& o, cudaStream_t) {
     ++o.dev_gen;
 }
 
+void RefineObj::release_mapping() {
+    if (registered) {
+        cudaHostUnregister(registered);
+        (void)cudaGetLastError();
+        registered = nullptr;
+    }
+    dev.ext = nullptr;
+    mapped = nullptr;
+    file.reset();
+}
+
+void RefineObj::materialize() {
+    if (!mapped) return;
+    data.assign(mapped, mapped + rows_len());
+    release_mapping();
+    dev_dirty = true;
+}
+
+// Mapped rows read in place: the file's pages holding them registered with
+// CUDA (mapped, read-only), so device loads reach them over the host link.
+// Returns the device address of the rows, or null when the registration is
+// refused (the rows are then copied into HBM as usual).
+static const float* map_rows_for_device(RefineObj& o) {
+    const size_t page = static_cast<size_t>(sysconf(_SC_PAGESIZE));
+    const uintptr_t b = reinterpret_cast<uintptr_t>(o.mapped) & ~(page - 1);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(o.mapped + o.rows_len()) + page - 1) & ~(page - 1);
+    if (e <= b) return nullptr;
+    if (!o.registered) {
+        if (cudaHostRegister(reinterpret_cast<void*>(b), e - b,
+                             cudaHostRegisterMapped | cudaHostRegisterPortable | cudaHostRegisterReadOnly) !=
+            cudaSuccess) {
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        o.registered = reinterpret_cast<void*>(b);
+    }
+    void* d = nullptr;
+    if (cudaHostGetDevicePointer(&d, const_cast<float*>(o.mapped), 0) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    return static_cast<const float*>(d);
+}
+
 void ensure_device(RefineObj& o, cudaStream_t st) {
     {
         std::lock_guard<std::mutex> g(o.dev_mu);
         if (o.dev_dirty) {
-            upload_rows(o.dev, o.data, o.map, resident_stream());
+            const float* ext = o.mapped && o.rows_len() ? map_rows_for_device(o) : nullptr;
+            if (ext) {
+                upload_rows(o.dev, {}, o.map, resident_stream());
+                o.dev.ext = ext;
+            } else if (o.mapped) {
+                upload_rows(o.dev, std::vector<float>(o.mapped, o.mapped + o.rows_len()), o.map, resident_stream());
+            } else {
+                upload_rows(o.dev, o.data, o.map, resident_stream());
+            }
             o.dev_dirty = false;
             ++o.dev_gen;
         }

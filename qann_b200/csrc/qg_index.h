@@ -31,8 +31,10 @@ struct DeviceIVF {
 // Device rows of a FlatIndex or of a RefineIndex's raw vectors.
 struct DeviceRows {
     DevBuf<float> rows;
+    const float* ext = nullptr;        // rows read in place from host memory (a mapped file), or null
     DevBuf<int64_t> labels;
     DevBuf<uint64_t> deleted;
+    const float* ptr() const { return ext ? ext : rows.get(); }
 };
 
 // A captured device-resident search (search_graph).
@@ -101,14 +103,26 @@ struct FlatObj : IndexObj {
 struct RefineObj : IndexObj {
     std::shared_ptr<IndexObj> base;
     uint64_t k_factor = 10;
-    std::vector<float> data;   // slots * dim raw rows
+    std::vector<float> data;   // slots * dim raw rows (empty while mapped)
+    // load(mmap=True) (reference include/vecengine/vector_store.hpp:50-110):
+    // the rows stay in the mapped file, and the re-rank reads them there
+    // through host-mapped memory instead of from an HBM copy, until the index
+    // changes (add, compact), which copies them into `data` first.
+    std::shared_ptr<const MappedFile> file;
+    const float* mapped = nullptr;
+    void* registered = nullptr;   // the page range registered with CUDA for mapped reads
     IdMap map;
     MetaBlob meta;
     DeviceRows dev;
     RefineObj() : IndexObj(Kind::Refine) {}
     ~RefineObj() override {
+        release_mapping();
         if (base) base->wrapped = false;
     }
+    const float* rows_host() const { return mapped ? mapped : data.data(); }
+    size_t rows_len() const { return mapped ? map.slots() * dim() : data.size(); }
+    void materialize();      // mapped rows into `data`, the mapping released
+    void release_mapping();
     size_t dim() const override { return base->dim(); }
     Metric metric() const override { return base->metric(); }
     IdMap& idmap() override { return map; }

@@ -316,7 +316,7 @@ static void refine_direct(RefineObj& o, const Prepared& p, const SearchRequest& 
     DevBuf<uint32_t> ds(n, st);
     QG_CUDA(cudaMemcpyAsync(ds.get(), slots.data(), n * 4, cudaMemcpyHostToDevice, st));
     DevBuf<float> rows(n * dim, st);
-    gather_rows(o.dev.rows.get(), ds.get(), n, dim, rows.get(), st);
+    gather_rows(o.dev.ptr(), ds.get(), n, dim, rows.get(), st);
     DevBuf<uint64_t> ck(r.nq * r.k, st);
     DevBuf<uint32_t> cs(r.nq * r.k, st);
     flat_candidates(p.q.get(), r.nq, rows.get(), n, dim, ip, r.k, nullptr, nullptr, ck.get(), cs.get(), st);
@@ -452,7 +452,7 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
         flat_candidates(p.q.get(), r.nq, b.dev.rows.get(), b.model.idmap.slots(), dim, ip, kp, p.filter.get(),
                         r.filter ? nullptr : b.dev.deleted.get(), ck.get(), cs.get(), st);
     }
-    refine_candidates(p.q.get(), static_cast<int>(r.nq), dim, o.dev.rows.get(), ck.get(), cs.get(), static_cast<int>(kp),
+    refine_candidates(p.q.get(), static_cast<int>(r.nq), dim, o.dev.ptr(), ck.get(), cs.get(), static_cast<int>(kp),
                       static_cast<int>(r.k), ip, o.dev.labels.get(), cosine, out_ids, out_d, st);
     finish(p);
 }
@@ -519,7 +519,7 @@ void finish_candidates(IndexObj& idx, const float* q_dev, size_t nq, size_t k, c
     prepare(idx, r, p, st);
     if (idx.kind == Kind::Refine) {
         auto& o = static_cast<RefineObj&>(idx);
-        refine_candidates(p.q.get(), static_cast<int>(nq), static_cast<int>(idx.dim()), o.dev.rows.get(), key, slot,
+        refine_candidates(p.q.get(), static_cast<int>(nq), static_cast<int>(idx.dim()), o.dev.ptr(), key, slot,
                           static_cast<int>(kp), static_cast<int>(k), ip, o.dev.labels.get(), cosine, out_ids, out_d, st);
     } else {
         finalize_ivf(key, slot, static_cast<int>(nq), static_cast<int>(kp), static_cast<int>(k), b.dev.labels.get(),
@@ -767,7 +767,7 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
         DevBuf<float> od(nb * kmax_g, st);
         const bool cosine = idx.metric() == Metric::Cosine, ip = idx.metric() == Metric::InnerProduct;
         if (ref)
-            refine_candidates(p.q.get(), static_cast<int>(nb), static_cast<int>(dim), ref->dev.rows.get(), ck.get(), cs.get(),
+            refine_candidates(p.q.get(), static_cast<int>(nb), static_cast<int>(dim), ref->dev.ptr(), ck.get(), cs.get(),
                               kpmax, static_cast<int>(kmax_g), ip, ref->dev.labels.get(), cosine, oid.get(), od.get(), st,
                               a.pq.kp, a.pq.k);
         else

@@ -532,6 +532,7 @@ void tensor_scan_candidates(const IvfView& v, int nq, int P, int kp, const uint3
     const size_t npairs = static_cast<size_t>(nq) * span;
     require(npairs < (size_t{1} << 31), "too many (query, list) pairs for the tensor-core scan", kUnsupported);
     DevBuf<uint32_t> push(static_cast<size_t>(nq) * P, st);
+    KernelTimer prep_timer("tscan_prep", st);   // push offsets .. unit table
     k_push_offsets<<<static_cast<unsigned>(ceil_div(static_cast<size_t>(nq) * 32, 256)), 256, 0, st>>>(
         probe, v.list_size, nq, P, push.get());
     QG_LAUNCH_CHECK();
@@ -563,6 +564,7 @@ void tensor_scan_candidates(const IvfView& v, int nq, int P, int kp, const uint3
     k_unit_table<<<static_cast<unsigned>(ceil_div(v.nlist, 256)), 256, 0, st>>>(off.get(), ubase.get(), v.nlist,
                                                                                 units.get(), nunits.get());
     QG_LAUNCH_CHECK();
+    prep_timer.stop();
 
     const uint32_t cap = tscan_cap(kp);
     DevBuf<uint64_t> cand(static_cast<size_t>(nq) * cap, st);

@@ -137,3 +137,20 @@ def test_where_and_metadata_point_to_the_bitmap_entry_point():
         idx.batch_query(np.zeros((1, 8), np.float32), 1, where={"a": 1})
     with pytest.raises(NotImplementedError, match="batch_query_bitmap"):
         idx.add(np.zeros((1, 8), np.float32), metadata=[{"a": 1}])
+
+
+def test_mapped_load_keeps_rows_in_the_file_and_saves_the_same_bytes(golden, tmp_path):
+    """load(mmap=True) leaves a RefineIndex's raw rows in the mapped file
+    (format 10 and later) and writes them back unchanged; no GPU needed."""
+    src = golden / "gen" / "refine_l2.qann"
+    idx = qb.load(src, mmap=True)
+    assert idx.rows_mapped == 1   # mapped; the device copy is made at the first search
+    out = tmp_path / "again.qann"
+    idx.save(out)
+    assert filecmp.cmp(src, out, shallow=False)
+    plain = qb.load(src)
+    assert plain.rows_mapped == 0
+    ivf = qb.load(golden / "gen" / "ivf_l2.qann", mmap=True)   # not a RefineIndex: read as usual
+    out2 = tmp_path / "ivf.qann"
+    ivf.save(out2)
+    assert filecmp.cmp(golden / "gen" / "ivf_l2.qann", out2, shallow=False)

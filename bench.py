@@ -716,11 +716,29 @@ def served_workload(args):
         filt = np.where(arng.random(nreq) < 0.3, arng.integers(0, len(fids), nreq), -1)
         fid = np.array([fids[f] if f >= 0 else -1 for f in filt], np.int32)
         srv.replay(q[:2000], ks[:2000], np.zeros(2000), nprobes=npb[:2000], filter_ids=fid[:2000])   # warm-up
-        for rate in rates:
+        from qann_b200 import profiling
+        by_kind = None
+        for ri, rate in enumerate(rates):
             arrivals = np.cumsum(arng.exponential(1.0 / rate, size=nreq))
+            if ri == 0:   # kernel time per batch at the lowest rate, where batches are smallest
+                profiling.enable(True)
+                profiling.reset()
+                b0 = srv.stats()["batches"]
             t = time.perf_counter()
             ids, _, lat = srv.replay(q, ks, arrivals, nprobes=npb, filter_ids=fid)
             wall = time.perf_counter() - t
+            if ri == 0:
+                nb = max(1, srv.stats()["batches"] - b0)
+                kernel_per_batch = {kk: round(v[0] / nb, 4) for kk in profiling.KERNELS
+                                    for v in [profiling.get(kk)] if v[1]}
+                profiling.enable(False)
+                # latency by request kind at this rate
+                kind = np.where(filt >= 0, np.where(ks == 100, "filtered_k100", "filtered_k10"),
+                                np.where(ks == 100, "k100", "k10"))
+                by_kind = {kd: {"requests": int((kind == kd).sum()),
+                                "p50_ms": round(float(np.median(lat[kind == kd])) * 1e3, 3),
+                                "p99_ms": round(float(np.quantile(lat[kind == kd], 0.99)) * 1e3, 3)}
+                           for kd in sorted(set(kind.tolist()))}
             lat_ms = np.sort(lat) * 1e3
             span = float(np.max(arrivals + lat))   # arrival schedule start to the last result
             out.append({"offered_qps": rate, "achieved_qps": round(nreq / span, 1),
@@ -759,6 +777,7 @@ def served_workload(args):
                    "k": [10, 100], "nprobe": "log-uniform 8..256", "filtered": 0.3, "selectivity": [0.01, 0.5],
                    "slots": 4, "max_batch": 256},
         "rates": out, "results_equal_solo_searches": same, "mean_batch": round(st["completed"] / st["batches"], 1),
+        "at_lowest_rate": {"kernel_ms_per_batch": kernel_per_batch, "latency_by_kind": by_kind},
         "plain_fp32_gpu_flat_qps": round(fp32_qps, 1), "batch_scan": batch}))
     return 0
 
@@ -961,6 +980,7 @@ def main():
     profiling.enable(True)
     profiling.reset()
     coarse0 = qb.tensor_filter_counts()
+    tscan0 = qb.tensor_scan_counts()
     launches0 = profiling.launch_count()
     step_ms = []
     barrier()
@@ -983,8 +1003,17 @@ def main():
               "queries": cq, "redone_exactly": coarse1["coarse_redone"] - coarse0["coarse_redone"],
               "lists_rescored_per_query": round((coarse1["coarse_candidates"] - coarse0["coarse_candidates"]) / cq, 1)
               if cq else None}
-    scan_ms, scan_n = profiling.get("scan")
+    tscan1 = qb.tensor_scan_counts()
+    # the fast-scan stage per step: the query-major kernel (all probes, or the
+    # first wave of the tensor-core path) and the tensor-core wave with its
+    # preparation and final cut
+    stage = {kname: profiling.get(kname) for kname in ("scan", "tscan_prep", "tscan", "tscan_final")}
+    scan_ms = sum(v[0] for v in stage.values())
+    scan_n = args.steps
     kernel_ms = {kname: profiling.get(kname) for kname in profiling.KERNELS}
+    tensor_scan = {"used": tscan1["calls"] > tscan0["calls"], "searches": tscan1["calls"] - tscan0["calls"],
+                   "queries_redone": tscan1["redone"] - tscan0["redone"],
+                   "ms_per_step": {kname: round(v[0] / args.steps, 4) for kname, v in stage.items() if v[1]}}
     total_ms = float(sum(step_ms))
     if dist is not None:
         t = torch.tensor([total_ms], device=dev)
@@ -1056,8 +1085,12 @@ def main():
         "rel_err_vs_fp64": fp64_error(base, queries, ids_h, d_h),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
-                     "kernel": "k_scan", "algorithmic_bytes_per_launch": alg_bytes,
-                     "launch_ms": round(per_launch_ms, 4)},
+                     "kernel": "fast-scan stage (k_scan; with the tensor-core path k_scan on the first 16 probes "
+                               "+ k_tscan on the rest)" if tensor_scan["used"] else "k_scan",
+                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": round(per_launch_ms, 4),
+                     "note": "algorithmic bytes count every probed list's codes; the codes (33 MB) stay in L2 and "
+                             "lists that cannot beat a query's bound are skipped, so this is not a DRAM rate"},
+        "tensor_scan": tensor_scan,
         "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": nq * cfg["d"] * 4,
                 "d2h_bytes_per_step": nq * k * 12, "timing": "host wall clock around the blocking batch_query"},
         "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "served": serving,

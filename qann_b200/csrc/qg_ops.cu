@@ -719,9 +719,11 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
                 any_filter = true;
                 h[kMin * nb + j] = static_cast<int>(min_probes_for(M, np, m.filter->count));
                 h[kWanted * nb + j] = static_cast<int>(std::min(kp, m.filter->count));
-                auto it = std::find(distinct.begin(), distinct.end(), m.filter);
-                which[j] = static_cast<size_t>(it - distinct.begin());
-                if (it == distinct.end()) distinct.push_back(m.filter);
+                if (!m.filter_dev) {   // (registered filters are on the device already)
+                    auto it = std::find(distinct.begin(), distinct.end(), m.filter);
+                    which[j] = static_cast<size_t>(it - distinct.begin());
+                    if (it == distinct.end()) distinct.push_back(m.filter);
+                }
             }
             npmax = std::max(npmax, static_cast<int>(np));
             kpmax = std::max(kpmax, static_cast<int>(kp));
@@ -732,15 +734,19 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
         DevBuf<uint64_t> fwords;
         DevBuf<const uint64_t*> fptr;
         if (any_filter) {
-            const size_t words = distinct.front()->words.size();
-            for (const SlotBits* f : distinct) require(f->words.size() == words, "filters of one batch differ in size");
-            fwords.alloc(words * distinct.size(), st);
+            const size_t words = (idx.idmap().slots() + 63) / 64;
+            for (size_t j = 0; j < nb; ++j)   // (a filter registered before the index grew no longer covers it)
+                if (const SlotBits* f = qs[batch[j]].filter)
+                    require(f->words.size() == words, "a filter does not cover the index's slots");
+            if (!distinct.empty()) fwords.alloc(words * distinct.size(), st);
             for (size_t d = 0; d < distinct.size(); ++d)
                 QG_CUDA(cudaMemcpyAsync(fwords.get() + d * words, distinct[d]->words.data(), words * 8,
                                         cudaMemcpyHostToDevice, st));
             std::vector<const uint64_t*> ptr(nb, nullptr);
-            for (size_t j = 0; j < nb; ++j)
+            for (size_t j = 0; j < nb; ++j) {
                 if (which[j] != SIZE_MAX) ptr[j] = fwords.get() + which[j] * words;
+                else if (qs[batch[j]].filter) ptr[j] = qs[batch[j]].filter_dev;
+            }
             fptr.alloc(nb, st);
             QG_CUDA(cudaMemcpyAsync(fptr.get(), ptr.data(), nb * sizeof(void*), cudaMemcpyHostToDevice, st));
         }

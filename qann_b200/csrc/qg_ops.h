@@ -56,6 +56,8 @@ struct MixedQuery {
     int k = 10;                      // results wanted, >= 1
     int nprobe = 0;                  // <= 0: the index's nprobe
     const SlotBits* filter = nullptr;   // allowed slots, or null
+    const uint64_t* filter_dev = nullptr;   // the same bitmap already on the device (a server's
+                                            // registered filter), or null: uploaded per batch
 };
 
 // A batch of queries that differ in k, nprobe and filter (host rows q, nq x

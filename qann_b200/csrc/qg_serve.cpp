@@ -14,6 +14,7 @@
 // request's results are the ones it gets searched alone.
 #include "../../include/qann_gpu.h"
 
+#include "qg_index.h"
 #include "qg_ops.h"
 
 #include <algorithm>
@@ -90,18 +91,31 @@ public:
     size_t nlist() const { return nlist_; }
     IndexObj& index() { return *idx_; }
 
+    // A registered filter is uploaded once, here, and its device copy serves
+    // every batch that uses it (without a usable device, batches upload the
+    // bitmap themselves, as for unregistered filters).
     int add_filter(std::shared_ptr<const SlotBits> f) {
+        auto reg = std::make_shared<Registered>();
+        try {
+            cudaStream_t st = resident_stream();
+            reg->dev.alloc(std::max<size_t>(1, f->words.size()), st);
+            QG_CUDA(cudaMemcpyAsync(reg->dev.get(), f->words.data(), f->words.size() * sizeof(uint64_t),
+                                    cudaMemcpyHostToDevice, st));
+            QG_CUDA(cudaStreamSynchronize(st));
+        } catch (const Error&) {
+            reg->dev = DevBuf<uint64_t>{};
+            (void)cudaGetLastError();
+        }
+        reg->bits = std::move(f);
         std::lock_guard<std::mutex> g(mu_);
-        filters_.push_back(std::move(f));
+        filters_.push_back(std::move(reg));
         return static_cast<int>(filters_.size() - 1);
     }
-    std::shared_ptr<const SlotBits> filter(int id) {
-        std::lock_guard<std::mutex> g(mu_);
-        require(id >= 0 && static_cast<size_t>(id) < filters_.size(), "unknown filter id");
-        return filters_[id];
-    }
+    std::shared_ptr<const SlotBits> filter(int id) { return registered(id)->bits; }
+    const uint64_t* filter_dev(int id) { return registered(id)->dev.get(); }
 
-    uint64_t submit(const float* q, int k, int nprobe, std::shared_ptr<const SlotBits> f, double t_arrive) {
+    uint64_t submit(const float* q, int k, int nprobe, std::shared_ptr<const SlotBits> f, double t_arrive,
+                    const uint64_t* f_dev = nullptr) {
         require(k >= 1, "k must be at least 1");
         require(nprobe <= 0 || nlist_ == 0 || static_cast<size_t>(nprobe) <= nlist_, "nprobe must be <= nlist");
         const size_t d = dim();
@@ -113,6 +127,7 @@ public:
         r->mq.nprobe = nprobe;
         r->filter = std::move(f);
         r->mq.filter = r->filter.get();
+        r->mq.filter_dev = r->filter ? f_dev : nullptr;
         r->t_arrive = t_arrive;
         r->bytes = footprint(*r);
         std::lock_guard<std::mutex> g(mu_);
@@ -155,6 +170,16 @@ public:
     }
 
 private:
+    struct Registered {
+        std::shared_ptr<const SlotBits> bits;
+        DevBuf<uint64_t> dev;
+    };
+    std::shared_ptr<Registered> registered(int id) {
+        std::lock_guard<std::mutex> g(mu_);
+        require(id >= 0 && static_cast<size_t>(id) < filters_.size(), "unknown filter id");
+        return filters_[id];
+    }
+
     // Device bytes one request adds to a batch: query copies, the coarse
     // scores (every list ranked when filtered), probe lists and terms, the
     // query's tables, candidate lists per probe chunk and after the merge,
@@ -165,7 +190,7 @@ private:
         const size_t kp = static_cast<size_t>(r.mq.k) * k_factor_;
         size_t b = 3 * d * 4 + nlist_ * 4 + np * 12 + m_ * 16 * 4 + 256;
         b += kp * 12 * (2 + (np + 15) / 16) + static_cast<size_t>(r.mq.k) * 12;
-        if (r.filter) b += nlist_ * 12 + r.filter->words.size() * 8;
+        if (r.filter) b += nlist_ * 12 + (r.mq.filter_dev ? 0 : r.filter->words.size() * 8);
         return b;
     }
 
@@ -257,7 +282,7 @@ private:
     std::condition_variable cv_in_, cv_out_;
     std::deque<uint64_t> queue_;
     std::unordered_map<uint64_t, std::unique_ptr<ServeRequest>> reqs_;
-    std::vector<std::shared_ptr<const SlotBits>> filters_;
+    std::vector<std::shared_ptr<Registered>> filters_;
     uint64_t next_ = 1;
     size_t in_flight_ = 0, peak_ = 0;
     int waiters_ = 0;   // threads inside wait()
@@ -334,10 +359,13 @@ int qg_server_submit(qg_server* s, const float* q, size_t k, int nprobe, const i
         if (allowed) {
             std::shared_lock<std::shared_mutex> lk(v.index().mu);
             f = std::make_shared<SlotBits>(v.index().idmap().filter({allowed, n_allowed}));
-        } else if (filter_id >= 0) {
-            f = v.filter(filter_id);
         }
-        *ticket = v.submit(q, static_cast<int>(k), nprobe, std::move(f), now_us());
+        const uint64_t* f_dev = nullptr;
+        if (!allowed && filter_id >= 0) {
+            f = v.filter(filter_id);
+            f_dev = v.filter_dev(filter_id);
+        }
+        *ticket = v.submit(q, static_cast<int>(k), nprobe, std::move(f), now_us(), f_dev);
     });
 }
 
@@ -354,8 +382,12 @@ int qg_server_replay(qg_server* s, const float* q, size_t nq, const int32_t* k, 
         const size_t d = v.dim();
         for (size_t i = 0; i < nq; ++i) require(k[i] >= 1 && static_cast<size_t>(k[i]) <= kmax, "k out of range");
         std::vector<std::shared_ptr<const SlotBits>> fs(nq);
+        std::vector<const uint64_t*> fdev(nq, nullptr);
         for (size_t i = 0; i < nq; ++i)
-            if (filter_id && filter_id[i] >= 0) fs[i] = v.filter(filter_id[i]);
+            if (filter_id && filter_id[i] >= 0) {
+                fs[i] = v.filter(filter_id[i]);
+                fdev[i] = v.filter_dev(filter_id[i]);
+            }
         std::vector<uint64_t> tickets(nq);
         // open loop: request i enters at t0 + arrival_us[i] whatever the state
         // of the others; its latency runs from that moment to its results
@@ -365,7 +397,7 @@ int qg_server_replay(qg_server* s, const float* q, size_t nq, const int32_t* k, 
             for (double t = now_us(); t < due; t = now_us()) {
                 if (due - t > 300.0) std::this_thread::sleep_for(std::chrono::microseconds(static_cast<int64_t>(due - t - 200.0)));
             }
-            tickets[i] = v.submit(q + i * d, k[i], nprobe ? nprobe[i] : 0, fs[i], due);
+            tickets[i] = v.submit(q + i * d, k[i], nprobe ? nprobe[i] : 0, fs[i], due, fdev[i]);
         }
         std::vector<int64_t> ids(kmax);
         std::vector<float> dd(kmax);

@@ -904,6 +904,8 @@ def main():
     ap.add_argument("--no-served", action="store_true", help="skip the continuous-batching server measurement")
     ap.add_argument("--nprobe", type=int, default=0, help="use this nprobe instead of the recall sweep (profiling)")
     ap.add_argument("--kf", type=int, default=0, help="use this k_factor instead of the recall sweep (profiling)")
+    ap.add_argument("--tensor-scan", type=int, default=1, choices=[0, 1, 2],
+                    help="fast-scan on the tensor cores: 0 never, 1 when it pays (default), 2 whenever it applies")
     ap.add_argument("--scan-shape", default="auto", choices=["auto", "global", "staged", "dense"],
                     help="fast-scan kernel shape: autotuned (default) or fixed (profiling)")
     ap.add_argument("--workload", default="angular", choices=["angular", "small", "flat", "train", "served"],
@@ -939,6 +941,7 @@ def main():
 
     if args.scan_shape != "auto":
         qb.set_scan_options(autotune=False, variant={"global": 0, "staged": 1, "dense": 2}[args.scan_shape])
+    qb.set_tensor_scan(args.tensor_scan)
     base = mixture(cfg, 0, cfg["n"])
     queries = mixture(cfg, 1 + rank, cfg["nq"])
     index, path = build_or_load(cfg, base, rank, world, barrier)
@@ -1013,6 +1016,9 @@ def main():
     kernel_ms = {kname: profiling.get(kname) for kname in profiling.KERNELS}
     tensor_scan = {"used": tscan1["calls"] > tscan0["calls"], "searches": tscan1["calls"] - tscan0["calls"],
                    "queries_redone": tscan1["redone"] - tscan0["redone"],
+                   "work_per_search": {kk: round((tscan1[kk] - tscan0[kk]) / max(1, tscan1["calls"] - tscan0["calls"]))
+                                       for kk in ("pairs", "pairs_kept", "units", "tiles", "luts_live",
+                                                  "luts_hopeless", "candidates")},
                    "ms_per_step": {kname: round(v[0] / args.steps, 4) for kname, v in stage.items() if v[1]}}
     total_ms = float(sum(step_ms))
     if dist is not None:

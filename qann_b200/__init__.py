@@ -159,6 +159,10 @@ def tensor_scan_counts() -> dict:
         v = C.c_int64()
         check(_lib.lib.qg_get_option(f"tensor_scan_{key}".encode(), C.byref(v)))
         out[key] = v.value
+    for key in ("units", "tiles", "luts_live", "luts_hopeless", "candidates", "pairs", "pairs_kept"):
+        v = C.c_int64()
+        check(_lib.lib.qg_get_option(f"tensor_scan_stat_{key}".encode(), C.byref(v)))
+        out[key] = v.value
     return out
 
 

@@ -654,6 +654,10 @@ int qg_get_option(const char* key, int64_t* value) {
         else if (k == "scan_tuned_shapes") *value = scan_tuned_shapes();
         else if (k == "scan_last_shape") *value = scan_last_shape();
         else if (k == "tensor_scan") *value = tensor_scan();
+        else if (k == "mapped_rows_error") *value = mapped_rows_error();
+        else if (k.rfind("tensor_scan_stat_", 0) == 0) {
+            require(tensor_scan_stat(k.substr(17), value), "unknown option: " + k);
+        }
         else if (k == "tensor_scan_calls" || k == "tensor_scan_redone") {
             int64_t c = 0, r = 0;
             tensor_scan_counts(&c, &r);

@@ -293,6 +293,7 @@ std::shared_ptr<const MappedFile> MappedFile::open(const std::string& path) {
         throw Error(kRuntimeError, "cannot stat " + path);
     }
     auto f = std::make_shared<MappedFile>();
+    f->path = path;
     f->size = static_cast<size_t>(sb.st_size);
     if (f->size) {
         void* p = ::mmap(nullptr, f->size, PROT_READ, MAP_SHARED, fd, 0);

@@ -185,6 +185,7 @@ struct FlatModel {
 struct MappedFile {
     const char* data = nullptr;
     size_t size = 0;
+    std::string path;
     static std::shared_ptr<const MappedFile> open(const std::string& path);
     ~MappedFile();
 };

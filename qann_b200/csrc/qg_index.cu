@@ -4,9 +4,12 @@
 #include "qg_ops.h"
 
 #include <algorithm>
+#include <atomic>
 #include <numeric>
 #include <thread>
 
+#include <fcntl.h>
+#include <sys/mman.h>
 #include <unistd.h>
 
 namespace qg {
@@ -255,6 +258,12 @@ void RefineObj::release_mapping() {
         (void)cudaGetLastError();
         registered = nullptr;
     }
+    if (priv) {
+        ::munmap(priv, priv_len);
+        priv = nullptr;
+        priv_len = 0;
+    }
+    dev_src = nullptr;
     dev.ext = nullptr;
     mapped = nullptr;
     file.reset();
@@ -268,25 +277,57 @@ void RefineObj::materialize() {
 }
 
 // Mapped rows read in place: the file's pages holding them registered with
-// CUDA (mapped, read-only), so device loads reach them over the host link.
-// Returns the device address of the rows, or null when the registration is
-// refused (the rows are then copied into HBM as usual).
+// CUDA as mapped host memory, so device loads reach them over the host link.
+// First the shared read-only mapping itself (read-only registration); where
+// the platform refuses that, a private writable view of the same file pages
+// (never written; pinning it copies the pages into host memory, still not
+// GPU memory). Returns the device address of the rows, or null when both are
+// refused (the rows are then copied into HBM as usual; the refusals are kept
+// in g_mapped_rows_error).
+static std::atomic<int> g_mapped_rows_error{0};
+int mapped_rows_error() { return g_mapped_rows_error.load(); }
+
 static const float* map_rows_for_device(RefineObj& o) {
     const size_t page = static_cast<size_t>(sysconf(_SC_PAGESIZE));
     const uintptr_t b = reinterpret_cast<uintptr_t>(o.mapped) & ~(page - 1);
     const uintptr_t e = (reinterpret_cast<uintptr_t>(o.mapped + o.rows_len()) + page - 1) & ~(page - 1);
-    if (e <= b) return nullptr;
+    if (e <= b || !o.file) return nullptr;
     if (!o.registered) {
-        if (cudaHostRegister(reinterpret_cast<void*>(b), e - b,
-                             cudaHostRegisterMapped | cudaHostRegisterPortable | cudaHostRegisterReadOnly) !=
-            cudaSuccess) {
+        const cudaError_t e1 = cudaHostRegister(reinterpret_cast<void*>(b), e - b,
+                                                cudaHostRegisterMapped | cudaHostRegisterPortable |
+                                                    cudaHostRegisterReadOnly);
+        if (e1 == cudaSuccess) {
+            o.registered = reinterpret_cast<void*>(b);
+            o.dev_src = o.mapped;
+        } else {
             (void)cudaGetLastError();
-            return nullptr;
+            const size_t off = b - reinterpret_cast<uintptr_t>(o.file->data);   // page aligned: the map starts the file
+            const int fd = ::open(o.file->path.c_str(), O_RDONLY | O_CLOEXEC);
+            void* p = fd >= 0 ? ::mmap(nullptr, e - b, PROT_READ | PROT_WRITE, MAP_PRIVATE, fd, static_cast<off_t>(off))
+                              : MAP_FAILED;
+            if (fd >= 0) ::close(fd);
+            cudaError_t e2 = cudaErrorUnknown;
+            if (p != MAP_FAILED) {
+                e2 = cudaHostRegister(p, e - b, cudaHostRegisterMapped | cudaHostRegisterPortable);
+                if (e2 == cudaSuccess) {
+                    o.priv = p;
+                    o.priv_len = e - b;
+                    o.registered = p;
+                    o.dev_src = reinterpret_cast<const float*>(static_cast<char*>(p) +
+                                                               (reinterpret_cast<uintptr_t>(o.mapped) - b));
+                } else {
+                    (void)cudaGetLastError();
+                    ::munmap(p, e - b);
+                }
+            }
+            if (!o.registered) {
+                g_mapped_rows_error.store(static_cast<int>(e1) * 1000 + static_cast<int>(e2));
+                return nullptr;
+            }
         }
-        o.registered = reinterpret_cast<void*>(b);
     }
     void* d = nullptr;
-    if (cudaHostGetDevicePointer(&d, const_cast<float*>(o.mapped), 0) != cudaSuccess) {
+    if (cudaHostGetDevicePointer(&d, const_cast<float*>(o.dev_src), 0) != cudaSuccess) {
         (void)cudaGetLastError();
         return nullptr;
     }

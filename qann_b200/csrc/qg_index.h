@@ -111,6 +111,9 @@ struct RefineObj : IndexObj {
     std::shared_ptr<const MappedFile> file;
     const float* mapped = nullptr;
     void* registered = nullptr;   // the page range registered with CUDA for mapped reads
+    void* priv = nullptr;         // a private view of the rows' pages, when the shared one cannot be registered
+    size_t priv_len = 0;
+    const float* dev_src = nullptr;   // the registered copy of the rows' first element
     IdMap map;
     MetaBlob meta;
     DeviceRows dev;
@@ -128,6 +131,10 @@ struct RefineObj : IndexObj {
     IdMap& idmap() override { return map; }
     const IdMap& idmap() const override { return map; }
 };
+
+// The last refused registration of mapped rows (two cudaError_t codes:
+// read-only shared view * 1000 + private view), 0 if none.
+int mapped_rows_error();
 
 // The library's own stream on the current device (never destroyed).
 cudaStream_t resident_stream();

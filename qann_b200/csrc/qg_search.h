@@ -7,6 +7,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 namespace qg {
@@ -169,6 +170,8 @@ void refine_candidates(const float* q, int nq, int dim, const float* rows, const
 void set_tensor_scan(int mode);
 int tensor_scan();
 void tensor_scan_counts(int64_t* calls, int64_t* redone);
+// work counters: "units", "tiles", "luts_live", "luts_hopeless", "candidates", "pairs", "pairs_kept"
+bool tensor_scan_stat(const std::string& name, int64_t* value);
 bool tensor_scan_applies(const IvfView& v, const IvfSearchArgs& s, int P, bool per_query);
 int tensor_scan_first(int P);   // probes per query that wave 0 scans query-major
 void fill_i32(int* a, int n, int value, cudaStream_t st);

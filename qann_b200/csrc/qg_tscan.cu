@@ -76,7 +76,14 @@ struct TScanArgs {
     uint32_t* ccount;          // nq
     uint32_t cap;
     int* err;                  // [2]: a tensor-core wait ran out
+    unsigned long long* stats; // kTsStats counters of this search
 };
+
+// Work counters of the tensor-core scan (summed over searches, for tuning):
+// units, (unit, vector tile) steps, LUTs rounded, LUTs skipped as hopeless,
+// candidate keys appended, wave-1 pairs, pairs left after the prefilter.
+enum { kStUnits, kStTiles, kStLutLive, kStLutDead, kStCand, kStPairs, kStPairsKept, kTsStats };
+std::atomic<long long> g_tscan_stat[kTsStats];
 
 // Candidate keys a query may collect in wave 1 before it is redone by the
 // query-major kernel.
@@ -158,6 +165,7 @@ __global__ void __launch_bounds__(kTsThreads, 1) k_tscan(TScanArgs a) {
         const int unit = s_unit;
         if (unit < 0) break;
         const uint32_t l = a.units[3 * unit], first = a.units[3 * unit + 1], cnt = a.units[3 * unit + 2];
+        if (tid == 0) atomicAdd(a.stats + kStUnits, 1ull);
         for (int j = tid; j < kTsQ; j += kTsThreads) {
             if (j < static_cast<int>(cnt)) {
                 const uint32_t pair = a.members[first + j];
@@ -198,19 +206,29 @@ __global__ void __launch_bounds__(kTsThreads, 1) k_tscan(TScanArgs a) {
                     for (int e = 0; e < 16; ++e) o[e] = __fadd_rn(o[e], A);
                 }
             };
+            // each lane holds its rows (lane, lane + 32; m <= 64) between the range
+            // pass and the rounding pass
+            float ta[16], tb[16];
+            const int ra = lane, rb = lane + 32;
             float widest = 0.0f;
-            float t16[16];
-            for (int r = lane; r < m; r += 32) {
-                row(r, t16);
-                float lo = t16[0], hi = t16[0];
+            auto ranges = [&](int r, const float* t) {
+                float lo = t[0], hi = t[0];
 #pragma unroll
                 for (int e = 1; e < 16; ++e) {
-                    lo = fminf(lo, t16[e]);
-                    hi = fmaxf(hi, t16[e]);
+                    lo = fminf(lo, t[e]);
+                    hi = fmaxf(hi, t[e]);
                 }
                 rmin[r] = lo;
                 const float w = __fsub_rn(hi, lo);
                 widest = widest < w ? w : widest;
+            };
+            if (ra < m) {
+                row(ra, ta);
+                ranges(ra, ta);
+            }
+            if (rb < m) {
+                row(rb, tb);
+                ranges(rb, tb);
             }
             widest = warp_max(widest);
             __syncwarp();
@@ -224,19 +242,15 @@ __global__ void __launch_bounds__(kTsThreads, 1) k_tscan(TScanArgs a) {
             // a list none of whose sums can reach under the bound: no LUT, no candidates
             const bool live = thr_hi == 0xFFFFFFFFu || float_key(fs_dist0(scale, offset)) <= thr_hi;
             if (live) {
-                for (int r = lane; r < m8; r += 32) {
-                    uint4 w = make_uint4(0, 0, 0, 0);
-                    if (r < m) {
-                        row(r, t16);
-                        w = round_row(t16, rmin[r], scale);
-                    }
-                    *reinterpret_cast<uint4*>(sB + sw_chunk(kTsQ, j, r)) = w;
-                }
+                const uint4 z = make_uint4(0, 0, 0, 0);
+                if (ra < m8) *reinterpret_cast<uint4*>(sB + sw_chunk(kTsQ, j, ra)) = ra < m ? round_row(ta, rmin[ra], scale) : z;
+                if (rb < m8) *reinterpret_cast<uint4*>(sB + sw_chunk(kTsQ, j, rb)) = rb < m ? round_row(tb, rmin[rb], scale) : z;
             }
             if (lane == 0) {
                 s_scale[j] = scale;
                 s_offset[j] = offset;
                 s_smax[j] = live ? sum_limit_fast(thr_hi, scale, offset) : -1;
+                atomicAdd(a.stats + (live ? kStLutLive : kStLutDead), 1ull);
             }
             __syncwarp();
         }
@@ -269,6 +283,7 @@ __global__ void __launch_bounds__(kTsThreads, 1) k_tscan(TScanArgs a) {
             fence_proxy_async_smem();
             __syncthreads();
             if (tid == 0) {
+                atomicAdd(a.stats + kStTiles, 1ull);
                 tc_fence_after();
                 const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
                 const int ksteps = K / 32;
@@ -315,7 +330,10 @@ __global__ void __launch_bounds__(kTsThreads, 1) k_tscan(TScanArgs a) {
                     const uint32_t q = s_q[col];
                     const int lead = __ffs(mask) - 1;
                     uint32_t at = 0;
-                    if (lane == lead) at = atomicAdd(a.ccount + q, static_cast<uint32_t>(__popc(mask)));
+                    if (lane == lead) {
+                        at = atomicAdd(a.ccount + q, static_cast<uint32_t>(__popc(mask)));
+                        atomicAdd(a.stats + kStCand, static_cast<unsigned long long>(__popc(mask)));
+                    }
                     at = __shfl_sync(0xffffffffu, at, lead) + __popc(mask & below);
                     if (pass && at < a.cap) a.cand[static_cast<size_t>(q) * a.cap + at] = key;
                 }
@@ -502,6 +520,17 @@ void tensor_scan_counts(int64_t* calls, int64_t* redone) {
     if (redone) *redone = g_tscan_redone.load();
 }
 
+bool tensor_scan_stat(const std::string& name, int64_t* value) {
+    static const char* names[kTsStats] = {"units", "tiles", "luts_live", "luts_hopeless", "candidates", "pairs",
+                                          "pairs_kept"};
+    for (int i = 0; i < kTsStats; ++i)
+        if (name == names[i]) {
+            *value = g_tscan_stat[i].load();
+            return true;
+        }
+    return false;
+}
+
 int tensor_scan_first(int P) { return std::min(P, kTsFirst); }
 
 static int kp_of(const IvfSearchArgs& s) { return s.kp; }
@@ -572,6 +601,8 @@ void tensor_scan_candidates(const IvfView& v, int nq, int P, int kp, const uint3
     QG_CUDA(cudaMemsetAsync(ccount.get(), 0, nq * sizeof(uint32_t), st));
     DevBuf<int> work(1, st);
     QG_CUDA(cudaMemsetAsync(work.get(), 0, sizeof(int), st));
+    DevBuf<unsigned long long> stats(kTsStats, st);
+    QG_CUDA(cudaMemsetAsync(stats.get(), 0, kTsStats * sizeof(unsigned long long), st));
     TScanArgs a{};
     a.v = v;
     a.P = P;
@@ -590,6 +621,7 @@ void tensor_scan_candidates(const IvfView& v, int nq, int P, int kp, const uint3
     a.ccount = ccount.get();
     a.cap = cap;
     a.err = d_err;
+    a.stats = stats.get();
     const size_t smem = tscan_smem(m, m8);
     allow_large_smem<k_tscan>();
     {
@@ -608,9 +640,15 @@ void tensor_scan_candidates(const IvfView& v, int nq, int P, int kp, const uint3
                                                                      redo.get(), nredo.get());
         QG_LAUNCH_CHECK();
     }
-    uint32_t nr = 0;
+    uint32_t nr = 0, kept = 0;
+    unsigned long long hs[kTsStats] = {};
     QG_CUDA(cudaMemcpyAsync(&nr, nredo.get(), sizeof(nr), cudaMemcpyDeviceToHost, st));
+    QG_CUDA(cudaMemcpyAsync(&kept, off.get() + v.nlist, sizeof(kept), cudaMemcpyDeviceToHost, st));
+    QG_CUDA(cudaMemcpyAsync(hs, stats.get(), sizeof(hs), cudaMemcpyDeviceToHost, st));
     QG_CUDA(cudaStreamSynchronize(st));
+    hs[kStPairs] = npairs;
+    hs[kStPairsKept] = kept;
+    for (int i = 0; i < kTsStats; ++i) g_tscan_stat[i].fetch_add(static_cast<long long>(hs[i]));
     if (nr) {
         std::vector<uint32_t> h(nr);
         QG_CUDA(cudaMemcpyAsync(h.data(), redo.get(), nr * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));

@@ -236,9 +236,10 @@ int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, con
  *   L2 tables on the tensor cores, list-major: each list's vectors as one-hot
  *   rows times the rounded LUTs of every query probing it, a tcgen05 int8 GEMM
  *   whose integer sums equal the lookups' (reference src/fast_scan.cpp:306-338
- *   computes them one query and block at a time). 0 = never, 1 = when the
- *   batch probes each list from enough queries (default), 2 = whenever it
- *   applies. Results are the same in every mode. qg_get_option also reads
+ *   computes them one query and block at a time). 0 = never, 1 = when it
+ *   pays (default; on the workloads measured so far it is slower than the
+ *   query-major kernel, so 1 does not pick it), 2 = whenever it applies.
+ *   Results are the same in every mode. qg_get_option also reads
  *   "tensor_scan_calls" and "tensor_scan_redone" (queries whose candidates
  *   overflowed and were rescanned query-major).
  * "search_graphs": 1 makes qg_search_device replay device-resident, unfiltered

@@ -146,8 +146,9 @@ def search_graph_counts() -> dict:
 def set_tensor_scan(mode: int) -> None:
     """The fast-scan on the tensor cores (list-major, int8 MMA over one-hot
     codes and rounded LUTs) for large unfiltered batches with per-list L2
-    tables: 0 never, 1 when the batch is large enough to pay (default), 2
-    whenever it applies. Results are identical in every mode."""
+    tables: 0 never, 1 when it pays (default; slower than the query-major
+    kernel on the workloads measured so far, so not picked), 2 whenever it
+    applies. Results are identical in every mode."""
     check(_lib.lib.qg_set_option(b"tensor_scan", int(mode)))
 
 

@@ -272,8 +272,11 @@ __global__ void k_ema_move(float* __restrict__ pos, float* __restrict__ mass, co
     const uint32_t cnt = off[j + 1] - off[j];
     if (cnt == 0) return;
     const float nj = __uint2float_rn(cnt);
-    const float grown = __fmaf_rn(alpha, nj, replace ? 0.0f : mass[j]);
-    const float w = __fdiv_rn(__fmul_rn(alpha, nj), grown);
+    // the reference's build rounds alpha * n_j once and uses it for both the
+    // new mass (a plain add, not fused) and the weight
+    const float an = __fmul_rn(alpha, nj);
+    const float grown = __fadd_rn(an, replace ? 0.0f : mass[j]);
+    const float w = __fdiv_rn(an, grown);
     float* c = pos + static_cast<size_t>(j) * d;
     const float* s = sums + static_cast<size_t>(j) * d;
     for (int l = lane; l < d; l += 32) {

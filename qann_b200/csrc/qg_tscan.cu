@@ -543,9 +543,13 @@ bool tensor_scan_applies(const IvfView& v, const IvfSearchArgs& s, int P, bool p
     const int F = std::min(P, kTsFirst);
     if (P - F < 1) return false;
     if (static_cast<size_t>(kp_of(s) + tscan_cap(kp_of(s))) * 8 > 200 * 1024) return false;   // the final cut's keys
-    if (mode == 2) return true;
-    // enough (query, list) pairs per list to fill the GEMM's query dimension
-    return static_cast<long long>(s.nq) * (P - F) >= 48ll * v.nlist;
+    // Mode 1 ("when it pays") does not pick it: measured on the 1.2M x 100
+    // angular batch (10,000 queries, nprobe 256, k' 200) the two waves took
+    // 9.8 ms against 6.9 ms for the query-major kernel alone. Per (unit, tile)
+    // step the one-hot expansion, the barriers around the MMA and the L2
+    // latency of the LUT inputs keep 16 warps at 28 % issue, and 56 % of the
+    // LUTs turn out hopeless only after their range pass.
+    return mode == 2;
 }
 
 // Wave 0 by `scan0` (the query-major kernel on each query's first F probes,

@@ -162,17 +162,21 @@ __device__ __forceinline__ bool col_allowed(const uint64_t* allow, const uint64_
 
 // Columns refused by allow / deny (bitmaps over col_base + column, either may
 // be null) rank last and come out as column 0xFFFFFFFF with score +inf.
-__global__ void __launch_bounds__(256) k_select_rows(const float* __restrict__ scores, size_t ld, int ncols, int P,
-                                                     const uint64_t* __restrict__ allow, const uint64_t* __restrict__ deny,
-                                                     size_t col_base, bool eq0, uint32_t* __restrict__ out_col,
-                                                     float* __restrict__ out_score) {
+// With `staged`, the row's keys are formed once into shared memory (ncols
+// words after the P slots) and every pass reads them there: for the small
+// batches of serving, whose few blocks would otherwise wait on L2 once per pass.
+__global__ void __launch_bounds__(1024) k_select_rows(const float* __restrict__ scores, size_t ld, int ncols, int P,
+                                                      const uint64_t* __restrict__ allow, const uint64_t* __restrict__ deny,
+                                                      size_t col_base, bool eq0, bool staged, uint32_t* __restrict__ out_col,
+                                                      float* __restrict__ out_score) {
     extern __shared__ uint8_t sm_raw[];
     const int Pp = next_pow2(P);
     uint64_t* skey = reinterpret_cast<uint64_t*>(sm_raw);
     int64_t* sval = reinterpret_cast<int64_t*>(skey + Pp);
+    uint32_t* rkey = reinterpret_cast<uint32_t*>(sval + Pp);   // staged: the row's keys
     __shared__ uint32_t hist[256];
     __shared__ uint32_t s_prefix, s_mask, s_remaining;
-    __shared__ uint32_t warp_cnt[2][8];
+    __shared__ uint32_t warp_cnt[2][32];
     const float* row = scores + static_cast<size_t>(blockIdx.x) * ld;
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -180,15 +184,18 @@ __global__ void __launch_bounds__(256) k_select_rows(const float* __restrict__ s
         s_mask = 0;
         s_remaining = static_cast<uint32_t>(P);
     }
+    auto key_of = [&](int c) -> uint32_t {
+        return col_allowed(allow, deny, col_base + c) ? (eq0 ? float_key_eq0(row[c]) : float_key(row[c])) : 0xFFFFFFFFu;
+    };
+    if (staged)
+        for (int c = tid; c < ncols; c += blockDim.x) rkey[c] = key_of(c);   // (the first pass's barrier orders these)
     for (int shift = 24; shift >= 0; shift -= 8) {
         for (int b = tid; b < 256; b += blockDim.x) hist[b] = 0;
         __syncthreads();
         const uint32_t prefix = s_prefix, mask = s_mask;
         for (int c0 = 0; c0 < ncols; c0 += blockDim.x) {   // (trip count block-uniform)
             const int c = c0 + tid;
-            const uint32_t k = c < ncols && col_allowed(allow, deny, col_base + c)
-                                   ? (eq0 ? float_key_eq0(row[c]) : float_key(row[c]))
-                                   : 0xFFFFFFFFu;
+            const uint32_t k = c < ncols ? (staged ? rkey[c] : key_of(c)) : 0xFFFFFFFFu;
             const int bin = c < ncols && (k & mask) == prefix ? static_cast<int>((k >> shift) & 255u) : -1;
             // lanes of a warp that share a bin add once (early passes put most keys in a few bins)
             const unsigned same = __match_any_sync(0xffffffffu, bin);
@@ -234,9 +241,7 @@ __global__ void __launch_bounds__(256) k_select_rows(const float* __restrict__ s
     const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
     const int span = ((ncols + nwarps - 1) / nwarps + 31) & ~31;
     const int c_begin = min(ncols, warp * span), c_end = min(ncols, c_begin + span);
-    auto key_at = [&](int c) -> uint32_t {
-        return col_allowed(allow, deny, col_base + c) ? (eq0 ? float_key_eq0(row[c]) : float_key(row[c])) : 0xFFFFFFFFu;
-    };
+    auto key_at = [&](int c) -> uint32_t { return staged ? rkey[c] : key_of(c); };
     uint32_t n_lt = 0, n_eq = 0;
     for (int c0 = c_begin; c0 < c_end; c0 += 32) {
         const int c = c0 + lane;
@@ -311,11 +316,17 @@ __global__ void __launch_bounds__(256) k_select_rows(const float* __restrict__ s
 void select_rows(const float* scores, size_t ld, int nrows, int ncols, int P, uint32_t* out_col, float* out_score,
                  cudaStream_t st, const uint64_t* allow, const uint64_t* deny, size_t col_base, bool eq0) {
     if (nrows == 0) return;
-    const size_t smem = static_cast<size_t>(next_pow2(P)) * 16;
+    // few rows (serving's small batches): 1,024 threads a row and the row's
+    // keys staged in shared memory; many rows: 256 threads, keys from L2
+    const bool few = nrows < 2 * sm_count();
+    const size_t base = static_cast<size_t>(next_pow2(P)) * 16;
+    const bool staged = few && base + static_cast<size_t>(ncols) * 4 <= 160 * 1024;
+    const size_t smem = base + (staged ? static_cast<size_t>(ncols) * 4 : 0);
     if (smem > 48 * 1024)
         allow_large_smem<k_select_rows>();
     KernelTimer kt("select_rows", st);
-    k_select_rows<<<nrows, 256, smem, st>>>(scores, ld, ncols, P, allow, deny, col_base, eq0, out_col, out_score);
+    k_select_rows<<<nrows, few ? 1024 : 256, smem, st>>>(scores, ld, ncols, P, allow, deny, col_base, eq0, staged,
+                                                          out_col, out_score);
     QG_LAUNCH_CHECK();
 }
 

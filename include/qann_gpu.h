@@ -220,10 +220,15 @@ int qg_fast_scan_noalloc_dev(const uint8_t* lut_dev, size_t nluts, size_t m, con
  *   "tensor_coarse_queries", "tensor_coarse_redone" (queries sent back to the exact path after too many
  *   near-ties) and "tensor_coarse_candidates" (lists rescored exactly). No counterpart in the reference, whose
  *   exact scores always come from its CPU distance kernels (reference src/flat_index.cpp:33-64).
+ *   Filtered IVF searches rank only the nearest lists their probe walk is expected to need, through the same
+ *   coarse step; "filtered_batches" counts filtered batches and "filtered_deep_walks" those of them whose walk
+ *   went past the ranked lists, so that every list was ranked (reference src/ivf_index.cpp:501-521 ranks every
+ *   list of every filtered query).
  * "scan_autotune": 1 (default) times the fast-scan kernel's candidate shapes
  *   (warps per block, lists per LUT group, codes read from global memory or
  *   staged through shared memory by bulk copies) on the first large search of
- *   each problem (scoring mode, m, k', nprobe, batch size) and keeps the
+ *   each problem (scoring mode, m, k', and nprobe and batch size by their power
+ *   of two) and keeps the
  *   fastest; 0 uses the first shape. "scan_variant": -1 (default) any shape,
  *   0 only unstaged shapes sized for two blocks per SM, 1 only staged, 2 only
  *   the dense unstaged shapes (registers sized for 3 blocks of 8 warps or 5

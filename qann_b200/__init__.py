@@ -93,7 +93,9 @@ def tensor_filter() -> int:
 
 def tensor_filter_counts() -> dict:
     """Queries answered through the tensor-core filter so far, and how many of
-    them were redone exactly because their candidate lists overflowed."""
+    them were redone exactly because their candidate lists overflowed; the
+    same for the coarse step; filtered batches, and how many of them ranked
+    every list because a probe walk went past the lists ranked first."""
     out = {}
     for key in ("queries", "redone"):
         v = C.c_int64()
@@ -103,6 +105,10 @@ def tensor_filter_counts() -> dict:
         v = C.c_int64()
         check(_lib.lib.qg_get_option(f"tensor_coarse_{key}".encode(), C.byref(v)))
         out[f"coarse_{key}"] = v.value
+    for key in ("batches", "deep_walks"):
+        v = C.c_int64()
+        check(_lib.lib.qg_get_option(f"filtered_{key}".encode(), C.byref(v)))
+        out[f"filtered_{key}"] = v.value
     return out
 
 

@@ -643,6 +643,11 @@ int qg_get_option(const char* key, int64_t* value) {
             *value = k == "tensor_coarse_queries" ? cq : cr;
         }
         else if (k == "tensor_coarse_candidates") *value = tensor_coarse_candidates();
+        else if (k == "filtered_batches" || k == "filtered_deep_walks") {
+            int64_t b = 0, dw = 0;
+            filtered_rank_counts(&b, &dw);
+            *value = k == "filtered_batches" ? b : dw;
+        }
         else if (k == "search_graphs") *value = search_graphs();
         else if (k == "search_graph_replays" || k == "search_graph_captures") {
             int64_t rp = 0, cp = 0;

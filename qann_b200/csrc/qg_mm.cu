@@ -773,15 +773,15 @@ static int coarse_cap(int nlist, int P) {
     return std::min(next_pow2(nlist), std::max(1024, next_pow2(4 * P)));
 }
 
-bool coarse_mm_supported(int nlist, int dim, int P, bool cent_prepared, bool capture) {
-    const int cap = capture ? next_pow2(nlist) : coarse_cap(nlist, P);
+bool coarse_mm_supported(int nlist, int dim, int P, bool cent_prepared, bool no_readback) {
+    const int cap = no_readback ? next_pow2(nlist) : coarse_cap(nlist, P);
     return cent_prepared && mm_supported(dim) && P >= 1 && P <= nlist && nlist <= 16384 &&
            coarse_recheck_smem(nlist, dim, cap) <= 200 * 1024;
 }
 
 void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t* probe, float* pdist,
-                      std::vector<int>& redo_q, cudaStream_t st, int* capture_err) {
-    const bool capture = capture_err != nullptr;
+                      std::vector<int>& redo_q, cudaStream_t st, int* err_dev) {
+    const bool no_readback = err_dev != nullptr;
     redo_q.clear();
     if (nq == 0) return;
     const int d = v.dim, nlist = v.nlist;
@@ -797,7 +797,7 @@ void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t*
         DevBuf<float> accm(static_cast<size_t>(nb) * ld, st);
         DevBuf<int> redo, err;
         DevBuf<unsigned long long> ncand;
-        if (!capture) {
+        if (!no_readback) {
             redo.alloc(nb, st);
             err.alloc(1, st);
             ncand.alloc(1, st);
@@ -818,7 +818,7 @@ void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t*
         a.ksteps = (d + 15) / 16;
         a.mtiles = static_cast<int>(ceil_div(static_cast<size_t>(nb), BM));
         a.ntiles = static_cast<int>(ceil_div(static_cast<size_t>(nlist), BN));
-        a.err = capture ? capture_err : err.get();
+        a.err = no_readback ? err_dev : err.get();
         a.store = accm.get();
         a.ld = ld;
         a.f16 = 1;
@@ -828,7 +828,7 @@ void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t*
                                                                                                                tmB, a);
             QG_LAUNCH_CHECK();
         }
-        const int cap = capture ? next_pow2(nlist) : coarse_cap(nlist, P);   // captured: every list fits
+        const int cap = no_readback ? next_pow2(nlist) : coarse_cap(nlist, P);   // no read-back: every list fits
         const size_t rsm = coarse_recheck_smem(nlist, d, cap);
         allow_large_smem<k_coarse_recheck>();
         // f16 inputs: unit roundoff 2^-11 in place of bf16's 2^-8 (subnormal
@@ -845,7 +845,7 @@ void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t*
                 c_lo, accm.get(), ld, P, cap, probe + q0 * P, pdist + q0 * P, redo.get(), ncand.get());
             QG_LAUNCH_CHECK();
         }
-        if (capture) continue;   // the flags are read after each replay
+        if (no_readback) continue;   // the caller reads the flag with the results
         int herr = 0;
         unsigned long long hcand = 0;
         std::vector<int> hredo(nb);

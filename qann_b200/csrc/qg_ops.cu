@@ -140,10 +140,14 @@ void tensor_coarse_counts(int64_t* queries, int64_t* redone) {
     *redone = g_coarse_redone.load();
 }
 
+// The coarse step on the tensor cores once the exact tiles' work passes
+// 2.5e7 multiply-adds (about 12 queries against 16,384 lists of 128
+// dimensions): there the exact scores and row select of a batch took 66 us
+// at 16 queries and 310 us at 256, the F16 GEMM and recheck 47 and 56 us.
 bool use_tensor_coarse(size_t nq, int nlist, int dim) {
     const int mode = g_tensor_filter.load();
     return mode > 0 && mm_supported(dim) &&
-           (mode == 2 || (nq >= 64 && static_cast<double>(nq) * nlist * dim >= 1e9));
+           (mode == 2 || static_cast<double>(nq) * nlist * dim >= 2.5e7);
 }
 
 void flat_candidates(const float* q_dev, size_t nq, const float* rows_dev, size_t n, int dim, bool ip, size_t k,
@@ -219,7 +223,7 @@ struct Prepared {
 };
 } // namespace
 
-static void prepare(IndexObj& idx, const SearchRequest& r, Prepared& p, cudaStream_t st) {
+static void prepare(IndexObj& idx, const SearchRequest& r, Prepared& p, cudaStream_t st, bool upload_filter = true) {
     const size_t dim = idx.dim();
     const size_t n = r.nq * dim;
     if (r.err_dev) {
@@ -242,7 +246,7 @@ static void prepare(IndexObj& idx, const SearchRequest& r, Prepared& p, cudaStre
     } else {
         QG_CUDA(cudaMemcpyAsync(p.q.get(), src, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
     }
-    if (r.filter) {
+    if (r.filter && upload_filter) {
         p.filter.alloc(r.filter->words.size(), st);
         QG_CUDA(cudaMemcpyAsync(p.filter.get(), r.filter->words.data(), r.filter->words.size() * 8,
                                 cudaMemcpyHostToDevice, st));
@@ -291,11 +295,23 @@ static size_t min_probes_for(const IVFModel& M, size_t nprobe, size_t count) {
     return std::clamp<size_t>(static_cast<size_t>(std::min(want, double(M.nlist))), nprobe, M.nlist);
 }
 
+// Lists a filtered query's probe walk is expected to need, to be ranked before
+// it: its min_probes, or twice as many lists as hold `wanted` allowed vectors
+// at the filter's mean density, plus 16; 0 (rank every list) from half of
+// them. A walk that goes further ranks every list, so this sets only the cost.
+static int rank_depth_for(const IVFModel& M, size_t min_probes, size_t wanted, size_t count) {
+    const double per_list = double(count) / double(M.nlist);
+    const double need = per_list > 0.0 ? 2.0 * double(wanted) / per_list : double(M.nlist);
+    const double r = std::max(double(min_probes), std::ceil(need)) + 16.0;
+    return 2.0 * r >= double(M.nlist) ? 0 : static_cast<int>(r);
+}
+
 static void filter_probing(IvfSearchArgs& a, const IVFModel& M, const SlotBits* f, const uint64_t* f_dev, size_t k) {
     if (!f) return;
     a.filter = f_dev;
     a.wanted = static_cast<int>(std::min(k, f->count));
     a.min_probes = static_cast<int>(min_probes_for(M, static_cast<size_t>(a.nprobe), f->count));
+    a.rank_depth = rank_depth_for(M, static_cast<size_t>(a.min_probes), static_cast<size_t>(a.wanted), f->count);
 }
 
 __global__ void k_cols_to_slots(uint32_t* __restrict__ cs, size_t n, const uint32_t* __restrict__ slots) {
@@ -420,11 +436,13 @@ void search(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
         return;
     }
     ensure_device(o, st);
-    Prepared p;
-    prepare(idx, r, p, st);
     // narrow filters through an IVF base: exact scores of the allowed rows
     // (RefineIndex::use_direct / direct_scan, reference src/refine_index.cpp:59-82)
-    if (r.filter && o.base->kind == Kind::IVF && r.filter->count <= 6 * static_cast<IVFObj&>(*o.base).model.nlist) {
+    const bool direct =
+        r.filter && o.base->kind == Kind::IVF && r.filter->count <= 6 * static_cast<IVFObj&>(*o.base).model.nlist;
+    Prepared p;
+    prepare(idx, r, p, st, !direct);   // (the direct scan lists the allowed slots on the host)
+    if (direct) {
         refine_direct(o, p, r, dim, ip, cosine, out_ids, out_d, st);
         finish(p);
         return;
@@ -668,14 +686,39 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
     const IVFModel& M = ivf->model;
     const size_t live = idx.idmap().live_count();
     std::vector<size_t> batch;
+    // narrow filters of a RefineIndex (RefineIndex::use_direct): exact scans of
+    // the allowed rows, one per (filter, k) among the batch's requests
+    std::vector<std::pair<std::pair<const SlotBits*, int>, std::vector<size_t>>> direct;
     for (size_t i = 0; i < nq; ++i) {
         const SlotBits* f = qs[i].filter;
         if (live == 0 || (f && f->count == 0)) continue;                      // nothing to return
-        if (ref && f && f->count <= 6 * M.nlist) {                             // RefineIndex::use_direct
-            alone(i);
+        if (ref && f && f->count <= 6 * M.nlist) {
+            const auto key = std::make_pair(f, qs[i].k);
+            auto it = std::find_if(direct.begin(), direct.end(), [&](const auto& g) { return g.first == key; });
+            if (it == direct.end()) direct.push_back({key, {i}});
+            else it->second.push_back(i);
             continue;
         }
         batch.push_back(i);
+    }
+    for (const auto& g : direct) {
+        const size_t n = g.second.size(), k = static_cast<size_t>(g.first.second);
+        std::vector<float> qh(n * dim);
+        for (size_t j = 0; j < n; ++j) std::copy_n(q + g.second[j] * dim, dim, qh.data() + j * dim);
+        std::vector<int64_t> gi(n * k);
+        std::vector<float> gd(n * k);
+        SearchRequest r;
+        r.q = qh.data();
+        r.nq = n;
+        r.k = k;
+        r.filter = g.first.first;
+        r.out_ids = gi.data();
+        r.out_d = gd.data();
+        search(idx, r, st);
+        for (size_t j = 0; j < n; ++j) {
+            std::copy_n(gi.data() + j * k, k, out_ids + g.second[j] * kmax);
+            std::copy_n(gd.data() + j * k, k, out_d + g.second[j] * kmax);
+        }
     }
     if (batch.empty()) return;
     if (ref) ensure_device(*ref, st);
@@ -705,8 +748,8 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
         std::vector<int> h(kFields * nb);
         std::vector<const SlotBits*> distinct;
         std::vector<size_t> which(nb, SIZE_MAX);
-        int npmax = 1, kpmax = 1;
-        bool any_filter = false;
+        int npmax = 1, kpmax = 1, depth = 1;
+        bool any_filter = false, deep = false;
         for (size_t j = 0; j < nb; ++j) {
             const MixedQuery& m = qs[batch[j]];
             const size_t np = std::min<size_t>(m.nprobe > 0 ? static_cast<size_t>(m.nprobe) : M.nprobe, M.nlist);
@@ -719,6 +762,10 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
                 any_filter = true;
                 h[kMin * nb + j] = static_cast<int>(min_probes_for(M, np, m.filter->count));
                 h[kWanted * nb + j] = static_cast<int>(std::min(kp, m.filter->count));
+                const int dj = rank_depth_for(M, static_cast<size_t>(h[kMin * nb + j]),
+                                              static_cast<size_t>(h[kWanted * nb + j]), m.filter->count);
+                deep = deep || dj == 0;
+                depth = std::max(depth, dj);
                 if (!m.filter_dev) {   // (registered filters are on the device already)
                     auto it = std::find(distinct.begin(), distinct.end(), m.filter);
                     which[j] = static_cast<size_t>(it - distinct.begin());
@@ -764,6 +811,7 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
         a.pq.min_probes = dh.get() + kMin * nb;
         a.pq.wanted = dh.get() + kWanted * nb;
         a.any_filter = any_filter;
+        a.rank_depth = deep ? 0 : std::max(depth, npmax);
         a.sm_count = sm_count_cached();
         a.d_err = p.err;
         DevBuf<uint64_t> ck(nb * kpmax, st);

@@ -767,7 +767,7 @@ struct ScanShape {
 };
 
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int, int>, ScanShape> g_tuned;   // (mode, m_pad, kp, P, log2 nq, variant) -> shape
+std::map<std::tuple<int, int, int, int, int, int>, ScanShape> g_tuned;   // (mode, m_pad, kp, log2 P, log2 nq, variant) -> shape
 std::atomic<int> g_autotune{1};    // 0: the first fitting unstaged shape, 1: tune
 std::atomic<int> g_force{-1};      // -1: any; 0: unstaged (two-block) only; 1: staged only; 2: dense only
 std::atomic<int> g_last_shape{0};  // the last scan's shape: warps * 1000 + lists per group * 10 + staged
@@ -938,16 +938,25 @@ static void scan_query_major(const IvfView& v, const IvfSearchArgs& s, int nq, i
     a.out_slot = direct ? out_slot : cslot.get();
     a.err = s.d_err;
     // the shape: tuned once per problem key on a search large enough to fill
-    // the GPU several times over, else the first candidate
+    // the GPU several times over, else the first candidate. Batch size and
+    // probe count enter the key by their power of two (served batches, whose
+    // largest nprobe or filtered probe count changes from batch to batch,
+    // would otherwise tune nearly every batch); a shape tuned for another
+    // member of the bucket is kept when it is among this search's candidates.
     const int nq_bucket = 31 - __builtin_clz(static_cast<unsigned>(std::max(1, nq)));
-    const auto key = std::make_tuple(v.mode, v.m_pad, kp, P, nq_bucket, g_force.load());
+    const int p_bucket = 31 - __builtin_clz(static_cast<unsigned>(std::max(1, P)));
+    const auto key = std::make_tuple(v.mode, v.m_pad, kp, p_bucket, nq_bucket, g_force.load());
     ScanShape shape = cands.front();
     bool tuned = !g_autotune.load();
     if (!tuned) {
         std::lock_guard<std::mutex> g(g_tune_mu);
         const auto it = g_tuned.find(key);
         if (it != g_tuned.end()) {
-            shape = it->second;
+            const ScanShape t = it->second;
+            if (std::any_of(cands.begin(), cands.end(), [&](const ScanShape& c) {
+                    return c.nw == t.nw && c.lc == t.lc && c.staged == t.staged && c.dense == t.dense;
+                }))
+                shape = t;
             tuned = true;
         }
     }
@@ -962,6 +971,46 @@ static void scan_query_major(const IvfView& v, const IvfSearchArgs& s, int nq, i
     if (!direct) merge_candidates(ckey.get(), cslot.get(), nq, nchunks, kp, out_key, out_slot, st);
 }
 
+void nearest_lists(const IvfView& v, const IvfSearchArgs& s, int nq, int P, uint32_t* probe, float* pdist,
+                   cudaStream_t st) {
+    if (nq == 0) return;
+    // exact pair scores, then the P nearest lists per query by (score, list),
+    // compared as the reference's heap of (float, uint16_t) pairs does: -0 == +0
+    auto exact_coarse = [&](const float* qs, int n, uint32_t* pr, float* pd) {
+        DevBuf<float> scores(static_cast<size_t>(n) * v.nlist, st);
+        pair_scores(qs, n, v.centroids, v.nlist, v.dim, v.ip_metric, scores.get(), v.nlist, st);
+        select_rows(scores.get(), v.nlist, n, v.nlist, P, pr, pd, st, nullptr, nullptr, 0, true);
+    };
+    // batches of at most one query per SM (and captured ones) read nothing
+    // back mid-search: their recheck holds every list, so none is redone
+    const bool no_readback = s.d_err && (s.capture || nq <= s.sm_count);
+    if (!use_tensor_coarse(nq, v.nlist, v.dim) ||
+        !coarse_mm_supported(v.nlist, v.dim, P, v.cent_f16 != nullptr, no_readback)) {
+        exact_coarse(s.q, nq, probe, pdist);
+        return;
+    }
+    std::vector<int> redo;
+    coarse_probes_mm(v, s.q, nq, P, probe, pdist, redo, st, no_readback ? s.d_err + 2 : nullptr);
+    if (!s.capture) count_tensor_coarse(nq, static_cast<int64_t>(redo.size()));
+    if (redo.empty()) return;
+    // queries with too many near-ties: the exact path, results copied into place
+    const size_t m = redo.size();
+    std::vector<uint32_t> hidx(redo.begin(), redo.end());
+    DevBuf<uint32_t> idx(m, st);
+    QG_CUDA(cudaMemcpyAsync(idx.get(), hidx.data(), m * 4, cudaMemcpyHostToDevice, st));
+    DevBuf<float> qs(m * v.dim, st);
+    gather_rows(s.q, idx.get(), m, v.dim, qs.get(), st);
+    DevBuf<uint32_t> pr(m * P, st);
+    DevBuf<float> pd(m * P, st);
+    exact_coarse(qs.get(), static_cast<int>(m), pr.get(), pd.get());
+    for (size_t j = 0; j < m; ++j) {
+        QG_CUDA(cudaMemcpyAsync(probe + static_cast<size_t>(redo[j]) * P, pr.get() + j * P, P * 4,
+                                cudaMemcpyDeviceToDevice, st));
+        QG_CUDA(cudaMemcpyAsync(pdist + static_cast<size_t>(redo[j]) * P, pd.get() + j * P, P * 4,
+                                cudaMemcpyDeviceToDevice, st));
+    }
+}
+
 void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st) {
     const int nq = s.nq, kp = s.kp;
     if (nq == 0) return;
@@ -971,46 +1020,13 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
     DevBuf<int> nprobe_q;
     const int* probes_of = s.pq.nprobe;   // unfiltered mixed batch: each query's own nprobe (<= P)
     if (s.filter || s.any_filter) {
-        // every list ranked, then each query's own probe count (reference src/ivf_index.cpp:501-521)
+        // the nearest lists ranked, then each query's own probe count (reference src/ivf_index.cpp:501-521)
         P = filtered_probes(v, s, probe, pdist, nprobe_q, st);
         probes_of = nprobe_q.get();
     } else {
         probe.alloc(static_cast<size_t>(nq) * P, st);
         pdist.alloc(static_cast<size_t>(nq) * P, st);
-        // coarse: exact pair scores, then the P nearest lists per query by
-        // (score, list), compared as the reference's heap of (float, uint16_t)
-        // pairs does: -0 == +0 (for queries `sel` of the batch, or all)
-        auto exact_coarse = [&](const float* qs, int n, uint32_t* pr, float* pd) {
-            DevBuf<float> scores(static_cast<size_t>(n) * v.nlist, st);
-            pair_scores(qs, n, v.centroids, v.nlist, v.dim, v.ip_metric, scores.get(), v.nlist, st);
-            select_rows(scores.get(), v.nlist, n, v.nlist, P, pr, pd, st, nullptr, nullptr, 0, true);
-        };
-        if (use_tensor_coarse(nq, v.nlist, v.dim) &&
-            coarse_mm_supported(v.nlist, v.dim, P, v.cent_f16 != nullptr, s.capture)) {
-            std::vector<int> redo;
-            coarse_probes_mm(v, s.q, nq, P, probe.get(), pdist.get(), redo, st, s.capture ? s.d_err + 2 : nullptr);
-            if (!s.capture) count_tensor_coarse(nq, static_cast<int64_t>(redo.size()));
-            if (!redo.empty()) {
-                // queries with too many near-ties: the exact path, results copied into place
-                const size_t m = redo.size();
-                std::vector<uint32_t> hidx(redo.begin(), redo.end());
-                DevBuf<uint32_t> idx(m, st);
-                QG_CUDA(cudaMemcpyAsync(idx.get(), hidx.data(), m * 4, cudaMemcpyHostToDevice, st));
-                DevBuf<float> qs(m * v.dim, st);
-                gather_rows(s.q, idx.get(), m, v.dim, qs.get(), st);
-                DevBuf<uint32_t> pr(m * P, st);
-                DevBuf<float> pd(m * P, st);
-                exact_coarse(qs.get(), static_cast<int>(m), pr.get(), pd.get());
-                for (size_t j = 0; j < m; ++j) {
-                    QG_CUDA(cudaMemcpyAsync(probe.get() + static_cast<size_t>(redo[j]) * P, pr.get() + j * P, P * 4,
-                                            cudaMemcpyDeviceToDevice, st));
-                    QG_CUDA(cudaMemcpyAsync(pdist.get() + static_cast<size_t>(redo[j]) * P, pd.get() + j * P, P * 4,
-                                            cudaMemcpyDeviceToDevice, st));
-                }
-            }
-        } else {
-            exact_coarse(s.q, nq, probe.get(), pdist.get());
-        }
+        nearest_lists(v, s, nq, P, probe.get(), pdist.get(), st);
     }
 
     DevBuf<float> pterm(static_cast<size_t>(nq) * P, st);

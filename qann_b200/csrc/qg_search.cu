@@ -13,8 +13,8 @@
 //                     (reference :421-641 and src/topk.hpp)
 //   k_merge           per query: the k' best of its chunks
 //   k_finalize_ivf /  the k results, sorted by (distance, id) (reference
-//   k_refine          src/topk.hpp:53-77), or re-ranked with exact distances
-//                     from the raw rows (reference src/refine_index.cpp:112-140)
+//   k_refine_scores + src/topk.hpp:53-77), or re-ranked with exact distances
+//   k_refine_select   from the raw rows (reference src/refine_index.cpp:112-140)
 #include "qg_device.cuh"
 #include "qg_search.h"
 
@@ -401,9 +401,11 @@ __global__ void k_query_tables(IvfView v, const float* __restrict__ q, float* __
 // from the top and stopping once every key of the chosen bin is kept, then
 // the survivors compacted and sorted. One block per query.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_merge(const uint64_t* __restrict__ in_key, const uint32_t* __restrict__ in_slot,
-                                               int nchunks, int kp, int npow, uint64_t* __restrict__ out_key,
-                                               uint32_t* __restrict__ out_slot) {
+// Every pass reads 4 keys a thread before it bins them, so that the loads of
+// a pass (from L2) overlap instead of each waiting for the last.
+__global__ void __launch_bounds__(1024) k_merge(const uint64_t* __restrict__ in_key, const uint32_t* __restrict__ in_slot,
+                                                int nchunks, int kp, int npow, uint64_t* __restrict__ out_key,
+                                                uint32_t* __restrict__ out_slot) {
     extern __shared__ uint8_t sm_raw[];
     uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);   // npow
     int64_t* val = reinterpret_cast<int64_t*>(key + npow);
@@ -418,8 +420,19 @@ __global__ void __launch_bounds__(256) k_merge(const uint64_t* __restrict__ in_k
         s_count = 0;
     }
     __syncthreads();
+    constexpr int U = 4;   // keys in flight per thread
+    const int step = U * blockDim.x;
     int mine = 0;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) mine += ik[e] != ~0ull;
+    for (int b0 = 0; b0 < total; b0 += step) {
+        uint64_t kk[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = b0 + u * blockDim.x + threadIdx.x;
+            kk[u] = e < total ? ik[e] : ~0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) mine += kk[u] != ~0ull;
+    }
     for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
     if (lane == 0) atomicAdd(&s_valid, mine);
     __syncthreads();
@@ -430,13 +443,21 @@ __global__ void __launch_bounds__(256) k_merge(const uint64_t* __restrict__ in_k
         for (;; shift -= 8) {
             for (int j = threadIdx.x; j < 256; j += blockDim.x) hist[j] = 0;
             __syncthreads();
-            for (int b0 = 0; b0 < total; b0 += blockDim.x) {   // (trip count is block-uniform)
-                const int e = b0 + threadIdx.x;
-                const uint64_t k = e < total ? ik[e] : ~0ull;
-                const bool in = k != ~0ull && (k & mask) == prefix;
-                const int bin = in ? static_cast<int>((k >> shift) & 255) : -1;
-                const unsigned same = __match_any_sync(0xffffffffu, bin);
-                if (in && lane == __ffs(same) - 1) atomicAdd(&hist[bin], __popc(same));
+            for (int b0 = 0; b0 < total; b0 += step) {   // (trip count is block-uniform)
+                uint64_t kk[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int e = b0 + u * blockDim.x + threadIdx.x;
+                    kk[u] = e < total ? ik[e] : ~0ull;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint64_t k = kk[u];
+                    const bool in = k != ~0ull && (k & mask) == prefix;
+                    const int bin = in ? static_cast<int>((k >> shift) & 255) : -1;
+                    const unsigned same = __match_any_sync(0xffffffffu, bin);
+                    if (in && lane == __ffs(same) - 1) atomicAdd(&hist[bin], __popc(same));
+                }
             }
             __syncthreads();
             if (threadIdx.x < 32) {
@@ -477,13 +498,22 @@ __global__ void __launch_bounds__(256) k_merge(const uint64_t* __restrict__ in_k
         lim = prefix | ((1ull << shift) - 1);
     }
     // the survivors (at most kp), then sorted
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const uint64_t k = ik[e];
-        if (k != ~0ull && k <= lim) {
-            const int pos = atomicAdd(&s_count, 1);
-            if (pos < npow) {
-                key[pos] = k;
-                val[pos] = static_cast<int64_t>(is[e]);
+    for (int b0 = 0; b0 < total; b0 += step) {
+        uint64_t kk[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = b0 + u * blockDim.x + threadIdx.x;
+            kk[u] = e < total ? ik[e] : ~0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = b0 + u * blockDim.x + threadIdx.x;
+            if (kk[u] != ~0ull && kk[u] <= lim) {
+                const int pos = atomicAdd(&s_count, 1);
+                if (pos < npow) {
+                    key[pos] = kk[u];
+                    val[pos] = static_cast<int64_t>(is[e]);
+                }
             }
         }
     }
@@ -542,93 +572,55 @@ __global__ void __launch_bounds__(128) k_finalize_ivf(const uint64_t* __restrict
 // Re-rank (reference src/refine_index.cpp:112-140): the exact score of every
 // candidate from the raw rows, then the k smallest by (score, slot), compared
 // as floats (so -0 == +0), ids mapped through the refine index's labels.
-// Candidate rows are gathered a tile at a time into shared memory, each warp
-// reading whole rows with coalesced loads, at an odd row stride so that the
-// threads' walks along their own rows fall on distinct banks.
+// Two kernels: every candidate of the batch scored at once, an 8-lane group
+// per candidate reading its row with 128-byte loads (so a batch of one query
+// spreads its gathers over the whole GPU as a large batch does), each score
+// kept as key(score) << 32 | slot; then per query those keys sorted.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 8) k_refine(const float* __restrict__ q, int dim, const float* __restrict__ rows,
-                                                const uint64_t* __restrict__ key_in, const uint32_t* __restrict__ slot_in,
-                                                int kp, int k, bool ip, const int64_t* __restrict__ labels, bool cosine,
-                                                int64_t* __restrict__ out_ids, float* __restrict__ out_d,
-                                                const int* __restrict__ kp_q, const int* __restrict__ k_q, int tile) {
-    extern __shared__ uint8_t sm_raw[];
-    const int kpow = max(2, next_pow2(kp));
-    uint64_t* key = reinterpret_cast<uint64_t*>(sm_raw);
-    int64_t* val = reinterpret_cast<int64_t*>(key + kpow);
-    float* qv = reinterpret_cast<float*>(val + kpow);
-    float* trow = qv + dim;
-    const int stride = dim | 1;
-    __shared__ uint32_t s_slot[64];   // the tile's slots (tile <= 64)
-    const int qi = blockIdx.x;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+template <bool kIP>
+__global__ void __launch_bounds__(256) k_refine_scores(const float* __restrict__ q, int dim,
+                                                       const float* __restrict__ rows,
+                                                       const uint64_t* __restrict__ key_in,
+                                                       const uint32_t* __restrict__ slot_in, int nq, int kp,
+                                                       const int* __restrict__ kp_q, uint64_t* __restrict__ scored) {
+    const size_t g = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;   // candidate, query-major
+    const size_t total = static_cast<size_t>(nq) * kp;
+    // whole 8-lane groups take part in the shuffles; groups past the end, and
+    // empty candidates, score the query against itself unused
+    const bool in = g < total;
+    const size_t gi = in ? g : 0;
+    const int qi = static_cast<int>(gi / kp), c = static_cast<int>(gi % kp);
     const int kpq = kp_q ? min(kp_q[qi], kp) : kp;   // the query's first kpq candidates by key64
+    const bool ok = in && c < kpq && key_in[gi] != ~0ull;
+    const uint32_t sl = ok ? slot_in[gi] : 0u;
+    const float* qv = q + static_cast<size_t>(qi) * dim;
+    const float* row = ok ? rows + static_cast<size_t>(sl) * dim : qv;
+    const float d = kIP ? -exact_avx2_group8<false, true>(qv, row, dim) : exact_avx2_group8<true, true>(qv, row, dim);
+    if (in && (threadIdx.x & 7) == 0)
+        scored[gi] = ok ? (static_cast<uint64_t>(float_key_eq0(d)) << 32) | sl : ~0ull;
+}
+
+__global__ void __launch_bounds__(1024) k_refine_select(const float* __restrict__ q, int dim,
+                                                        const float* __restrict__ rows,
+                                                        const uint64_t* __restrict__ scored, int kp, int k, bool ip,
+                                                        const int64_t* __restrict__ labels, bool cosine,
+                                                        int64_t* __restrict__ out_ids, float* __restrict__ out_d,
+                                                        const int* __restrict__ k_q) {
+    extern __shared__ uint64_t rkey[];
+    const int kpow = max(2, next_pow2(kp));
+    const int qi = blockIdx.x;
     const int kq = k_q ? min(k_q[qi], k) : k;
-    for (int t = threadIdx.x; t < dim; t += blockDim.x) qv[t] = q[static_cast<size_t>(qi) * dim + t];
-    for (int i = kpq + threadIdx.x; i < kpow; i += blockDim.x) {
-        key[i] = ~0ull;
-        val[i] = INT64_MAX;
-    }
-    for (int t0 = 0; t0 < kpq; t0 += tile) {
-        const int nt = min(tile, kpq - t0);
-        __syncthreads();   // the previous tile's rows are consumed
-        // the tile's slots first (0xFFFFFFFF: no candidate), so that the row
-        // loads below do not wait on them batch by batch
-        for (int c = threadIdx.x; c < nt; c += blockDim.x) {
-            const size_t ci = static_cast<size_t>(qi) * kp + t0 + c;
-            s_slot[c] = key_in[ci] != ~0ull ? slot_in[ci] : 0xFFFFFFFFu;
-        }
-        __syncthreads();
-        // each warp gathers 8 rows at a time, 32 loads per lane in flight
-        for (int c0 = warp; c0 < nt; c0 += 8 * nwarps) {
-            const float* src[8];
-            bool ok[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int c = c0 + u * nwarps;
-                const uint32_t sl = c < nt ? s_slot[c] : 0xFFFFFFFFu;
-                ok[u] = sl != 0xFFFFFFFFu;
-                src[u] = ok[u] ? rows + static_cast<size_t>(sl) * dim : rows;
-            }
-            for (int e0 = 0; e0 < dim; e0 += 128) {
-                float x[8][4];
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int e = e0 + lane + 32 * j;
-                        x[u][j] = ok[u] && e < dim ? __ldg(src[u] + e) : 0.0f;
-                    }
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int e = e0 + lane + 32 * j;
-                        if (ok[u] && e < dim) trow[(c0 + u * nwarps) * stride + e] = x[u][j];
-                    }
-            }
-        }
-        __syncthreads();
-        for (int c = threadIdx.x; c < nt; c += blockDim.x) {
-            const int i = t0 + c;
-            const uint32_t sl = s_slot[c];
-            if (sl == 0xFFFFFFFFu) {
-                key[i] = ~0ull;
-                val[i] = INT64_MAX;
-                continue;
-            }
-            const float d = exact_score(qv, trow + c * stride, dim, ip);
-            key[i] = float_key_eq0(d);
-            val[i] = sl;
-        }
-    }
-    bitonic_sort(key, val, kpow);
+    for (int i = threadIdx.x; i < kpow; i += blockDim.x)
+        rkey[i] = i < kp ? scored[static_cast<size_t>(qi) * kp + i] : ~0ull;
+    bitonic_sort_keys(rkey, kpow);
+    const float* qv = q + static_cast<size_t>(qi) * dim;
     for (int i = threadIdx.x; i < k; i += blockDim.x) {
         const size_t o = static_cast<size_t>(qi) * k + i;
-        if (i >= kq || key[i] == ~0ull) {
+        if (i >= kq || rkey[i] == ~0ull) {
             out_ids[o] = -1;
             out_d[o] = __int_as_float(0x7f800000);
         } else {
-            const uint32_t slot = static_cast<uint32_t>(val[i]);
+            const uint32_t slot = static_cast<uint32_t>(rkey[i]);
             // recompute: float_key_eq0 folded -0 into +0, and the reference returns the value itself
             const float d = exact_score(qv, rows + static_cast<size_t>(slot) * dim, dim, ip);
             out_ids[o] = labels ? labels[slot] : static_cast<int64_t>(slot);
@@ -718,7 +710,8 @@ void merge_candidates(const uint64_t* in_key, const uint32_t* in_slot, int nq, i
     if (msm > 48 * 1024)
         allow_large_smem<k_merge>();
     KernelTimer kt("merge", st);
-    k_merge<<<nq, 256, msm, st>>>(in_key, in_slot, nchunks, kp, npow, out_key, out_slot);
+    // few queries (serving's small batches): 1,024 threads a query
+    k_merge<<<nq, nq < 2 * sm_count() ? 1024 : 256, msm, st>>>(in_key, in_slot, nchunks, kp, npow, out_key, out_slot);
     QG_LAUNCH_CHECK();
 }
 
@@ -736,17 +729,23 @@ void refine_candidates(const float* q, int nq, int dim, const float* rows, const
                        cudaStream_t st, const int* kp_q, const int* k_q) {
     if (nq == 0 || k == 0) return;
     const int kpow = std::max(2, next_pow2(kp));
-    // candidate rows staged per tile: up to 64 rows within ~48 KB, so that
-    // several blocks share an SM and their gathers overlap
-    const size_t row_bytes = static_cast<size_t>(dim | 1) * 4;
-    const int tile = static_cast<int>(std::clamp<size_t>((48 * 1024) / row_bytes, 1, 64));
-    const size_t rsm = static_cast<size_t>(kpow) * 16 + static_cast<size_t>(dim) * 4 + tile * row_bytes;
-    require(rsm <= 200 * 1024, "re-rank shared memory exceeds the B200 limit for this k * k_factor and dim",
-            kUnsupported);
-    allow_large_smem<k_refine>();
+    const size_t ssm = static_cast<size_t>(kpow) * 8;
+    require(ssm <= 200 * 1024, "re-rank shared memory exceeds the B200 limit for this k * k_factor", kUnsupported);
+    const size_t total = static_cast<size_t>(nq) * kp;
+    DevBuf<uint64_t> scored(total, st);
     KernelTimer kt("refine", st);
-    k_refine<<<nq, 128, rsm, st>>>(q, dim, rows, key, slot, kp, k, ip, labels, cosine, out_ids, out_d, kp_q, k_q,
-                                   tile);
+    const unsigned blocks = static_cast<unsigned>(ceil_div(total * 8, size_t{256}));
+    if (ip)
+        k_refine_scores<true><<<blocks, 256, 0, st>>>(q, dim, rows, key, slot, nq, kp, kp_q, scored.get());
+    else
+        k_refine_scores<false><<<blocks, 256, 0, st>>>(q, dim, rows, key, slot, nq, kp, kp_q, scored.get());
+    QG_LAUNCH_CHECK();
+    if (ssm > 48 * 1024)
+        allow_large_smem<k_refine_select>();
+    // few queries (serving's small batches): 1,024 threads a query for the sort
+    const int threads = nq < 2 * sm_count() ? 1024 : 256;
+    k_refine_select<<<nq, threads, ssm, st>>>(q, dim, rows, scored.get(), kp, k, ip, labels, cosine, out_ids, out_d,
+                                              k_q);
     QG_LAUNCH_CHECK();
 }
 

@@ -86,6 +86,9 @@ struct IvfSearchArgs {
     // filtered probing (reference src/ivf_index.cpp:501-521): probes run past
     // nprobe to at least min_probes, then until `wanted` allowed vectors were seen
     int min_probes = 0, wanted = 0;
+    // filtered batches: the nearest lists ranked per query before the walk
+    // (0 = every list); a walk that runs past them ranks every list instead
+    int rank_depth = 0;
     PerQuery pq;                // mixed batches; nprobe above is then the largest nprobe
     bool any_filter = false;    // some query of a mixed batch has a filter
     int sm_count = 0;
@@ -110,11 +113,20 @@ void probe_terms(const IvfView& v, const float* q, int nq, int P, const uint32_t
                  cudaStream_t st);
 void query_tables(const IvfView& v, const float* q, int nq, float* qC, uint4* qlut, float* qscale, float* qoffset,
                   cudaStream_t st);
-// Probe lists of filtered queries: every list ranked by (score, list), each
-// query's probe count (nprobe_q) from the filter's per-list allowed counts;
-// probe / pdist are nq x Pmax, and Pmax is returned.
+// Probe lists of filtered queries: the s.rank_depth nearest lists (or every
+// list) ranked by (score, list), each query's probe count (nprobe_q) from the
+// filter's per-list allowed counts; probe / pdist are nq x Pmax, and Pmax is
+// returned.
 int filtered_probes(const IvfView& v, const IvfSearchArgs& s, DevBuf<uint32_t>& probe, DevBuf<float>& pdist,
                     DevBuf<int>& nprobe_q, cudaStream_t st);
+// Filtered batches ranked so far, and how many of them ranked every list
+// because a walk went past their rank_depth nearest lists.
+void filtered_rank_counts(int64_t* batches, int64_t* deep);
+// The P nearest lists of each query by (exact score, list), -0 == +0, nearest
+// first, with their scores (reference src/ivf_index.cpp:305-419): the tensor
+// cores' estimates and exact recheck, or exact tiles and a row select.
+void nearest_lists(const IvfView& v, const IvfSearchArgs& s, int nq, int P, uint32_t* probe, float* pdist,
+                   cudaStream_t st);
 // The k' = s.kp best candidates of each query, as sorted (key64, slot) lists
 // (key64 = key(dist) << 32 | push index; 0xFFFF... marks an empty entry).
 void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key, uint32_t* out_slot, cudaStream_t st);
@@ -123,7 +135,7 @@ void ivf_candidates(const IvfView& v, const IvfSearchArgs& s, uint64_t* out_key,
 // error bound and an exact recheck; queries with too many near-ties are
 // listed in redo_q for the exact path. use_tensor_coarse: whether the batch
 // goes this way (the process-wide tensor-filter mode and the work's size).
-bool coarse_mm_supported(int nlist, int dim, int P, bool cent_prepared, bool capture = false);
+bool coarse_mm_supported(int nlist, int dim, int P, bool cent_prepared, bool no_readback = false);
 bool use_tensor_coarse(size_t nq, int nlist, int dim);
 // Queries whose coarse step went through the tensor cores, and those of them redone exactly.
 void count_tensor_coarse(int64_t queries, int64_t redone);
@@ -131,11 +143,12 @@ void tensor_coarse_counts(int64_t* queries, int64_t* redone);
 // Lists rescored exactly by the tensor-core coarse step so far (its candidates).
 void count_tensor_coarse_candidates(int64_t n);
 int64_t tensor_coarse_candidates();
-// Under capture (capture_err non-null) nothing is read back: every list fits
-// the recheck, queries with extreme norms rescore every list, and a pipeline
-// timeout is flagged in *capture_err.
+// With err_dev (under graph capture, and for batches of at most one query per
+// SM) nothing is read back and redo_q stays empty: every list fits the
+// recheck, queries with extreme norms rescore every list, and a pipeline
+// timeout is flagged in *err_dev for the caller to read with the results.
 void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t* probe, float* pdist,
-                      std::vector<int>& redo_q, cudaStream_t st, int* capture_err = nullptr);
+                      std::vector<int>& redo_q, cudaStream_t st, int* err_dev = nullptr);
 // Rows scaled by powers of two (2^exps) and rounded to f16 (zero-padded to
 // dpad, a multiple of 8), with their float squared norms (unscaled).
 void prepare_f16_rows(const float* rows, size_t n, int dim, DevBuf<uint16_t>& f16, DevBuf<float>& sq,

@@ -7,7 +7,7 @@ import ctypes as C
 from . import _lib
 
 KERNELS = ("pair_scores", "select_rows", "coarse_mm", "coarse_recheck", "probe_terms", "query_tables", "scan", "merge",
-           "refine", "rank_lists", "mm_filter", "tscan_prep", "tscan", "tscan_final")
+           "refine", "rank_lists", "probe_walk", "mm_filter", "tscan_prep", "tscan", "tscan_final")
 
 
 def enable(on: bool = True) -> None:

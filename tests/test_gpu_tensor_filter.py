@@ -151,17 +151,24 @@ def test_coarse_identical(metric, d):
 
 def test_coarse_overflow_redone_exactly():
     """More lists within the error bound than the recheck holds (queries far
-    from every list, 2048 lists): those queries go back to the exact path."""
+    from every list, 2048 lists). In a batch of more queries than SMs those
+    queries go back to the exact path; in a smaller batch the recheck holds
+    every list and rescores them all in place, with nothing redone."""
     d = 32
     x = clustered(11, 30000, d, centres=1000, sigma=0.2)
     ivf = qb.IVFIndex(d, 2048, 16)
     ivf.enable_pq(8, fast_scan=True)
     ivf.train(x, seed=5)
     ivf.add(x)
-    qs = np.vstack([clustered(12, 100, d, centres=1000, sigma=0.2), np.full((4, d), 1000.0, dtype=np.float32)])
+    far = np.full((4, d), 1000.0, dtype=np.float32)
+    qs = np.vstack([clustered(12, 300, d, centres=1000, sigma=0.2), far])
     exact, fast, redone = coarse_runs(lambda: ivf.batch_query(qs, 10))
     assert_same(exact, fast)
     assert redone >= 4
+    qs = np.vstack([clustered(13, 60, d, centres=1000, sigma=0.2), far])
+    exact, fast, redone = coarse_runs(lambda: ivf.batch_query(qs, 10))
+    assert_same(exact, fast)
+    assert redone == 0
 
 
 @pytest.mark.parametrize("name", ["l2", "l2_adc", "ip", "cos_ip", "cos_l2", "l2_custom_del"])

@@ -58,6 +58,66 @@ __device__ __noinline__ static void bitonic_sort_keys(uint64_t* key, int n) {
     __syncthreads();
 }
 
+// One warp sorts n <= 32 * K keys in registers (a network of 32 * K, the
+// places past n holding all-ones keys that sort last): element
+// e = i * 32 + lane sits in register i of lane `lane`. Partners within a
+// lane's registers compare in place, partners across lanes through two 32-bit
+// shuffles; no block barrier. Keys in shared memory, read and written by the
+// calling warp only (the caller orders them with the other warps).
+template <int K>
+__device__ __forceinline__ void warp_sort_keys_reg(uint64_t* key, int n) {
+    const int lane = threadIdx.x & 31;
+    uint64_t r[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) r[i] = i * 32 + lane < n ? key[i * 32 + lane] : ~0ull;
+    constexpr int N = 32 * K;
+#pragma unroll
+    for (int size = 2; size <= N; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            if (stride >= 32) {   // partners in this lane's registers
+                const int rs = stride >> 5;
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    if (i & rs) continue;
+                    const int e = i * 32 + lane;
+                    const bool up = (e & size) == 0;
+                    const uint64_t a = r[i], b = r[i | rs];
+                    const bool sw = up ? (b < a) : (a < b);
+                    r[i] = sw ? b : a;
+                    r[i | rs] = sw ? a : b;
+                }
+            } else {              // partners in lane ^ stride
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    const int e = i * 32 + lane;
+                    const bool up = (e & size) == 0;
+                    const uint32_t lo = __shfl_xor_sync(0xffffffffu, static_cast<uint32_t>(r[i]), stride);
+                    const uint32_t hi = __shfl_xor_sync(0xffffffffu, static_cast<uint32_t>(r[i] >> 32), stride);
+                    const uint64_t o = (static_cast<uint64_t>(hi) << 32) | lo;
+                    const bool lower = (lane & stride) == 0;
+                    const bool take_min = lower == up;
+                    r[i] = take_min ? (o < r[i] ? o : r[i]) : (o > r[i] ? o : r[i]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < K; ++i)
+        if (i * 32 + lane < n) key[i * 32 + lane] = r[i];
+}
+
+// warp_sort_keys_reg for n <= 256 keys; false (nothing done) when n is larger.
+__device__ __forceinline__ bool warp_sort_keys(uint64_t* key, int n) {
+    if (n <= 32) warp_sort_keys_reg<1>(key, n);
+    else if (n <= 64) warp_sort_keys_reg<2>(key, n);
+    else if (n <= 128) warp_sort_keys_reg<4>(key, n);
+    else if (n <= 256) warp_sort_keys_reg<8>(key, n);
+    else return false;
+    __syncwarp();
+    return true;
+}
+
 __host__ __device__ __forceinline__ int next_pow2(int n) {
     int p = 1;
     while (p < n) p <<= 1;

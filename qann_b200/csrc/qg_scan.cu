@@ -740,14 +740,22 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
         }
         for (int i = lane; i < s_wcount[warp]; i += 32) gath[off + i] = wbuf[i];
         __syncthreads();
-        if (total > kp) {
-            if (warp == 0) warp_select_keep(gath, total, kp, hist);
-            __syncthreads();
-        }
         const int kept = min(total, kp);
-        const int ns = next_pow2(kept < 2 ? 2 : kept);
-        for (int i = kept + tid; i < ns; i += NT) gath[i] = ~0ull;
-        bitonic_sort_keys(gath, ns);
+        if (kept <= 256) {   // warp 0 alone cuts to k' and sorts in registers; one barrier
+            if (warp == 0) {
+                if (total > kp) warp_select_keep(gath, total, kp, hist);
+                warp_sort_keys(gath, kept);
+            }
+            __syncthreads();
+        } else {
+            if (total > kp) {
+                if (warp == 0) warp_select_keep(gath, total, kp, hist);
+                __syncthreads();
+            }
+            const int ns = next_pow2(kept);
+            for (int i = kept + tid; i < ns; i += NT) gath[i] = ~0ull;
+            bitonic_sort_keys(gath, ns);
+        }
         for (int i = tid; i < kp; i += NT) {
             if (i < kept) {
                 const uint64_t key = gath[i];

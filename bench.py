@@ -234,6 +234,25 @@ def measured_peak(key, fallback):
         return fallback, "fallback"
 
 
+def alu_roofline(alg_bytes, launch_ms, clocks, dev):
+    """The scan against the integer pipe: 4-bit lookups per second over the
+    peak rate of the lookup core. Every probed vector costs m lookups (m / 2
+    code bytes, so lookups = 2 x the algorithmic bytes). The core spends one
+    integer op per lookup (two byte permutes and one three-input add per four
+    lookups, and the 16-bit widening of the byte sums), and an SM issues 64
+    integer lane-ops per clock (32-bit add, logic, permute), so the peak is
+    SMs x 64 x the median SM clock sampled during the timed region."""
+    import torch
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    lookups = 2 * alg_bytes
+    achieved = lookups / (launch_ms / 1e3) / 1e12
+    peak = sms * 64 * mhz * 1e6 / 1e12
+    return {"bound": "integer pipe", "achieved": round(achieved, 3), "peak": round(peak, 3),
+            "unit": "T lookups/s", "frac": round(achieved / peak, 4), "lookups_per_launch": lookups,
+            "ops_per_lookup": 1.0, "sms": sms, "sm_mhz": mhz}
+
+
 def scan_traffic():
     """dram bytes per scan launch from the committed ncu summary, when present."""
     p = ROOT / "profiles" / "scan_traffic.txt"
@@ -1098,6 +1117,8 @@ def main():
             serving["served_over_fp32_ivf_batch"] = round(serving["best_qps_at_p99_le_2ms"] / ivf32, 2)
     cpu, cmp = (None, None) if (args.no_cpu_baseline or world > 1) else \
         reference_check(path, queries, k, op, ids_h, d_h)
+    clocks = clk.summary()
+    alu = alu_roofline(alg_bytes, per_launch_ms, clocks, dev)
     srt = sorted(step_ms)
     line = {
         "metric": METRIC,
@@ -1122,10 +1143,11 @@ def main():
                      "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": round(per_launch_ms, 4),
                      "note": "algorithmic bytes count every probed list's codes; the codes (33 MB) stay in L2 and "
                              "lists that cannot beat a query's bound are skipped, so this is not a DRAM rate"},
+        "alu_roofline": alu,
         "tensor_scan": tensor_scan,
         "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": nq * cfg["d"] * 4,
                 "d2h_bytes_per_step": nq * k * 12, "timing": "host wall clock around the blocking batch_query"},
-        "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "served": serving,
+        "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu, "served": serving,
     }
     print(json.dumps(line))
     if dist is not None:

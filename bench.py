@@ -684,7 +684,7 @@ def train_workload(args):
 def served_workload(args):
     """Served stream over a device-resident IVF-PQ fast-scan + refine index of
     5,000,000 x 128 (Gaussian mixture, 8,192 centres, sigma 0.2), nlist 16,384,
-    PQ 64 x 4-bit, k_factor 10: Poisson arrivals at 5k-200k queries/s, k in
+    PQ 64 x 4-bit, k_factor 10: Poisson arrivals at 5k-300k queries/s, k in
     {10, 100}, nprobe log-uniform in 8..256, 30% of requests with an allowed-id
     bitmap of selectivity uniform in [1%, 50%]; p50 / p99 latency per rate."""
     import torch
@@ -728,7 +728,7 @@ def served_workload(args):
         sel = rng.uniform(0.01, 0.5)
         bits = rng.random(n) < sel
         pool.append(bits)
-    rates = (5_000, 10_000, 20_000, 50_000, 100_000, 200_000)
+    rates = (5_000, 10_000, 20_000, 50_000, 100_000, 200_000, 300_000)
     out = []
     same = True
     with qb.Server(index, slots=4, max_batch=256, mem_budget=4 << 30) as srv:

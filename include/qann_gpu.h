@@ -266,7 +266,10 @@ int qg_get_option(const char* key, int64_t* value);
  * time, and only while the estimated device memory of all batches in flight
  * stays within mem_budget_bytes; 0 = 2 GiB) and search them as one mixed batch.
  * Each request has its own k, nprobe (<= 0: the index's) and filter, and gets
- * the results it gets searched alone (qg_search with that nprobe set).
+ * the results it gets searched alone (qg_search with that nprobe set). Over a
+ * RefineIndex, requests whose filter allows at most 6 * nlist slots (those the
+ * RefineIndex answers by its exact direct scan) queue apart and run on one
+ * extra worker thread, so that they never hold up the approximate batches.
  *
  * qg_server_add_filter registers a slot bitmap (deleted slots are masked out)
  *   that requests then name by filter_id.

@@ -455,7 +455,9 @@ class Server:
     stream each) take the oldest waiting requests as soon as they are free,
     up to max_batch at a time while the estimated device memory of all
     batches in flight fits mem_budget bytes, and search each batch as one
-    mixed batch. Every request gets the results it gets searched alone.
+    mixed batch. Every request gets the results it gets searched alone. Over
+    a RefineIndex, requests with a filter narrow enough for its exact direct
+    scan (at most 6 * nlist allowed ids) run on one extra worker of their own.
     """
 
     def __init__(self, index: DenseIndex, *, slots: int = 4, max_batch: int = 512, mem_budget: int = 2 << 30):

@@ -323,20 +323,28 @@ __global__ void k_cols_to_slots(uint32_t* __restrict__ cs, size_t n, const uint3
 // first pushed (lowest slot) among ties, then sorted by (distance, id).
 static void refine_direct(RefineObj& o, const Prepared& p, const SearchRequest& r, int dim, bool ip, bool cosine,
                           int64_t* out_ids, float* out_d, cudaStream_t st) {
-    std::vector<uint32_t> slots;
-    slots.reserve(r.filter->count);
-    for (size_t w = 0; w < r.filter->words.size(); ++w)
-        for (uint64_t bits = r.filter->words[w]; bits; bits &= bits - 1)
-            slots.push_back(static_cast<uint32_t>(w * 64 + __builtin_ctzll(bits)));
-    const size_t n = slots.size();
-    DevBuf<uint32_t> ds(n, st);
-    QG_CUDA(cudaMemcpyAsync(ds.get(), slots.data(), n * 4, cudaMemcpyHostToDevice, st));
+    // the allowed slots in ascending order: a server's registered filter keeps
+    // them on the device; otherwise they are listed from the bitmap here
+    DevBuf<uint32_t> ds;
+    const uint32_t* slots_dev = r.filter_slots_dev;
+    size_t n = r.filter->count;
+    if (!slots_dev) {
+        std::vector<uint32_t> slots;
+        slots.reserve(r.filter->count);
+        for (size_t w = 0; w < r.filter->words.size(); ++w)
+            for (uint64_t bits = r.filter->words[w]; bits; bits &= bits - 1)
+                slots.push_back(static_cast<uint32_t>(w * 64 + __builtin_ctzll(bits)));
+        n = slots.size();
+        ds.alloc(n, st);
+        QG_CUDA(cudaMemcpyAsync(ds.get(), slots.data(), n * 4, cudaMemcpyHostToDevice, st));
+        slots_dev = ds.get();
+    }
     DevBuf<float> rows(n * dim, st);
-    gather_rows(o.dev.ptr(), ds.get(), n, dim, rows.get(), st);
+    gather_rows(o.dev.ptr(), slots_dev, n, dim, rows.get(), st);
     DevBuf<uint64_t> ck(r.nq * r.k, st);
     DevBuf<uint32_t> cs(r.nq * r.k, st);
     flat_candidates(p.q.get(), r.nq, rows.get(), n, dim, ip, r.k, nullptr, nullptr, ck.get(), cs.get(), st);
-    k_cols_to_slots<<<static_cast<unsigned>(ceil_div(r.nq * r.k, 256)), 256, 0, st>>>(cs.get(), r.nq * r.k, ds.get());
+    k_cols_to_slots<<<static_cast<unsigned>(ceil_div(r.nq * r.k, 256)), 256, 0, st>>>(cs.get(), r.nq * r.k, slots_dev);
     QG_LAUNCH_CHECK();
     finalize_ivf(ck.get(), cs.get(), static_cast<int>(r.nq), static_cast<int>(r.k), static_cast<int>(r.k),
                  o.dev.labels.get(), cosine, out_ids, out_d, st);
@@ -689,35 +697,42 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
     // narrow filters of a RefineIndex (RefineIndex::use_direct): exact scans of
     // the allowed rows, one per (filter, k) among the batch's requests
     std::vector<std::pair<std::pair<const SlotBits*, int>, std::vector<size_t>>> direct;
+    std::vector<const uint32_t*> direct_slots;   // each group's filter's device slot list, or null
     for (size_t i = 0; i < nq; ++i) {
         const SlotBits* f = qs[i].filter;
         if (live == 0 || (f && f->count == 0)) continue;                      // nothing to return
         if (ref && f && f->count <= 6 * M.nlist) {
             const auto key = std::make_pair(f, qs[i].k);
             auto it = std::find_if(direct.begin(), direct.end(), [&](const auto& g) { return g.first == key; });
-            if (it == direct.end()) direct.push_back({key, {i}});
-            else it->second.push_back(i);
+            if (it == direct.end()) {
+                direct.push_back({key, {i}});
+                direct_slots.push_back(qs[i].filter_slots_dev);
+            } else {
+                it->second.push_back(i);
+            }
             continue;
         }
         batch.push_back(i);
     }
-    for (const auto& g : direct) {
+    for (size_t gi = 0; gi < direct.size(); ++gi) {
+        const auto& g = direct[gi];
         const size_t n = g.second.size(), k = static_cast<size_t>(g.first.second);
         std::vector<float> qh(n * dim);
         for (size_t j = 0; j < n; ++j) std::copy_n(q + g.second[j] * dim, dim, qh.data() + j * dim);
-        std::vector<int64_t> gi(n * k);
-        std::vector<float> gd(n * k);
+        std::vector<int64_t> hi(n * k);
+        std::vector<float> hd(n * k);
         SearchRequest r;
         r.q = qh.data();
         r.nq = n;
         r.k = k;
         r.filter = g.first.first;
-        r.out_ids = gi.data();
-        r.out_d = gd.data();
+        r.filter_slots_dev = direct_slots[gi];
+        r.out_ids = hi.data();
+        r.out_d = hd.data();
         search(idx, r, st);
         for (size_t j = 0; j < n; ++j) {
-            std::copy_n(gi.data() + j * k, k, out_ids + g.second[j] * kmax);
-            std::copy_n(gd.data() + j * k, k, out_d + g.second[j] * kmax);
+            std::copy_n(hi.data() + j * k, k, out_ids + g.second[j] * kmax);
+            std::copy_n(hd.data() + j * k, k, out_d + g.second[j] * kmax);
         }
     }
     if (batch.empty()) return;

@@ -24,6 +24,9 @@ struct SearchRequest {
     int nprobe = 0;                  // > 0: probes instead of the IVF index's nprobe
     bool capture = false;            // being captured into a CUDA graph: no host reads or waits
     int* err_dev = nullptr;          // caller-owned error flags (3 ints), read by the caller, or null
+    // the filter's allowed slots in ascending order on the device (filter->count
+    // of them), or null: RefineIndex direct scans then list them from the bitmap
+    const uint32_t* filter_slots_dev = nullptr;
 };
 
 // Runs a batch query on `st` and, for host I/O, waits for it.
@@ -58,6 +61,7 @@ struct MixedQuery {
     const SlotBits* filter = nullptr;   // allowed slots, or null
     const uint64_t* filter_dev = nullptr;   // the same bitmap already on the device (a server's
                                             // registered filter), or null: uploaded per batch
+    const uint32_t* filter_slots_dev = nullptr;   // its allowed slots, ascending, on the device, or null
 };
 
 // A batch of queries that differ in k, nprobe and filter (host rows q, nq x

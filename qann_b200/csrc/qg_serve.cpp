@@ -11,7 +11,10 @@
 // search (search_mixed: one coarse step, one scan and one re-rank for all of
 // it), so requests that arrive while others are on the GPU start as soon as a
 // slot frees, and batches on different slots overlap on the device. Each
-// request's results are the ones it gets searched alone.
+// request's results are the ones it gets searched alone. Over a RefineIndex,
+// requests whose filter is narrow enough for its exact direct scan (at most
+// 6 * nlist allowed slots) queue in a lane of their own with one more worker,
+// so that approximate batches never wait for those scans.
 #include "../../include/qann_gpu.h"
 
 #include "qg_index.h"
@@ -64,7 +67,9 @@ public:
             m_ = M.pq.m;
         }
         if (idx_->kind == Kind::Refine) k_factor_ = static_cast<RefineObj&>(*idx_).k_factor;
-        for (int s = 0; s < slots; ++s) workers_.emplace_back([this] { worker(); });
+        direct_lane_ = idx_->kind == Kind::Refine && nlist_ > 0;
+        for (int s = 0; s < slots; ++s) workers_.emplace_back([this] { worker(0); });
+        if (direct_lane_) workers_.emplace_back([this] { worker(1); });
     }
 
     ~Server() {
@@ -72,7 +77,7 @@ public:
             std::lock_guard<std::mutex> g(mu_);
             stop_ = true;
         }
-        cv_in_.notify_all();
+        for (auto& cv : cv_in_) cv.notify_all();
         for (auto& t : workers_) t.join();
         std::unique_lock<std::mutex> lk(mu_);
         for (auto& [id, r] : reqs_)
@@ -93,7 +98,10 @@ public:
 
     // A registered filter is uploaded once, here, and its device copy serves
     // every batch that uses it (without a usable device, batches upload the
-    // bitmap themselves, as for unregistered filters).
+    // bitmap themselves, as for unregistered filters). A filter narrow enough
+    // for a RefineIndex's direct scan (at most 6 * nlist allowed slots) also
+    // keeps its allowed slots, ascending, on the device, so that the scan
+    // need not list them from the bitmap on every batch.
     int add_filter(std::shared_ptr<const SlotBits> f) {
         auto reg = std::make_shared<Registered>();
         try {
@@ -101,9 +109,22 @@ public:
             reg->dev.alloc(std::max<size_t>(1, f->words.size()), st);
             QG_CUDA(cudaMemcpyAsync(reg->dev.get(), f->words.data(), f->words.size() * sizeof(uint64_t),
                                     cudaMemcpyHostToDevice, st));
+            std::vector<uint32_t> slots;
+            if (idx_->kind == Kind::Refine && nlist_ > 0 && f->count > 0 && f->count <= 6 * nlist_) {
+                slots.reserve(f->count);
+                for (size_t w = 0; w < f->words.size(); ++w)
+                    for (uint64_t bits = f->words[w]; bits; bits &= bits - 1)
+                        slots.push_back(static_cast<uint32_t>(w * 64 + __builtin_ctzll(bits)));
+                if (slots.size() == f->count) {
+                    reg->slots.alloc(slots.size(), st);
+                    QG_CUDA(cudaMemcpyAsync(reg->slots.get(), slots.data(), slots.size() * 4, cudaMemcpyHostToDevice,
+                                            st));
+                }
+            }
             QG_CUDA(cudaStreamSynchronize(st));
         } catch (const Error&) {
             reg->dev = DevBuf<uint64_t>{};
+            reg->slots = DevBuf<uint32_t>{};
             (void)cudaGetLastError();
         }
         reg->bits = std::move(f);
@@ -113,9 +134,10 @@ public:
     }
     std::shared_ptr<const SlotBits> filter(int id) { return registered(id)->bits; }
     const uint64_t* filter_dev(int id) { return registered(id)->dev.get(); }
+    const uint32_t* filter_slots(int id) { return registered(id)->slots.get(); }
 
     uint64_t submit(const float* q, int k, int nprobe, std::shared_ptr<const SlotBits> f, double t_arrive,
-                    const uint64_t* f_dev = nullptr) {
+                    const uint64_t* f_dev = nullptr, const uint32_t* f_slots = nullptr) {
         require(k >= 1, "k must be at least 1");
         require(nprobe <= 0 || nlist_ == 0 || static_cast<size_t>(nprobe) <= nlist_, "nprobe must be <= nlist");
         const size_t d = dim();
@@ -128,13 +150,19 @@ public:
         r->filter = std::move(f);
         r->mq.filter = r->filter.get();
         r->mq.filter_dev = r->filter ? f_dev : nullptr;
+        r->mq.filter_slots_dev = r->filter ? f_slots : nullptr;
         r->t_arrive = t_arrive;
         r->bytes = footprint(*r);
+        const size_t r_filter_count = r->filter ? r->filter->count : SIZE_MAX;
         std::lock_guard<std::mutex> g(mu_);
         const uint64_t id = next_++;
         reqs_.emplace(id, std::move(r));
-        queue_.push_back(id);
-        cv_in_.notify_one();
+        // narrow filters of a RefineIndex over IVF take the exact direct scan
+        // (RefineIndex::use_direct): their own lane and worker, so that a
+        // batch of approximate searches never waits for one
+        const int lane = direct_lane_ && r_filter_count <= 6 * nlist_ && r_filter_count > 0 ? 1 : 0;
+        queue_[lane].push_back(id);
+        cv_in_[lane].notify_one();
         return id;
     }
 
@@ -173,6 +201,7 @@ private:
     struct Registered {
         std::shared_ptr<const SlotBits> bits;
         DevBuf<uint64_t> dev;
+        DevBuf<uint32_t> slots;   // narrow filters of a RefineIndex: the allowed slots, ascending
     };
     std::shared_ptr<Registered> registered(int id) {
         std::lock_guard<std::mutex> g(mu_);
@@ -194,7 +223,8 @@ private:
         return b;
     }
 
-    void worker() {
+    // lane 0: every request but the narrow-filter ones; lane 1: those (see submit)
+    void worker(int lane) {
         cudaStream_t st = nullptr;
         if (cudaSetDevice(idx_->device) != cudaSuccess ||
             cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
@@ -211,17 +241,18 @@ private:
             size_t bytes = 0;
             {
                 std::unique_lock<std::mutex> lk(mu_);
-                cv_in_.wait(lk, [&] {
-                    return stop_ || (!queue_.empty() &&
-                                     (in_flight_ == 0 || in_flight_ + reqs_.at(queue_.front())->bytes <= budget_));
+                std::deque<uint64_t>& queue = queue_[lane];
+                cv_in_[lane].wait(lk, [&] {
+                    return stop_ || (!queue.empty() &&
+                                     (in_flight_ == 0 || in_flight_ + reqs_.at(queue.front())->bytes <= budget_));
                 });
                 if (stop_) break;
-                while (!queue_.empty() && b.size() < static_cast<size_t>(max_batch_)) {
-                    ServeRequest* r = reqs_.at(queue_.front()).get();
+                while (!queue.empty() && b.size() < static_cast<size_t>(max_batch_)) {
+                    ServeRequest* r = reqs_.at(queue.front()).get();
                     if ((in_flight_ > 0 || !b.empty()) && in_flight_ + bytes + r->bytes > budget_) break;
                     b.push_back(r);
                     bytes += r->bytes;
-                    queue_.pop_front();
+                    queue.pop_front();
                 }
                 in_flight_ += bytes;
                 peak_ = std::max(peak_, in_flight_);
@@ -269,7 +300,7 @@ private:
                 ++batches_;
             }
             cv_out_.notify_all();
-            cv_in_.notify_all();
+            for (auto& cv : cv_in_) cv.notify_all();
         }
         if (st) cudaStreamDestroy(st);
     }
@@ -279,8 +310,9 @@ private:
     size_t budget_;
     size_t nlist_ = 0, nprobe_ = 0, m_ = 0, k_factor_ = 1;
     std::mutex mu_;
-    std::condition_variable cv_in_, cv_out_;
-    std::deque<uint64_t> queue_;
+    std::condition_variable cv_in_[2], cv_out_;
+    std::deque<uint64_t> queue_[2];   // the lanes (see worker)
+    bool direct_lane_ = false;
     std::unordered_map<uint64_t, std::unique_ptr<ServeRequest>> reqs_;
     std::vector<std::shared_ptr<Registered>> filters_;
     uint64_t next_ = 1;
@@ -361,11 +393,13 @@ int qg_server_submit(qg_server* s, const float* q, size_t k, int nprobe, const i
             f = std::make_shared<SlotBits>(v.index().idmap().filter({allowed, n_allowed}));
         }
         const uint64_t* f_dev = nullptr;
+        const uint32_t* f_slots = nullptr;
         if (!allowed && filter_id >= 0) {
             f = v.filter(filter_id);
             f_dev = v.filter_dev(filter_id);
+            f_slots = v.filter_slots(filter_id);
         }
-        *ticket = v.submit(q, static_cast<int>(k), nprobe, std::move(f), now_us(), f_dev);
+        *ticket = v.submit(q, static_cast<int>(k), nprobe, std::move(f), now_us(), f_dev, f_slots);
     });
 }
 
@@ -383,10 +417,12 @@ int qg_server_replay(qg_server* s, const float* q, size_t nq, const int32_t* k, 
         for (size_t i = 0; i < nq; ++i) require(k[i] >= 1 && static_cast<size_t>(k[i]) <= kmax, "k out of range");
         std::vector<std::shared_ptr<const SlotBits>> fs(nq);
         std::vector<const uint64_t*> fdev(nq, nullptr);
+        std::vector<const uint32_t*> fslots(nq, nullptr);
         for (size_t i = 0; i < nq; ++i)
             if (filter_id && filter_id[i] >= 0) {
                 fs[i] = v.filter(filter_id[i]);
                 fdev[i] = v.filter_dev(filter_id[i]);
+                fslots[i] = v.filter_slots(filter_id[i]);
             }
         std::vector<uint64_t> tickets(nq);
         // open loop: request i enters at t0 + arrival_us[i] whatever the state
@@ -397,7 +433,7 @@ int qg_server_replay(qg_server* s, const float* q, size_t nq, const int32_t* k, 
             for (double t = now_us(); t < due; t = now_us()) {
                 if (due - t > 300.0) std::this_thread::sleep_for(std::chrono::microseconds(static_cast<int64_t>(due - t - 200.0)));
             }
-            tickets[i] = v.submit(q + i * d, k[i], nprobe ? nprobe[i] : 0, fs[i], due, fdev[i]);
+            tickets[i] = v.submit(q + i * d, k[i], nprobe ? nprobe[i] : 0, fs[i], due, fdev[i], fslots[i]);
         }
         std::vector<int64_t> ids(kmax);
         std::vector<float> dd(kmax);

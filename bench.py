@@ -763,7 +763,9 @@ def served_workload(args):
         for ri, rate in enumerate(rates):
             arrivals = np.cumsum(arng.exponential(1.0 / rate, size=nreq))
             t = time.perf_counter()
-            ids, _, lat = srv.replay(q, ks, arrivals, nprobes=npb, filter_ids=fid)
+            ids, dists, lat = srv.replay(q, ks, arrivals, nprobes=npb, filter_ids=fid)
+            if ri == 0:
+                err64 = fp64_error_l2(x, q, ids, dists)
             wall = time.perf_counter() - t
             lat_ms = np.sort(lat) * 1e3
             span = float(np.max(arrivals + lat))   # arrival schedule start to the last result
@@ -819,6 +821,7 @@ def served_workload(args):
                    "k": [10, 100], "nprobe": "log-uniform 8..256", "filtered": 0.3, "selectivity": [0.01, 0.5],
                    "slots": 4, "max_batch": 256},
         "rates": out, "results_equal_solo_searches": same, "mean_batch": round(st["completed"] / st["batches"], 1),
+        "rel_err_vs_fp64": err64,
         "at_lowest_rate": {"kernel_ms_per_batch": kernel_per_batch}, "one_at_a_time": solo,
         "plain_fp32_gpu_flat_qps": round(fp32_qps, 1),
         "fp32_ivf_batch_qps": {"qps": round(fp32_ivf, 1), "nq": 10_000, "k": 10, "nprobe": 64,
@@ -921,6 +924,20 @@ def fp64_error(base, queries, ids, dists, sample=2000):
     err = np.abs(dists[:s].astype(np.float64) - d64) / np.maximum(np.abs(d64), 1e-30)
     return {"max": float(err.max()), "mean": float(err.mean()), "sample": f"{s} queries x {ids.shape[1]} results",
             "fp64": "0.5 * |q/|q| - x/|x||^2 of the raw rows"}
+
+
+def fp64_error_l2(base, queries, ids, dists, sample=2000):
+    """Relative error of served squared-L2 distances against FP64 over the
+    first `sample` requests' results (ids of -1 past a request's own k are
+    skipped)."""
+    s = min(sample, queries.shape[0])
+    ok = ids[:s] >= 0
+    qi = np.nonzero(ok)[0]
+    x = base[ids[:s][ok]].astype(np.float64)
+    d64 = ((queries[:s].astype(np.float64)[qi] - x) ** 2).sum(-1)
+    err = np.abs(dists[:s][ok].astype(np.float64) - d64) / np.maximum(np.abs(d64), 1e-30)
+    return {"max": float(err.max()), "mean": float(err.mean()), "sample": f"{int(ok.sum())} results of {s} requests",
+            "fp64": "|q - x|^2 of the raw rows"}
 
 
 def index_matches_reference_build(path, cfg):

@@ -195,6 +195,46 @@ __device__ __forceinline__ float exact_avx2_vec(const float* __restrict__ a, con
     return exact_tail<kL2>(a, b, n8, n, r);
 }
 
+// exact_avx2 of one row by the 4 lanes of an aligned lane group: lane h runs
+// AVX2 lanes 2h and 2h + 1 (their four FMA chains, packed, over one 8-byte load
+// of a and of b per step), so each step of the group reads one 32-byte sector
+// of b. Lanes h and h ^ 2 add their lane sums pairwise and lanes h and h ^ 1
+// add those, which is exact_avx2's tree ((s0 + s4) + (s1 + s5)) + ((s2 + s6) +
+// (s3 + s7)) (float addition of two operands is commutative, so every lane
+// ends with the same bits); every lane adds the tail. All 32 lanes of the warp
+// call it together. a and b 8-byte aligned, n even; a in any address space, b
+// global memory read through the read-only path.
+template <bool kL2>
+__device__ __forceinline__ float exact_avx2_group4(const float* a, const float* __restrict__ b, int n) {
+    const int h = threadIdx.x & 3;
+    const int n32 = n & ~31, n8 = n & ~7;
+    float2 acc[4];   // accumulator j of AVX2 lanes 2h and 2h + 1
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[j] = make_float2(0.f, 0.f);
+    auto step = [&](int e, int j) {
+        const float2 x = *reinterpret_cast<const float2*>(a + e);
+        const float2 y = __ldg(reinterpret_cast<const float2*>(b + e));
+        if (kL2) {
+            const float2 dv = sub2(x, y);
+            acc[j] = __ffma2_rn(dv, dv, acc[j]);
+        } else {
+            acc[j] = __ffma2_rn(x, y, acc[j]);
+        }
+    };
+    int i = 0;
+    for (; i < n32; i += 32) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) step(i + 8 * j + 2 * h, j);
+    }
+    for (; i < n8; i += 8) step(i + 2 * h, 0);   // 8-float steps into accumulator 0
+    const float s0 = __fadd_rn(__fadd_rn(acc[0].x, acc[1].x), __fadd_rn(acc[2].x, acc[3].x));   // AVX2 lane 2h
+    const float s1 = __fadd_rn(__fadd_rn(acc[0].y, acc[1].y), __fadd_rn(acc[2].y, acc[3].y));   // AVX2 lane 2h + 1
+    const float o0 = __shfl_xor_sync(0xffffffffu, s0, 2, 4), o1 = __shfl_xor_sync(0xffffffffu, s1, 2, 4);
+    const float u = __fadd_rn(__fadd_rn(s0, o0), __fadd_rn(s1, o1));
+    const float r = __fadd_rn(u, __shfl_xor_sync(0xffffffffu, u, 1, 4));
+    return exact_tail<kL2>(a, b, n8, n, r);
+}
+
 // exact_avx2 of one row by the 8 lanes of an aligned lane group: lane L of the
 // group runs AVX2 lane L's four FMA chains (elements i + 8 j + L), the groups'
 // lane sums meet in exact_avx2's tree order through shuffles, and every lane

@@ -481,12 +481,19 @@ static void mm_topk_block(const float* q, size_t nq, const float* rows, const Mm
                                                                                             xterm.get());
     QG_LAUNCH_CHECK();
 
-    // seed: the exact top-k of the first rows
-    const size_t seed = std::min(n, std::max<size_t>(4096, 4 * k));
+    // seed: the exact top-k of the first rows, which gives the first filter
+    // chunk its threshold. The exact tiles run far below the tensor cores, so
+    // the seed is a small share of the rows: 1/64 of them, at least 256 (and
+    // 4k) and at most 4,096 (and 4k). Nearest-centroid assignment against
+    // 4,096 to 16,384 centroids otherwise spends most of its time here.
+    const size_t seed_lo = std::max<size_t>(256, 4 * k), seed_hi = std::max<size_t>(4096, 4 * k);
+    const size_t seed = std::min(n, std::clamp<size_t>(n / 64, seed_lo, seed_hi));
     flat_candidates(q, nq, rows, seed, d, ip, k, allow, deny, out_key, out_slot, st, /*allow_mm=*/false);
     if (seed == n) return;
 
     const int cap = static_cast<int>(std::clamp<size_t>(4 * k, 1024, 4096));
+    // chunks grow 4x while about 3k new rows pass per chunk stay well under the cap, else 2x
+    const size_t growth = 12 * k <= static_cast<size_t>(cap) ? 4 : 2;
     DevBuf<uint32_t> cnt(nq, st), crow(nq * static_cast<size_t>(cap), st);
     DevBuf<int> ovf(nq, st), err(1, st);
     QG_CUDA(cudaMemsetAsync(ovf.get(), 0, nq * sizeof(int), st));
@@ -515,7 +522,7 @@ static void mm_topk_block(const float* q, size_t nq, const float* rows, const Mm
     a.cand_row = crow.get();
     a.cap = cap;
     a.err = err.get();
-    size_t n0 = seed, chunk = seed;
+    size_t n0 = seed, chunk = (growth - 1) * seed;
     while (n0 < n) {
         const size_t n1 = std::min(n, n0 + chunk);
         k_mm_thresholds<<<static_cast<unsigned>(ceil_div(nq, 256)), 256, 0, st>>>(out_key, static_cast<int>(nq),
@@ -537,7 +544,7 @@ static void mm_topk_block(const float* q, size_t nq, const float* rows, const Mm
                                                                       ovf.get());
         QG_LAUNCH_CHECK();
         n0 = n1;
-        chunk = std::min<size_t>(chunk * 2, size_t{1} << 21);
+        chunk = std::min<size_t>(n0 * (growth - 1), size_t{1} << 21);
     }
     int herr = 0;
     std::vector<int> hovf(nq);
@@ -620,6 +627,41 @@ __device__ uint32_t block_threshold_u32(const uint32_t* keys, int n, int k, uint
 // x * 2^e), ldexpf itself otherwise.
 __device__ __forceinline__ float scale_pow2(float x, int e) {
     return (e >= -126 && e <= 127) ? __fmul_rn(x, __int_as_float((e + 127) << 23)) : ldexpf(x, e);
+}
+
+// The P smallest of the cnt distinct keys key[0, cnt) written in order, key by
+// key, for P <= cnt <= 32 K x warps: each warp sorts a run of up to 32 K keys
+// in registers; a key's rank is then the number of keys below it in each run
+// (binary searches over the sorted runs; its own run counts its place in it),
+// and a key of rank < P goes to place rank. One block barrier.
+template <int K>
+__device__ void ranked_out(uint64_t* key, int cnt, int P, const float* score_of, uint32_t* probe_q, float* pdist_q) {
+    constexpr int R = 32 * K;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int n_w = max(0, min(R, cnt - R * warp));
+    if (n_w > 0) warp_sort_keys_reg<K>(key + R * warp, n_w);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        const int e = R * warp + i * 32 + lane;
+        if (e >= cnt) continue;
+        const uint64_t k = key[e];
+        int rank = 0;
+        for (int w = 0; w < nw; ++w) {
+            const int len = max(0, min(R, cnt - R * w));
+            const uint64_t* run = key + R * w;
+            int pos = 0;   // keys of the run below k
+#pragma unroll
+            for (int step = R; step > 0; step >>= 1)
+                if (pos + step <= len && run[pos + step - 1] < k) pos += step;
+            rank += pos;
+        }
+        if (rank < P) {
+            const uint32_t j = static_cast<uint32_t>(k);
+            probe_q[rank] = j;
+            pdist_q[rank] = score_of[j];
+        }
+    }
 }
 
 __global__ void __launch_bounds__(256, 6) k_coarse_recheck(const float* __restrict__ q, const float* __restrict__ q2,
@@ -734,7 +776,23 @@ __global__ void __launch_bounds__(256, 6) k_coarse_recheck(const float* __restri
     // exact scores, one candidate per 8-lane group; each list's score is kept
     // by list (over its upper bound, no longer needed) for the output
     float* score_of = reinterpret_cast<float*>(ub);
-    {
+    if ((d & 1) == 0 && (reinterpret_cast<uintptr_t>(cent) & 7) == 0) {
+        // rows 8-byte aligned: one candidate per 4-lane group, one 32-byte
+        // sector of its row per step
+        const int ngrp = blockDim.x >> 2, grp = threadIdx.x >> 2;
+        const int rounds = (cnt + ngrp - 1) / ngrp;   // (block-uniform)
+        for (int rd = 0; rd < rounds; ++rd) {
+            const int i = rd * ngrp + grp;
+            const bool act = i < cnt;
+            const int j = act ? static_cast<int>(ckey[i]) : 0;   // idle groups score row 0 unused
+            const float* row = cent + static_cast<size_t>(j) * d;
+            const float sc = ip ? -exact_avx2_group4<false>(qv, row, d) : exact_avx2_group4<true>(qv, row, d);
+            if (act && (threadIdx.x & 3) == 0) {
+                ckey[i] = (static_cast<uint64_t>(float_key_eq0(sc)) << 32) | static_cast<uint32_t>(j);
+                score_of[j] = sc;
+            }
+        }
+    } else {
         const int ngrp = blockDim.x >> 3, grp = threadIdx.x >> 3;
         const int rounds = (cnt + ngrp - 1) / ngrp;   // (block-uniform)
         for (int rd = 0; rd < rounds; ++rd) {
@@ -750,7 +808,15 @@ __global__ void __launch_bounds__(256, 6) k_coarse_recheck(const float* __restri
         }
     }
     __syncthreads();
-    // the P smallest by (score, list), then sorted
+    // the P smallest by (score, list), in order
+    if (cnt <= 32 * (static_cast<int>(blockDim.x) >> 5)) {
+        ranked_out<1>(ckey, cnt, P, score_of, probe + static_cast<size_t>(qi) * P, pdist + static_cast<size_t>(qi) * P);
+        return;
+    }
+    if (cnt <= 64 * (static_cast<int>(blockDim.x) >> 5)) {
+        ranked_out<2>(ckey, cnt, P, score_of, probe + static_cast<size_t>(qi) * P, pdist + static_cast<size_t>(qi) * P);
+        return;
+    }
     if (cnt > P) {
         if (threadIdx.x < 32) warp_select_keep(ckey, cnt, P, hist);
         __syncthreads();

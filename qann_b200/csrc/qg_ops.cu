@@ -69,8 +69,14 @@ static void flat_candidates_fp32(const float* q_dev, size_t nq, const float* row
     QG_CUDA(cudaMemsetAsync(out_key, 0xFF, nq * k * sizeof(uint64_t), st));
     QG_CUDA(cudaMemsetAsync(out_slot, 0xFF, nq * k * sizeof(uint32_t), st));
     if (n == 0) return;
-    const size_t QB = std::min<size_t>(nq, 4096);
+    size_t QB = std::min<size_t>(nq, 4096);
     const size_t T = std::min<size_t>(n, std::max<size_t>(k, (size_t{256} << 20) / (QB * sizeof(float))));
+    // a short row range (a seed of a few hundred rows) takes larger query
+    // blocks in the same 256 MB of scores and of per-query keys (at most
+    // 65,536 queries: 4,096 tile rows)
+    const size_t big = std::min<size_t>({size_t{65536}, (size_t{256} << 20) / (T * sizeof(float)),
+                                         (size_t{256} << 20) / (k * 16)});
+    QB = std::min<size_t>(nq, std::max<size_t>(QB, big));
     DevBuf<float> scores(QB * T, st);
     DevBuf<uint32_t> col(QB * std::min(k, T), st);
     DevBuf<float> sc(QB * std::min(k, T), st);

@@ -382,7 +382,7 @@ def reference_arm(args, cfg):
 def served(index, queries, k, nprobe, batch_ids,
            rates=(25_000, 50_000, 100_000, 200_000, 225_000, 250_000, 275_000, 300_000, 350_000, 400_000, 450_000,
                   500_000, 600_000),
-           per_rate=20_000, slots=4, max_batch=256):
+           per_rate=20_000, slots=2, max_batch=512):
     """Open-loop Poisson arrivals through the continuous-batching server:
     achieved QPS and p50 / p99 latency (arrival to results) per offered rate;
     every served result must equal the batch path's."""

@@ -286,14 +286,14 @@ __global__ void k_ema_move(float* __restrict__ pos, float* __restrict__ mass, co
     if (lane == 0) mass[j] = grown;
 }
 
-__global__ void k_pass_accumulate(float* __restrict__ pass_sums, uint32_t* __restrict__ pass_counts,
+__global__ void k_pass_accumulate(float* __restrict__ close_sum, uint32_t* __restrict__ close_cnt,
                                   const float* __restrict__ sums, const uint32_t* __restrict__ off, int k, int d) {
     const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= static_cast<size_t>(k) * d) return;
-    pass_sums[t] = __fadd_rn(pass_sums[t], sums[t]);
+    close_sum[t] = __fadd_rn(close_sum[t], sums[t]);
     if (t % d == 0) {
         const size_t j = t / d;
-        pass_counts[j] += off[j + 1] - off[j];
+        close_cnt[j] += off[j + 1] - off[j];
     }
 }
 
@@ -328,12 +328,12 @@ __global__ void k_split_into(float* __restrict__ pos, float* __restrict__ mass, 
 }
 
 // closing: clusters with points in the last pass move to their mean
-__global__ void k_pass_close(float* __restrict__ pos, const float* __restrict__ pass_sums,
-                             const uint32_t* __restrict__ pass_counts, int k, int d) {
+__global__ void k_pass_close(float* __restrict__ pos, const float* __restrict__ close_sum,
+                             const uint32_t* __restrict__ close_cnt, int k, int d) {
     const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= static_cast<size_t>(k) * d) return;
-    const uint32_t cnt = pass_counts[t / d];
-    if (cnt > 0) pos[t] = __fdiv_rn(pass_sums[t], __uint2float_rn(cnt));
+    const uint32_t cnt = close_cnt[t / d];
+    if (cnt > 0) pos[t] = __fdiv_rn(close_sum[t], __uint2float_rn(cnt));
 }
 
 __global__ void k_fill_f32(float* __restrict__ a, size_t n, float v) {
@@ -347,18 +347,18 @@ void EMeansState::init(int k_, int d_, cudaStream_t st) {
     const size_t kd = static_cast<size_t>(k) * d;
     pos.alloc(kd, st);
     mass.alloc(k, st);
-    pass_sums.alloc(kd, st);
-    pass_counts.alloc(k, st);
+    close_sum.alloc(kd, st);
+    close_cnt.alloc(k, st);
     k_fill_f32<<<static_cast<unsigned>(ceil_div(k, 256)), 256, 0, st>>>(mass.get(), k, 1.0f / 65536.0f);
     QG_LAUNCH_CHECK();
-    QG_CUDA(cudaMemsetAsync(pass_sums.get(), 0, kd * sizeof(float), st));
-    QG_CUDA(cudaMemsetAsync(pass_counts.get(), 0, k * sizeof(uint32_t), st));
+    QG_CUDA(cudaMemsetAsync(close_sum.get(), 0, kd * sizeof(float), st));
+    QG_CUDA(cudaMemsetAsync(close_cnt.get(), 0, k * sizeof(uint32_t), st));
 }
 
 void EMeansState::step(const float* sums, const uint32_t* off, double alpha, bool accumulate, cudaStream_t st) {
     const size_t kd = static_cast<size_t>(k) * d;
     if (accumulate) {
-        k_pass_accumulate<<<static_cast<unsigned>(ceil_div(kd, 256)), 256, 0, st>>>(pass_sums.get(), pass_counts.get(),
+        k_pass_accumulate<<<static_cast<unsigned>(ceil_div(kd, 256)), 256, 0, st>>>(close_sum.get(), close_cnt.get(),
                                                                                      sums, off, k, d);
         QG_LAUNCH_CHECK();
     }
@@ -385,8 +385,8 @@ void EMeansState::split(const std::vector<uint32_t>& pairs, cudaStream_t st) {
 
 void EMeansState::close(cudaStream_t st) {
     const size_t kd = static_cast<size_t>(k) * d;
-    k_pass_close<<<static_cast<unsigned>(ceil_div(kd, 256)), 256, 0, st>>>(pos.get(), pass_sums.get(),
-                                                                          pass_counts.get(), k, d);
+    k_pass_close<<<static_cast<unsigned>(ceil_div(kd, 256)), 256, 0, st>>>(pos.get(), close_sum.get(),
+                                                                          close_cnt.get(), k, d);
     QG_LAUNCH_CHECK();
 }
 

@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_mm_filter(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, MmArgs a) {
     using namespace sm100;
     extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(16) float s_xt[kEpiWarps][32];   // epilogue: each warp's current run of row terms
     uint8_t* base = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const uint32_t a_bytes = static_cast<uint32_t>(a.kblocks) * BM * 128;
     const uint32_t b_bytes = static_cast<uint32_t>(a.kblocks) * BN * 128;
@@ -258,13 +259,32 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     continue;
                 }
-                const float xt = r0 + lane < a.n1 ? a.xterm[r0 + lane] : 0.0f;
+                // the run's row terms, staged for broadcast reads
+                float* sx = s_xt[ew];
+                __syncwarp();   // the previous run's reads are done
+                sx[lane] = r0 + lane < a.n1 ? a.xterm[r0 + lane] : 0.0f;
+                __syncwarp();
+                // the smallest lb of this lane's run: when it is above thr, no
+                // row of the run passes, and the element loop runs only when
+                // some lane's run may hold one
+                float lbmin = __int_as_float(0x7f800000);
+#pragma unroll
+                for (int j = 0; j < 32; j += 4) {
+                    const float4 x4 = *reinterpret_cast<const float4*>(sx + j);
+                    const float l0 = __fmaf_rn(-a.mult, __uint_as_float(v[j]), x4.x);
+                    const float l1 = __fmaf_rn(-a.mult, __uint_as_float(v[j + 1]), x4.y);
+                    const float l2 = __fmaf_rn(-a.mult, __uint_as_float(v[j + 2]), x4.z);
+                    const float l3 = __fmaf_rn(-a.mult, __uint_as_float(v[j + 3]), x4.w);
+                    lbmin = fminf(lbmin, fminf(fminf(l0, l1), fminf(l2, l3)));
+                }
+                const bool maybe = live && lbmin <= thr;
+                if (!__any_sync(0xffffffffu, maybe)) continue;
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
-                    const float xj = __shfl_sync(0xffffffffu, xt, j);
+                    const float xj = sx[j];
                     const int row = r0 + j;
                     const float lb = __fmaf_rn(-a.mult, __uint_as_float(v[j]), xj);
-                    if (live && row < a.n1 && lb <= thr) {
+                    if (maybe && row < a.n1 && lb <= thr) {
                         const bool allowed = (!a.allow || ((a.allow[row >> 6] >> (row & 63)) & 1ull)) &&
                                              (!a.deny || !((a.deny[row >> 6] >> (row & 63)) & 1ull));
                         if (allowed) {
@@ -396,6 +416,56 @@ __global__ void __launch_bounds__(256) k_mm_merge(const float* __restrict__ q, i
     }
 }
 
+// k_mm_merge for k <= 24 and rows with an even dim at 8-byte alignment: one
+// warp per query (8 per block). Candidates go in rounds of 8, scored exactly
+// by 4-lane groups (exact_avx2_group4, the same bits as exact_score); lanes
+// 0..k-1 hold the running top-k keys, lanes k..k+7 the round's, and one
+// register sort of the 32 keys keeps the k smallest in lanes 0..k-1.
+__global__ void __launch_bounds__(256) k_mm_merge_warp(const float* __restrict__ q, int d, const float* __restrict__ rows,
+                                                       bool ip, int k, int nq, int cap,
+                                                       const uint32_t* __restrict__ cand_count,
+                                                       const uint32_t* __restrict__ cand_row,
+                                                       uint64_t* __restrict__ run_key, uint32_t* __restrict__ run_slot,
+                                                       int* __restrict__ overflow) {
+    extern __shared__ __align__(16) uint8_t sm_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qi = blockIdx.x * 8 + warp;
+    if (qi >= nq) return;
+    uint32_t cnt = cand_count[qi];
+    if (cnt == 0) return;
+    if (cnt > static_cast<uint32_t>(cap)) {
+        if (lane == 0) overflow[qi] = 1;
+        cnt = cap;
+    }
+    const int dp = (d + 3) & ~3;
+    float* qv = reinterpret_cast<float*>(sm_raw) + warp * dp;
+    uint64_t* keys = reinterpret_cast<uint64_t*>(reinterpret_cast<float*>(sm_raw) + 8 * dp) + warp * 32;
+    for (int t = lane; t < d; t += 32) qv[t] = q[static_cast<size_t>(qi) * d + t];
+    uint64_t mine = lane < k ? run_key[static_cast<size_t>(qi) * k + lane] : ~0ull;
+    __syncwarp();
+    const uint32_t* cq = cand_row + static_cast<size_t>(qi) * cap;
+    const int grp = lane >> 2;
+    for (uint32_t c0 = 0; c0 < cnt; c0 += 8) {
+        const uint32_t i = c0 + grp;
+        const bool act = i < cnt;
+        const uint32_t row = act ? cq[i] : 0u;   // idle groups score row 0 unused
+        const float* rp = rows + static_cast<size_t>(row) * d;
+        const float s = ip ? -exact_avx2_group4<false>(qv, rp, d) : exact_avx2_group4<true>(qv, rp, d);
+        const uint64_t key = act ? (static_cast<uint64_t>(float_key_eq0(s)) << 32) | row : ~0ull;
+        // group g's key to lane k + g
+        const uint64_t got = __shfl_sync(0xffffffffu, key, 4 * ((lane - k) & 7));
+        keys[lane] = lane < k ? mine : (lane < k + 8 ? got : ~0ull);
+        __syncwarp();
+        warp_sort_keys_reg<1>(keys, 32);
+        __syncwarp();
+        mine = lane < k ? keys[lane] : ~0ull;
+    }
+    if (lane < k) {
+        run_key[static_cast<size_t>(qi) * k + lane] = mine;
+        run_slot[static_cast<size_t>(qi) * k + lane] = mine == ~0ull ? 0xFFFFFFFFu : static_cast<uint32_t>(mine);
+    }
+}
+
 namespace {
 
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -508,6 +578,8 @@ static void mm_topk_block(const float* q, size_t nq, const float* rows, const Mm
     require(merge_smem <= 200 * 1024, "k too large for the tensor-core filter", kUnsupported);
     allow_large_smem<k_mm_merge>();
     const int sms = sm_count();
+    // small k: a warp per query merges the candidates (8 queries per block)
+    const bool warp_merge = k <= 24 && (d & 1) == 0 && (reinterpret_cast<uintptr_t>(rows) & 7) == 0;
     MmArgs a{};
     a.nq = static_cast<int>(nq);
     a.kblocks = kblocks;
@@ -539,9 +611,16 @@ static void mm_topk_block(const float* q, size_t nq, const float* rows, const Mm
             k_mm_filter<<<static_cast<unsigned>(std::min(tiles, sms)), kThreads, smem, st>>>(tmA, tmB, a);
             QG_LAUNCH_CHECK();
         }
-        k_mm_merge<<<static_cast<unsigned>(nq), 256, merge_smem, st>>>(q, d, rows, ip, static_cast<int>(k), cap,
-                                                                      cnt.get(), crow.get(), out_key, out_slot,
-                                                                      ovf.get());
+        if (warp_merge) {
+            const size_t wsm = 8 * static_cast<size_t>((d + 3) & ~3) * 4 + 8 * 32 * 8;
+            k_mm_merge_warp<<<static_cast<unsigned>(ceil_div(nq, 8)), 256, wsm, st>>>(
+                q, d, rows, ip, static_cast<int>(k), static_cast<int>(nq), cap, cnt.get(), crow.get(), out_key,
+                out_slot, ovf.get());
+        } else {
+            k_mm_merge<<<static_cast<unsigned>(nq), 256, merge_smem, st>>>(q, d, rows, ip, static_cast<int>(k), cap,
+                                                                          cnt.get(), crow.get(), out_key, out_slot,
+                                                                          ovf.get());
+        }
         QG_LAUNCH_CHECK();
         n0 = n1;
         chunk = std::min<size_t>(n0 * (growth - 1), size_t{1} << 21);

@@ -65,8 +65,8 @@ void unit_rows_dev(const float* src, size_t k, int d, float* dst, cudaStream_t s
 // e-means state between steps (positions, masses, the closing pass's sums).
 struct EMeansState {
     int k = 0, d = 0;
-    DevBuf<float> pos, mass, pass_sums;
-    DevBuf<uint32_t> pass_counts;
+    DevBuf<float> pos, mass, close_sum;
+    DevBuf<uint32_t> close_cnt;
     void init(int k, int d, cudaStream_t st);   // masses 2^-16, pass sums zero
     // one mini-batch: member sums and cluster offsets of the batch, the step's alpha
     void step(const float* sums, const uint32_t* off, double alpha, bool accumulate, cudaStream_t st);

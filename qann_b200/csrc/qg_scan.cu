@@ -727,6 +727,9 @@ __global__ void __launch_bounds__(NW * 32, kMinB) k_scan(ScanArgs a) {
 
         // ---- the unit's k' best: each warp's own, gathered, cut to k', sorted ----
         __syncwarp();
+        // keys above the block threshold first (as at a trim), so that fewer
+        // reach warp 0's cut below
+        wcount = warp_keep_upto(wbuf, min(wcount, wcap), *reinterpret_cast<volatile unsigned long long*>(&s_thr));
         if (wcount > kp) {
             warp_select_keep(wbuf, min(wcount, wcap), kp, hist);
             wcount = kp;

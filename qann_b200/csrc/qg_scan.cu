@@ -78,23 +78,32 @@ __device__ __forceinline__ bool warp_lut3(RowFn row, int m, int m_pad, float* ro
         lo_out = lo;
         return __fsub_rn(hi, lo);
     };
+    auto low = [&](const float* v) {
+        float lo = v[0];
+#pragma unroll
+        for (int j = 1; j < 16; ++j) lo = fminf(lo, v[j]);
+        return lo;
+    };
+    // one round (m <= 64): the rows stay in registers, and their maxima are
+    // formed only once the list is known not to be hopeless
+    const bool one_round = m <= 64;
     int base = 0;
     for (;; base += 64) {
         const int ra = base + lane, rb = ra + 32;
         row(min(ra, m - 1), va);   // (lanes past the last row form row m - 1 again, unused)
         row(min(rb, m - 1), vb);
-        const float wa = range(va, mina), wb = range(vb, minb);
-        if (ra < m) {
-            row_min[ra] = mina;
-            widest = widest < wa ? wa : widest;
+        if (one_round) {
+            mina = low(va);
+            minb = low(vb);
+        } else {
+            const float wa = range(va, mina), wb = range(vb, minb);
+            if (ra < m) widest = widest < wa ? wa : widest;
+            if (rb < m) widest = widest < wb ? wb : widest;
         }
-        if (rb < m) {
-            row_min[rb] = minb;
-            widest = widest < wb ? wb : widest;
-        }
+        if (ra < m) row_min[ra] = mina;
+        if (rb < m) row_min[rb] = minb;
         if (base + 64 >= m) break;
     }
-    widest = warp_max(widest);
     __syncwarp();
     float part = 0.0f;
     if (lane < 4)
@@ -109,6 +118,27 @@ __device__ __forceinline__ bool warp_lut3(RowFn row, int m, int m_pad, float* ro
     const float p0 = __shfl_sync(0xffffffffu, part, 0), p1 = __shfl_sync(0xffffffffu, part, 1);
     const float p2 = __shfl_sync(0xffffffffu, part, 2), p3 = __shfl_sync(0xffffffffu, part, 3);
     const float offset = __fadd_rn(__fadd_rn(p0, p1), __fadd_rn(p2, p3));
+    if (one_round) {
+        // a zero sum's distance is 0 + offset for any scale > 0 and NaN (key
+        // 0xFFFFFFFF, above every threshold but the open one) for scale 0, so a
+        // list whose 0 + offset is above the threshold is hopeless at any scale
+        if (thr_hi != 0xFFFFFFFFu && float_key(__fadd_rn(0.0f, offset)) > thr_hi) {
+            scale_out = 1.0f;
+            offset_out = offset;
+            __syncwarp();
+            return false;
+        }
+        float hia = va[0], hib = vb[0];
+#pragma unroll
+        for (int j = 1; j < 16; ++j) {
+            hia = fmaxf(hia, va[j]);
+            hib = fmaxf(hib, vb[j]);
+        }
+        const float wa = __fsub_rn(hia, mina), wb = __fsub_rn(hib, minb);
+        if (lane < m) widest = widest < wa ? wa : widest;
+        if (lane + 32 < m) widest = widest < wb ? wb : widest;
+    }
+    widest = warp_max(widest);
     const float scale = widest > 0.0f ? __fdiv_rn(static_cast<float>(kLutMax), widest) : 1.0f;
     const bool live = thr_hi == 0xFFFFFFFFu || float_key(fs_dist0(scale, offset)) <= thr_hi;   // (warp-uniform)
     if (live) {

@@ -732,7 +732,7 @@ def served_workload(args):
     rates = (5_000, 10_000, 20_000, 50_000, 100_000, 200_000, 300_000)
     out = []
     same = True
-    with qb.Server(index, slots=4, max_batch=256, mem_budget=4 << 30) as srv:
+    with qb.Server(index, slots=2, max_batch=512, mem_budget=4 << 30) as srv:
         fids = [srv.add_filter(np.packbits(np.concatenate([b, np.zeros((-n) % 64, bool)]), bitorder="little")
                                .view(np.uint64)) for b in pool]
         arng = np.random.default_rng(3)
@@ -820,7 +820,7 @@ def served_workload(args):
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": f"served_{n}x{d}_nl{nlist}_m{m}_kf{kf}", "requests_per_rate": nreq,
                    "k": [10, 100], "nprobe": "log-uniform 8..256", "filtered": 0.3, "selectivity": [0.01, 0.5],
-                   "slots": 4, "max_batch": 256},
+                   "slots": 2, "max_batch": 512},
         "rates": out, "results_equal_solo_searches": same, "mean_batch": round(st["completed"] / st["batches"], 1),
         "rel_err_vs_fp64": err64,
         "at_lowest_rate": {"kernel_ms_per_batch": kernel_per_batch}, "one_at_a_time": solo,

@@ -631,7 +631,7 @@ def flat_workload(args):
                      "frac": round(l2["tensor_tflops"] / peak, 4), "traffic": None, "peak_source": peak_src},
         "e2e": {"value": l2["e2e_qps"], "unit": "queries/s", "h2d_bytes_per_step": nq * d * 4,
                 "d2h_bytes_per_step": nq * k * 12},
-        "gpu_launches": l2["gpu_launches"], "cpu_baseline": cpu}))
+        "gpu_launches": l2["gpu_launches"], "filter_schedule": qb.filter_options(), "cpu_baseline": cpu}))
     return 0
 
 
@@ -678,7 +678,7 @@ def train_workload(args):
         "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": round(secs * 1e3, 1),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 filter + f32/f64",
         "data": "synthetic", "config": {"workload": f"train_{n}x{d}_nl{nlist}_lloyd{iters}_pq{m}"},
-        "assign_pairs_per_s": round(pairs / secs, 1), "cpu_baseline": cpu}))
+        "assign_pairs_per_s": round(pairs / secs, 1), "filter_schedule": qb.filter_options(), "cpu_baseline": cpu}))
     return 0
 
 

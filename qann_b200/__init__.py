@@ -182,6 +182,31 @@ def scan_options() -> dict:
     return out
 
 
+def set_filter_options(autotune: bool | None = None, epilogue_warps: int | None = None) -> None:
+    """The tensor-core filter's schedule (flat search, direct scans,
+    nearest-centroid assignment, the coarse step). autotune: time its 8- and
+    16-warp epilogues on the first large launch of each problem and keep the
+    faster (default on); off, the 8-warp one. epilogue_warps: 8 or 16 forces
+    that epilogue on every launch, 0 leaves the pick to the autotuner. Results
+    are identical under every setting."""
+    if autotune is not None:
+        check(_lib.lib.qg_set_option(b"filter_autotune", int(bool(autotune))))
+    if epilogue_warps is not None:
+        check(_lib.lib.qg_set_option(b"filter_epilogue_warps", int(epilogue_warps)))
+
+
+def filter_options() -> dict:
+    """autotune (on or off), tuned_problems (problems timed so far),
+    last_epilogue_warps (8 or 16, the last filter launch's schedule) and
+    epilogue_warps (the forced schedule, 0 for none)."""
+    out = {}
+    for key in ("autotune", "tuned_problems", "last_epilogue_warps", "epilogue_warps"):
+        v = C.c_int64()
+        check(_lib.lib.qg_get_option(f"filter_{key}".encode(), C.byref(v)))
+        out[key] = v.value
+    return out
+
+
 class DenseIndex:
     """An index of dense float32 vectors. Not constructed directly."""
 

@@ -622,6 +622,12 @@ int qg_set_option(const char* key, int64_t value) {
         } else if (k == "tensor_scan") {
             require(value >= 0 && value <= 2, "tensor_scan must be 0, 1 or 2");
             set_tensor_scan(static_cast<int>(value));
+        } else if (k == "filter_autotune") {
+            require(value == 0 || value == 1, "filter_autotune must be 0 or 1");
+            set_filter_autotune(static_cast<int>(value));
+        } else if (k == "filter_epilogue_warps") {
+            require(value == 0 || value == 8 || value == 16, "filter_epilogue_warps must be 0, 8 or 16");
+            set_filter_epilogue_warps(static_cast<int>(value));
         } else {
             throw Error(kInvalidArgument, "unknown option: " + k);
         }
@@ -659,6 +665,10 @@ int qg_get_option(const char* key, int64_t* value) {
         else if (k == "scan_tuned_shapes") *value = scan_tuned_shapes();
         else if (k == "scan_last_shape") *value = scan_last_shape();
         else if (k == "tensor_scan") *value = tensor_scan();
+        else if (k == "filter_autotune") *value = filter_autotune();
+        else if (k == "filter_tuned_problems") *value = filter_tuned_problems();
+        else if (k == "filter_last_epilogue_warps") *value = filter_last_epilogue_warps();
+        else if (k == "filter_epilogue_warps") *value = filter_epilogue_warps();
         else if (k == "mapped_rows_error") *value = mapped_rows_error();
         else if (k.rfind("tensor_scan_stat_", 0) == 0) {
             require(tensor_scan_stat(k.substr(17), value), "unknown option: " + k);

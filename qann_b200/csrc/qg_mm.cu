@@ -31,7 +31,9 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -43,8 +45,10 @@ constexpr int BM = 128;         // queries per tile (TMEM lanes)
 constexpr int BN = 256;         // base rows per tile (accumulator columns)
 constexpr int KA = 64;          // bf16 elements per 128-byte swizzle row
 constexpr int kStages = 2;      // base tile buffers
-constexpr int kEpiWarps = 8;    // two per TMEM lane quadrant, each on half the columns
-constexpr int kThreads = (2 + kEpiWarps) * 32;
+// epilogue warps: EPI / 4 per TMEM lane quadrant, each on BN / (EPI / 4) columns of a tile
+// (8 or 16, picked per problem by the filter's autotuner)
+template <int EPI>
+constexpr int filter_threads() { return (2 + EPI) * 32; }
 constexpr uint32_t kTmemCols = 2 * BN;
 constexpr int kMaxKBlocks = 2;  // d <= 128
 
@@ -88,11 +92,13 @@ __device__ __forceinline__ void tile_coords(int t, int mtiles, int ntiles, int& 
     nt = group * kGroupN + (rem - mt * gsize);
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+template <int EPI>
+__global__ void __launch_bounds__(filter_threads<EPI>(), 1)
     k_mm_filter(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, MmArgs a) {
+    static_assert(EPI == 8 || EPI == 16, "8 or 16 epilogue warps");
     using namespace sm100;
     extern __shared__ uint8_t smem_raw[];
-    __shared__ __align__(16) float s_xt[kEpiWarps][32];   // epilogue: each warp's current run of row terms
+    __shared__ __align__(16) float s_xt[EPI][32];   // epilogue: each warp's current run of row terms
     uint8_t* base = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const uint32_t a_bytes = static_cast<uint32_t>(a.kblocks) * BM * 128;
     const uint32_t b_bytes = static_cast<uint32_t>(a.kblocks) * BN * 128;
@@ -119,7 +125,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_init(empty_a, 1);
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], kEpiWarps);
+            mbar_init(&tempty[b], EPI);
         }
         mbar_init(mma_done, 1);
         *abort = 0;
@@ -218,9 +224,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_wait(mma_done, 0, &never);
         }
     } else {
-        const int ew = warp - 2;      // 0..7
+        const int ew = warp - 2;      // 0..EPI-1
         const int quad = warp & 3;    // this warp's TMEM lanes: 32 * quad ..
-        const int col0 = (ew >> 2) * (BN / 2);
+        constexpr int kCols = BN / (EPI / 4);   // this warp's columns of a tile
+        const int col0 = (ew >> 2) * kCols;
         const int row_in_tile = quad * 32 + lane;
         int ti = 0;
         for (int t = t_begin; t < t_end; ++t) {
@@ -236,7 +243,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int qi = mt * BM + row_in_tile;
             const bool live = qi < a.nq;
             const float thr = live && !a.store ? a.thr[qi] : 0.0f;
-            for (int c = 0; c < BN / 2; c += 32) {
+            for (int c = 0; c < kCols; c += 32) {
                 uint32_t v[32];
                 tmem_ld32(tmem + (static_cast<uint32_t>(quad * 32) << 16) + static_cast<uint32_t>(acc * BN + col0 + c),
                           v);
@@ -519,6 +526,93 @@ void mm_prepare(const float* rows, size_t n, int dim, MmRows& out, cudaStream_t 
     }
 }
 
+// ---------------------------------------------------------------------------
+// The filter's schedule and its autotuner. The epilogue limits the filter, so
+// its warp count is the schedule choice: 8 epilogue warps (two per TMEM lane
+// quadrant, 128 columns of a tile each) or 16 (four per quadrant, 64 columns
+// each). On the first launch of a problem (store or filter mode, K blocks,
+// query tiles and base tiles by their power of two) with at least 8 tiles per
+// SM, both are timed twice on the launch's own inputs and the faster kept for
+// the rest of the process; a filter run appends candidates, so their counts are
+// cleared before each timed run, and the last timed run's candidates are the
+// launch's result. Both give the same candidate sets. Launches that must not
+// wait on the host (the coarse step without read-back, graph capture) use the
+// problem's pick if there is one, else 8.
+// ---------------------------------------------------------------------------
+namespace {
+std::mutex g_ftune_mu;
+std::map<uint64_t, int> g_ftune;   // problem key -> epilogue warps
+std::atomic<int> g_ftune_on{1}, g_ftune_last{8}, g_ftune_force{0};   // force: 0, or 8 / 16 epilogue warps
+
+template <int EPI>
+void launch_filter_epi(const CUtensorMap& tmA, const CUtensorMap& tmB, const MmArgs& a, size_t smem, cudaStream_t st) {
+    allow_large_smem<k_mm_filter<EPI>>();
+    const int tiles = a.mtiles * a.ntiles;
+    k_mm_filter<EPI><<<static_cast<unsigned>(std::min(tiles, sm_count())), filter_threads<EPI>(), smem, st>>>(tmA, tmB,
+                                                                                                            a);
+    QG_LAUNCH_CHECK();
+}
+
+void launch_filter_as(int epi, const CUtensorMap& tmA, const CUtensorMap& tmB, const MmArgs& a, size_t smem,
+                      cudaStream_t st) {
+    if (epi == 16) launch_filter_epi<16>(tmA, tmB, a, smem, st);
+    else launch_filter_epi<8>(tmA, tmB, a, smem, st);
+    g_ftune_last.store(epi);
+}
+
+void launch_filter(const CUtensorMap& tmA, const CUtensorMap& tmB, const MmArgs& a, size_t smem, cudaStream_t st,
+                   bool may_tune) {
+    if (const int f = g_ftune_force.load()) {
+        launch_filter_as(f, tmA, tmB, a, smem, st);
+        return;
+    }
+    const uint64_t key = (static_cast<uint64_t>(a.store != nullptr) << 48) | (static_cast<uint64_t>(a.kblocks) << 40) |
+                         (static_cast<uint64_t>(next_pow2(a.mtiles)) << 20) | static_cast<uint64_t>(next_pow2(a.ntiles));
+    {
+        std::lock_guard<std::mutex> g(g_ftune_mu);
+        const auto it = g_ftune.find(key);
+        if (it != g_ftune.end()) {
+            launch_filter_as(it->second, tmA, tmB, a, smem, st);
+            return;
+        }
+    }
+    if (!may_tune || !g_ftune_on.load() || a.mtiles * a.ntiles < 8 * sm_count()) {
+        launch_filter_as(8, tmA, tmB, a, smem, st);
+        return;
+    }
+    cudaEvent_t e0, e1;
+    QG_CUDA(cudaEventCreate(&e0));
+    QG_CUDA(cudaEventCreate(&e1));
+    constexpr int kCand[2] = {8, 16};
+    float fastest[2] = {0.0f, 0.0f};
+    for (int round = 0; round < 2; ++round)
+        for (int c = 0; c < 2; ++c) {
+            if (!a.store) QG_CUDA(cudaMemsetAsync(a.cand_count, 0, static_cast<size_t>(a.nq) * sizeof(uint32_t), st));
+            QG_CUDA(cudaEventRecord(e0, st));
+            launch_filter_as(kCand[c], tmA, tmB, a, smem, st);
+            QG_CUDA(cudaEventRecord(e1, st));
+            QG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            QG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (round == 0 || ms < fastest[c]) fastest[c] = ms;
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> g(g_ftune_mu);
+    g_ftune[key] = fastest[1] < fastest[0] ? 16 : 8;
+}
+} // namespace
+
+void set_filter_autotune(int on) { g_ftune_on.store(on); }
+int filter_autotune() { return g_ftune_on.load(); }
+int64_t filter_tuned_problems() {
+    std::lock_guard<std::mutex> g(g_ftune_mu);
+    return static_cast<int64_t>(g_ftune.size());
+}
+int filter_last_epilogue_warps() { return g_ftune_last.load(); }
+void set_filter_epilogue_warps(int warps) { g_ftune_force.store(warps); }
+int filter_epilogue_warps() { return g_ftune_force.load(); }
+
 static void mm_topk_block(const float* q, size_t nq, const float* rows, const MmRows& base, bool ip, size_t k,
                           const uint64_t* allow, const uint64_t* deny, uint64_t* out_key, uint32_t* out_slot,
                           std::vector<int>& overflow_q, size_t q_first, cudaStream_t st);
@@ -573,11 +667,9 @@ static void mm_topk_block(const float* q, size_t nq, const float* rows, const Mm
     const CUtensorMap tmB = make_map(reinterpret_cast<const __nv_bfloat16*>(base.bf16.get()), n, base.dpad, BN);
     // more than half an SM's shared memory: one CTA per SM, so no two CTAs wait on each other's TMEM
     const size_t smem = std::max<size_t>(filter_smem_bytes(kblocks), 116 * 1024);
-    allow_large_smem<k_mm_filter>();
     const size_t merge_smem = ((static_cast<size_t>(d) * 4 + 15) & ~size_t{15}) + static_cast<size_t>(next_pow2(static_cast<int>(k) + cap)) * 8;
     require(merge_smem <= 200 * 1024, "k too large for the tensor-core filter", kUnsupported);
     allow_large_smem<k_mm_merge>();
-    const int sms = sm_count();
     // small k: a warp per query merges the candidates (8 queries per block)
     const bool warp_merge = k <= 24 && (d & 1) == 0 && (reinterpret_cast<uintptr_t>(rows) & 7) == 0;
     MmArgs a{};
@@ -605,11 +697,9 @@ static void mm_topk_block(const float* q, size_t nq, const float* rows, const Mm
         a.n0 = static_cast<int>(n0);
         a.n1 = static_cast<int>(n1);
         a.ntiles = static_cast<int>(ceil_div(n1 - n0, BN));
-        const int tiles = a.mtiles * a.ntiles;
         {
             KernelTimer kt("mm_filter", st);
-            k_mm_filter<<<static_cast<unsigned>(std::min(tiles, sms)), kThreads, smem, st>>>(tmA, tmB, a);
-            QG_LAUNCH_CHECK();
+            launch_filter(tmA, tmB, a, smem, st, /*may_tune=*/true);
         }
         if (warp_merge) {
             const size_t wsm = 8 * static_cast<size_t>((d + 3) & ~3) * 4 + 8 * 32 * 8;
@@ -954,7 +1044,6 @@ void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t*
         const CUtensorMap tmA = make_map(qh.get(), nb, qdpad, BM, true);
         const CUtensorMap tmB = make_map(v.cent_f16, nlist, v.cent_dpad, BN, true);
         const size_t smem = std::max<size_t>(filter_smem_bytes(kblocks), 116 * 1024);
-        allow_large_smem<k_mm_filter>();
         MmArgs a{};
         a.nq = nb;
         a.n0 = 0;
@@ -969,9 +1058,7 @@ void coarse_probes_mm(const IvfView& v, const float* q, int nq, int P, uint32_t*
         a.f16 = 1;
         {
             KernelTimer kt("coarse_mm", st);
-            k_mm_filter<<<static_cast<unsigned>(std::min(a.mtiles * a.ntiles, sm_count())), kThreads, smem, st>>>(tmA,
-                                                                                                               tmB, a);
-            QG_LAUNCH_CHECK();
+            launch_filter(tmA, tmB, a, smem, st, /*may_tune=*/!no_readback);
         }
         const int cap = no_readback ? next_pow2(nlist) : coarse_cap(nlist, P);   // no read-back: every list fits
         const size_t rsm = coarse_recheck_smem(nlist, d, cap);

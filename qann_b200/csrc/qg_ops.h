@@ -91,6 +91,14 @@ struct MmRows {
     DevBuf<float> sq;
 };
 bool mm_supported(int dim);
+// The filter's epilogue-warp autotuner (qg_mm.cu): on or off, problems tuned, the last launch's pick.
+void set_filter_autotune(int on);
+int filter_autotune();
+int64_t filter_tuned_problems();
+int filter_last_epilogue_warps();
+// 0: the autotuner's pick; 8 or 16: that epilogue on every filter launch.
+void set_filter_epilogue_warps(int warps);
+int filter_epilogue_warps();
 void mm_prepare(const float* rows, size_t n, int dim, MmRows& out, cudaStream_t st);
 // The exact top-k by the BF16 tensor-core filter and FP32 recheck (qg_mm.cu);
 // queries whose candidate lists overflowed are listed in overflow_q and must

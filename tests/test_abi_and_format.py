@@ -86,6 +86,24 @@ def test_scan_options_validate():
     assert qb.scan_options()["variant"] == -1 and qb.scan_options()["autotune"] == 1
 
 
+def test_filter_options_validate():
+    """Tensor-core filter schedule options (host state only): a forced
+    epilogue of 0, 8 or 16 warps is kept, anything else is refused and leaves
+    the setting as it was."""
+    try:
+        for warps in (8, 16, 0):
+            qb.set_filter_options(autotune=False, epilogue_warps=warps)
+            assert qb.filter_options()["epilogue_warps"] == warps
+            assert qb.filter_options()["autotune"] == 0
+        for bad in (-1, 4, 12, 32):
+            with pytest.raises(ValueError, match="filter_epilogue_warps"):
+                qb.set_filter_options(epilogue_warps=bad)
+            assert qb.filter_options()["epilogue_warps"] == 0
+    finally:
+        qb.set_filter_options(autotune=True, epilogue_warps=0)
+    assert qb.filter_options()["autotune"] == 1
+
+
 @pytest.mark.parametrize("name", ["gen/refine_l2.qann", "gen/ivf_cos_ip.qann", "gen/ivf_l2_custom_del.qann",
                                   "gen/refine_l2_custom_del.qann", "gen/refine_cos_l2.qann"])
 def test_resave_is_byte_identical(golden, tmp_path, name):

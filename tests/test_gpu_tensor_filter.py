@@ -181,3 +181,55 @@ def test_coarse_matches_reference_files(golden, name):
         ids, d = idx.batch_query(q, 10)
         np.testing.assert_array_equal(ids, np.load(golden / "gen" / f"{kind}_{name}_ids.npy"))
         np.testing.assert_array_equal(d, np.load(golden / "gen" / f"{kind}_{name}_dists.npy"))
+
+
+@pytest.fixture
+def filter_schedule_reset():
+    yield
+    qb.set_filter_options(autotune=True, epilogue_warps=0)
+
+
+def test_filter_epilogue_schedules_identical(filter_schedule_reset):
+    """The filter's 8- and 16-warp epilogues, and the autotuner's pick, return
+    exactly the exact path's flat-search results; the autotuner times a
+    launch large enough to tune (at least 8 tiles per SM) and records it."""
+    d, n = 96, 200_000
+    x = lognormal_rows(21, n, d)
+    q = lognormal_rows(22, 3000, d)
+    idx = qb.FlatIndex(d, metric=qb.Metric(0))
+    idx.add(x)
+    qb.set_tensor_filter(0)
+    exact = idx.batch_query(q, 10)
+    qb.set_tensor_filter(2)
+    for warps in (8, 16):
+        qb.set_filter_options(epilogue_warps=warps)
+        got = idx.batch_query(q, 10)
+        assert_same(exact, got)
+        assert qb.filter_options()["last_epilogue_warps"] == warps
+    qb.set_filter_options(autotune=True, epilogue_warps=0)
+    before = qb.filter_options()["tuned_problems"]
+    assert_same(exact, idx.batch_query(q, 10))
+    assert qb.filter_options()["tuned_problems"] > before
+    assert_same(exact, idx.batch_query(q, 10))   # the kept pick
+
+
+def test_coarse_step_epilogue_schedules_identical(filter_schedule_reset):
+    """The tensor-core coarse step (store mode) under either epilogue returns
+    the exact path's results."""
+    d, nlist = 64, 1024
+    x = clustered(31, 60_000, d, centres=200)
+    q = clustered(32, 2000, d, centres=200)
+    ivf = qb.IVFIndex(d, nlist, 8)
+    ivf.enable_pq(16, fast_scan=True)
+    ivf.train(x, seed=1)
+    ivf.add(x)
+    ivf.nprobe = 32
+    qb.set_tensor_filter(0)
+    exact = ivf.batch_query(q, 10)
+    qb.set_tensor_filter(1)
+    for warps in (8, 16):
+        qb.set_filter_options(epilogue_warps=warps)
+        before = qb.tensor_filter_counts()
+        got = ivf.batch_query(q, 10)
+        assert qb.tensor_filter_counts()["coarse_queries"] > before["coarse_queries"], "the coarse step was not on the tensor cores"
+        assert_same(exact, got)

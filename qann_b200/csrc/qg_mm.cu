@@ -19,9 +19,10 @@
 // The filter kernel (k_mm_filter) is persistent and warp-specialised: warp 0
 // loads 128-row query tiles and 256-row base tiles with TMA (128-byte swizzle,
 // K-major bf16), warp 1 issues tcgen05.mma into one of two TMEM accumulators
-// (128 lanes x 256 columns each), and 8 epilogue warps read the accumulator
-// with tcgen05.ld, form the lower bound with one FMA and append the rows that
-// pass to the query's candidate list.
+// (128 lanes x 256 columns each), and 8 or 16 epilogue warps (the schedule
+// autotuner's pick) read the accumulator with tcgen05.ld, form the lower
+// bound with one FMA and append the rows that pass to the query's candidate
+// list.
 #include "qg_device.cuh"
 #include "qg_ops.h"
 #include "qg_sm100.cuh"

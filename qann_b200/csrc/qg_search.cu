@@ -337,13 +337,17 @@ void select_rows(const float* scores, size_t ld, int nrows, int ncols, int P, ui
 //   mode IP          : offset term = A = -(q . c)
 //   mode cosine-IP   : base = (A + 1) - |e|^2 (reference src/ivf_index.cpp:577-579)
 // ---------------------------------------------------------------------------
-// One (query, probe) pair per 8-lane group: the exact distance to the list's
-// residual center in exact_avx2's order (each group reads its row as 32-byte
-// segments, so the rows cross L2 once).
+// One (query, probe) pair per lane group of G: the exact distance to the
+// list's residual center in exact_avx2's order, by 8 lanes (each reads its
+// row as 32-byte segments, so the rows cross L2 once) or, for rows of an even
+// dim at 8-byte alignment, by 4 (each lane two AVX2 lanes, one 32-byte sector
+// of the row per group step; half the lane instructions).
+template <int G>
 __global__ void k_probe_terms(IvfView v, const float* __restrict__ q, int nq, int P, const uint32_t* __restrict__ probe,
                               const float* __restrict__ pdist, float* __restrict__ term) {
+    static_assert(G == 4 || G == 8, "lane groups of 4 or 8");
     const size_t n = static_cast<size_t>(nq) * P;
-    const size_t i0 = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;
+    const size_t i0 = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G;
     const bool in = i0 < n;   // (whole warps call the group scorer together)
     const size_t i = in ? i0 : 0;
     const int qi = static_cast<int>(i / P);
@@ -352,10 +356,10 @@ __global__ void k_probe_terms(IvfView v, const float* __restrict__ q, int nq, in
     if (v.has_resid) {
         const float* qa = q + static_cast<size_t>(qi) * v.dim;
         const float* rc = v.resid + static_cast<size_t>(list) * v.dim;
-        A = exact_avx2_group8<true, true>(qa, rc, v.dim);
+        A = G == 4 ? exact_avx2_group4<true>(qa, rc, v.dim) : exact_avx2_group8<true, true>(qa, rc, v.dim);
     }
     if (v.mode == kModeCosIP) A = __fsub_rn(__fadd_rn(A, 1.0f), v.sqnorm[list]);
-    if (in && (threadIdx.x & 7) == 0) term[i] = A;
+    if (in && (threadIdx.x & (G - 1)) == 0) term[i] = A;
 }
 
 // ---------------------------------------------------------------------------
@@ -577,15 +581,16 @@ __global__ void __launch_bounds__(128) k_finalize_ivf(const uint64_t* __restrict
 // spreads its gathers over the whole GPU as a large batch does), each score
 // kept as key(score) << 32 | slot; then per query those keys sorted.
 // ---------------------------------------------------------------------------
-template <bool kIP>
+template <bool kIP, int G>
 __global__ void __launch_bounds__(256) k_refine_scores(const float* __restrict__ q, int dim,
                                                        const float* __restrict__ rows,
                                                        const uint64_t* __restrict__ key_in,
                                                        const uint32_t* __restrict__ slot_in, int nq, int kp,
                                                        const int* __restrict__ kp_q, uint64_t* __restrict__ scored) {
-    const size_t g = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 3;   // candidate, query-major
+    static_assert(G == 4 || G == 8, "lane groups of 4 or 8");
+    const size_t g = (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) / G;   // candidate, query-major
     const size_t total = static_cast<size_t>(nq) * kp;
-    // whole 8-lane groups take part in the shuffles; groups past the end, and
+    // whole G-lane groups take part in the shuffles; groups past the end, and
     // empty candidates, score the query against itself unused
     const bool in = g < total;
     const size_t gi = in ? g : 0;
@@ -595,8 +600,10 @@ __global__ void __launch_bounds__(256) k_refine_scores(const float* __restrict__
     const uint32_t sl = ok ? slot_in[gi] : 0u;
     const float* qv = q + static_cast<size_t>(qi) * dim;
     const float* row = ok ? rows + static_cast<size_t>(sl) * dim : qv;
-    const float d = kIP ? -exact_avx2_group8<false, true>(qv, row, dim) : exact_avx2_group8<true, true>(qv, row, dim);
-    if (in && (threadIdx.x & 7) == 0)
+    float d;
+    if constexpr (G == 4) d = kIP ? -exact_avx2_group4<false>(qv, row, dim) : exact_avx2_group4<true>(qv, row, dim);
+    else d = kIP ? -exact_avx2_group8<false, true>(qv, row, dim) : exact_avx2_group8<true, true>(qv, row, dim);
+    if (in && (threadIdx.x & (G - 1)) == 0)
         scored[gi] = ok ? (static_cast<uint64_t>(float_key_eq0(d)) << 32) | sl : ~0ull;
 }
 
@@ -626,6 +633,70 @@ __global__ void __launch_bounds__(1024) k_refine_select(const float* __restrict_
             out_ids[o] = labels ? labels[slot] : static_cast<int64_t>(slot);
             out_d[o] = cosine ? __fmul_rn(d, 0.5f) : d;
         }
+    }
+}
+
+// k_refine_select for kp <= 256 K with 8 warps: each warp sorts a run of up
+// to 32 K candidate keys in registers; a key's rank is then the number of
+// keys below it in each run (binary searches over the sorted runs; its own run
+// counts its place in it), and the keys of rank below k are written at their
+// rank. The keys are unique but for the all-ones key of empty candidates,
+// which takes no place. One block barrier, where the bitonic sort takes one per
+// stage.
+template <int K>
+__global__ void __launch_bounds__(256) k_refine_select_ranked(const float* __restrict__ q, int dim,
+                                                              const float* __restrict__ rows,
+                                                              const uint64_t* __restrict__ scored, int kp, int k,
+                                                              bool ip, const int64_t* __restrict__ labels, bool cosine,
+                                                              int64_t* __restrict__ out_ids, float* __restrict__ out_d,
+                                                              const int* __restrict__ k_q) {
+    constexpr int R = 32 * K, NW = 8;
+    __shared__ uint64_t rkey[NW * R];
+    const int qi = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kq = k_q ? min(k_q[qi], k) : k;
+    const uint64_t* src = scored + static_cast<size_t>(qi) * kp;
+    uint64_t* run = rkey + R * warp;
+    const int n_w = max(0, min(R, kp - R * warp));
+    for (int i = lane; i < n_w; i += 32) run[i] = src[R * warp + i];
+    __syncwarp();
+    if (n_w > 0) warp_sort_keys_reg<K>(run, n_w);
+    __syncthreads();
+    auto below = [&](uint64_t key) {   // keys < key over all runs
+        int rank = 0;
+        for (int w = 0; w < NW; ++w) {
+            const int len = max(0, min(R, kp - R * w));
+            const uint64_t* rw = rkey + R * w;
+            int pos = 0;
+#pragma unroll
+            for (int step = R; step > 0; step >>= 1)
+                if (pos + step <= len && rw[pos + step - 1] < key) pos += step;
+            rank += pos;
+        }
+        return rank;
+    };
+    const float* qv = q + static_cast<size_t>(qi) * dim;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        const int e = i * 32 + lane;
+        if (e >= n_w) continue;
+        const uint64_t key = run[e];
+        if (key == ~0ull) continue;
+        const int rank = below(key);
+        if (rank >= kq) continue;
+        const size_t o = static_cast<size_t>(qi) * k + rank;
+        const uint32_t slot = static_cast<uint32_t>(key);
+        // recompute: float_key_eq0 folded -0 into +0, and the reference returns the value itself
+        const float d = exact_score(qv, rows + static_cast<size_t>(slot) * dim, dim, ip);
+        out_ids[o] = labels ? labels[slot] : static_cast<int64_t>(slot);
+        out_d[o] = cosine ? __fmul_rn(d, 0.5f) : d;
+    }
+    if (static_cast<int>(threadIdx.x) < k) {
+        const int filled = min(kq, below(~0ull));   // places taken by real candidates
+        for (int i = threadIdx.x; i < k; i += blockDim.x)
+            if (i >= filled) {
+                out_ids[static_cast<size_t>(qi) * k + i] = -1;
+                out_d[static_cast<size_t>(qi) * k + i] = __int_as_float(0x7f800000);
+            }
     }
 }
 
@@ -687,7 +758,10 @@ void probe_terms(const IvfView& v, const float* q, int nq, int P, const uint32_t
     const size_t n = static_cast<size_t>(nq) * P;
     if (n == 0) return;
     KernelTimer kt("probe_terms", st);
-    k_probe_terms<<<static_cast<unsigned>(ceil_div(n * 8, 256)), 256, 0, st>>>(v, q, nq, P, probe, pdist, term);
+    const bool g4 = v.has_resid && (v.dim & 1) == 0 && (reinterpret_cast<uintptr_t>(q) & 7) == 0 &&
+                    (reinterpret_cast<uintptr_t>(v.resid) & 7) == 0;
+    if (g4) k_probe_terms<4><<<static_cast<unsigned>(ceil_div(n * 4, 256)), 256, 0, st>>>(v, q, nq, P, probe, pdist, term);
+    else k_probe_terms<8><<<static_cast<unsigned>(ceil_div(n * 8, 256)), 256, 0, st>>>(v, q, nq, P, probe, pdist, term);
     QG_LAUNCH_CHECK();
 }
 
@@ -734,18 +808,33 @@ void refine_candidates(const float* q, int nq, int dim, const float* rows, const
     const size_t total = static_cast<size_t>(nq) * kp;
     DevBuf<uint64_t> scored(total, st);
     KernelTimer kt("refine", st);
-    const unsigned blocks = static_cast<unsigned>(ceil_div(total * 8, size_t{256}));
-    if (ip)
-        k_refine_scores<true><<<blocks, 256, 0, st>>>(q, dim, rows, key, slot, nq, kp, kp_q, scored.get());
+    // rows of an even dim at 8-byte alignment: one candidate per 4-lane group
+    const bool g4 = (dim & 1) == 0 && (reinterpret_cast<uintptr_t>(q) & 7) == 0 &&
+                    (reinterpret_cast<uintptr_t>(rows) & 7) == 0;
+    const unsigned blocks = static_cast<unsigned>(ceil_div(total * (g4 ? 4 : 8), size_t{256}));
+    if (g4 && ip)
+        k_refine_scores<true, 4><<<blocks, 256, 0, st>>>(q, dim, rows, key, slot, nq, kp, kp_q, scored.get());
+    else if (g4)
+        k_refine_scores<false, 4><<<blocks, 256, 0, st>>>(q, dim, rows, key, slot, nq, kp, kp_q, scored.get());
+    else if (ip)
+        k_refine_scores<true, 8><<<blocks, 256, 0, st>>>(q, dim, rows, key, slot, nq, kp, kp_q, scored.get());
     else
-        k_refine_scores<false><<<blocks, 256, 0, st>>>(q, dim, rows, key, slot, nq, kp, kp_q, scored.get());
+        k_refine_scores<false, 8><<<blocks, 256, 0, st>>>(q, dim, rows, key, slot, nq, kp, kp_q, scored.get());
     QG_LAUNCH_CHECK();
     if (ssm > 48 * 1024)
         allow_large_smem<k_refine_select>();
-    // few queries (serving's small batches): 1,024 threads a query for the sort
-    const int threads = nq < 2 * sm_count() ? 1024 : 256;
-    k_refine_select<<<nq, threads, ssm, st>>>(q, dim, rows, scored.get(), kp, k, ip, labels, cosine, out_ids, out_d,
-                                              k_q);
+    if (kp <= 256) {
+        k_refine_select_ranked<1><<<nq, 256, 0, st>>>(q, dim, rows, scored.get(), kp, k, ip, labels, cosine, out_ids,
+                                                       out_d, k_q);
+    } else if (kp <= 512) {
+        k_refine_select_ranked<2><<<nq, 256, 0, st>>>(q, dim, rows, scored.get(), kp, k, ip, labels, cosine, out_ids,
+                                                       out_d, k_q);
+    } else {
+        // few queries (serving's small batches): 1,024 threads a query for the sort
+        const int threads = nq < 2 * sm_count() ? 1024 : 256;
+        k_refine_select<<<nq, threads, ssm, st>>>(q, dim, rows, scored.get(), kp, k, ip, labels, cosine, out_ids,
+                                                  out_d, k_q);
+    }
     QG_LAUNCH_CHECK();
 }
 

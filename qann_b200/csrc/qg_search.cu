@@ -61,18 +61,31 @@ constexpr int kTA = 16, kTB = 32;
 template <bool kIP>
 __global__ void __launch_bounds__(256) k_pair_scores(const float* __restrict__ A, int na, const float* __restrict__ Bm,
                                                      int nb, int d, float* __restrict__ out, size_t ld_out) {
-    __shared__ float sa[kTA][33];
-    __shared__ float sb[kTB][33];
+    // rows padded to 34 floats: 8-byte loads stay aligned, and the 16 B rows a
+    // half-warp reads fall on distinct bank pairs
+    __shared__ __align__(8) float sa[kTA][34];
+    __shared__ __align__(8) float sb[kTB][34];
     const int ta = threadIdx.x >> 4;          // 0..15: row of a
     const int tb = threadIdx.x & 15;          // pairs (tb) and (tb + 16) of b
     const int a0 = blockIdx.y * kTA, b0 = blockIdx.x * kTB;
-    float acc[2][4][8];
+    // acc[p][j][h]: accumulator j of AVX2 lanes 2h and 2h + 1, advanced as one
+    // packed pair (each component rounds as the scalar FMA does)
+    float2 acc[2][4][4];
 #pragma unroll
     for (int p = 0; p < 2; ++p)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int L = 0; L < 8; ++L) acc[p][j][L] = 0.0f;
+            for (int h = 0; h < 4; ++h) acc[p][j][h] = make_float2(0.0f, 0.0f);
+    auto step = [&](float2& c, const float* qa, const float* qb, int e) {
+        const float2 x = *reinterpret_cast<const float2*>(qa + e), y = *reinterpret_cast<const float2*>(qb + e);
+        if (kIP) {
+            c = __ffma2_rn(x, y, c);
+        } else {
+            const float2 df = sub2(x, y);
+            c = __ffma2_rn(df, df, c);
+        }
+    };
 
     const int n32 = d & ~31;
     auto stage = [&](int base, int len) {
@@ -97,15 +110,7 @@ __global__ void __launch_bounds__(256) k_pair_scores(const float* __restrict__ A
 #pragma unroll
             for (int j = 0; j < 4; ++j)
 #pragma unroll
-                for (int L = 0; L < 8; ++L) {
-                    const int e = 8 * j + L;
-                    if (kIP) {
-                        acc[p][j][L] = __fmaf_rn(qa[e], qb[e], acc[p][j][L]);
-                    } else {
-                        const float df = __fsub_rn(qa[e], qb[e]);
-                        acc[p][j][L] = __fmaf_rn(df, df, acc[p][j][L]);
-                    }
-                }
+                for (int h = 0; h < 4; ++h) step(acc[p][j][h], qa, qb, 8 * j + 2 * h);
         }
         __syncthreads();
     }
@@ -119,20 +124,16 @@ __global__ void __launch_bounds__(256) k_pair_scores(const float* __restrict__ A
     for (int p = 0; p < 2; ++p) {
         const float* qa = sa[ta];
         const float* qb = sb[tb + 16 * p];
-        for (int u = 0; u < rem8; u += 8)
+        for (int u = 0; u < rem8; u += 8)   // 8-float steps into accumulator 0
 #pragma unroll
-            for (int L = 0; L < 8; ++L) {
-                if (kIP) {
-                    acc[p][0][L] = __fmaf_rn(qa[u + L], qb[u + L], acc[p][0][L]);
-                } else {
-                    const float df = __fsub_rn(qa[u + L], qb[u + L]);
-                    acc[p][0][L] = __fmaf_rn(df, df, acc[p][0][L]);
-                }
-            }
+            for (int h = 0; h < 4; ++h) step(acc[p][0][h], qa, qb, u + 2 * h);
         float s[8];
 #pragma unroll
-        for (int L = 0; L < 8; ++L)
-            s[L] = __fadd_rn(__fadd_rn(acc[p][0][L], acc[p][1][L]), __fadd_rn(acc[p][2][L], acc[p][3][L]));
+        for (int h = 0; h < 4; ++h) {
+            s[2 * h] = __fadd_rn(__fadd_rn(acc[p][0][h].x, acc[p][1][h].x), __fadd_rn(acc[p][2][h].x, acc[p][3][h].x));
+            s[2 * h + 1] =
+                __fadd_rn(__fadd_rn(acc[p][0][h].y, acc[p][1][h].y), __fadd_rn(acc[p][2][h].y, acc[p][3][h].y));
+        }
         float r = __fadd_rn(__fadd_rn(__fadd_rn(s[0], s[4]), __fadd_rn(s[1], s[5])),
                             __fadd_rn(__fadd_rn(s[2], s[6]), __fadd_rn(s[3], s[7])));
         r = exact_tail<!kIP>(qa, qb, rem8, rem, r);   // the n % 8 tail as the reference build computes it
@@ -313,8 +314,47 @@ __global__ void __launch_bounds__(1024) k_select_rows(const float* __restrict__ 
     }
 }
 
+// select_rows for P = 1: a warp per row keeps the smallest (key, column)
+// pair of its row (a column that is not allowed has the all-ones key, as in
+// k_select_rows) and writes its column and score, or -1 and +inf when the
+// pick is not allowed.
+__global__ void __launch_bounds__(256) k_select_min_rows(const float* __restrict__ scores, size_t ld, int nrows,
+                                                         int ncols, const uint64_t* __restrict__ allow,
+                                                         const uint64_t* __restrict__ deny, size_t col_base, bool eq0,
+                                                         uint32_t* __restrict__ out_col, float* __restrict__ out_score) {
+    const int r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (r >= nrows) return;
+    const float* row = scores + static_cast<size_t>(r) * ld;
+    uint64_t best = ~0ull;
+    for (int c = lane; c < ncols; c += 32) {
+        const uint32_t k = col_allowed(allow, deny, col_base + c) ? (eq0 ? float_key_eq0(row[c]) : float_key(row[c]))
+                                                                  : 0xFFFFFFFFu;
+        const uint64_t kc = (static_cast<uint64_t>(k) << 32) | static_cast<uint32_t>(c);
+        best = kc < best ? kc : best;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const uint32_t lo = __shfl_xor_sync(0xffffffffu, static_cast<uint32_t>(best), o);
+        const uint32_t hi = __shfl_xor_sync(0xffffffffu, static_cast<uint32_t>(best >> 32), o);
+        const uint64_t other = (static_cast<uint64_t>(hi) << 32) | lo;
+        best = other < best ? other : best;
+    }
+    if (lane == 0) {
+        const uint32_t col = static_cast<uint32_t>(best);
+        const bool ok = ncols > 0 && col_allowed(allow, deny, col_base + col);
+        out_col[r] = ok ? col : 0xFFFFFFFFu;
+        out_score[r] = ok ? row[col] : __int_as_float(0x7f800000);
+    }
+}
+
 void select_rows(const float* scores, size_t ld, int nrows, int ncols, int P, uint32_t* out_col, float* out_score,
                  cudaStream_t st, const uint64_t* allow, const uint64_t* deny, size_t col_base, bool eq0) {
+    if (nrows > 0 && P == 1) {
+        KernelTimer kt("select_rows", st);
+        k_select_min_rows<<<static_cast<unsigned>(ceil_div(static_cast<size_t>(nrows), 8)), 256, 0, st>>>(
+            scores, ld, nrows, ncols, allow, deny, col_base, eq0, out_col, out_score);
+        QG_LAUNCH_CHECK();
+        return;
+    }
     if (nrows == 0) return;
     // few rows (serving's small batches): 1,024 threads a row and the row's
     // keys staged in shared memory; many rows: 256 threads, keys from L2

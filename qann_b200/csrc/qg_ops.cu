@@ -7,7 +7,9 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <exception>
 #include <numeric>
+#include <thread>
 
 namespace qg {
 
@@ -661,7 +663,7 @@ bool search_graph(IndexObj& idx, const SearchRequest& r, cudaStream_t st) {
 // Mixed batches (served requests with their own k, nprobe and filter)
 // ---------------------------------------------------------------------------
 void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs, size_t kmax, int64_t* out_ids,
-                  float* out_d, cudaStream_t st) {
+                  float* out_d, cudaStream_t st, cudaStream_t st2) {
     require_unsharded(idx);
     std::fill(out_ids, out_ids + nq * kmax, int64_t{-1});
     std::fill(out_d, out_d + nq * kmax, std::numeric_limits<float>::infinity());
@@ -752,7 +754,7 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
     // One batched search per class of k' (up to 256, above): a few requests
     // with a large k' would otherwise size every query's candidate lists and
     // scan trims by theirs.
-    auto run = [&](const std::vector<size_t>& batch) {
+    auto run = [&](const std::vector<size_t>& batch, cudaStream_t st) {
         const size_t nb = batch.size();
         size_t kmax_g = 1;
         for (size_t i : batch) kmax_g = std::max(kmax_g, static_cast<size_t>(qs[i].k));
@@ -860,8 +862,36 @@ void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs
     };
     std::vector<size_t> small, large;
     for (size_t i : batch) (kp_of(i) <= 256 ? small : large).push_back(i);
-    if (!small.empty()) run(small);
-    if (!large.empty()) run(large);
+    if (st2 && !small.empty() && !large.empty()) {
+        // both classes at once: the larger k' on st2 from a second thread (the
+        // two write disjoint requests' results); its error, if any, rethrown here
+        // st2 starts after what st holds so far (device copies of the index)
+        cudaEvent_t ready;
+        QG_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        QG_CUDA(cudaEventRecord(ready, st));
+        QG_CUDA(cudaStreamWaitEvent(st2, ready, 0));
+        QG_CUDA(cudaEventDestroy(ready));
+        std::exception_ptr err2;
+        std::thread t2([&] {
+            try {
+                QG_CUDA(cudaSetDevice(idx.device));
+                run(large, st2);
+            } catch (...) {
+                err2 = std::current_exception();
+            }
+        });
+        try {
+            run(small, st);
+        } catch (...) {
+            t2.join();
+            throw;
+        }
+        t2.join();
+        if (err2) std::rethrow_exception(err2);
+        return;
+    }
+    if (!small.empty()) run(small, st);
+    if (!large.empty()) run(large, st);
 }
 
 } // namespace qg

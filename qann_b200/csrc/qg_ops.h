@@ -68,9 +68,11 @@ struct MixedQuery {
 // dim). IVF indexes and RefineIndexes over IVF run the batch as one coarse
 // step, one scan and one re-rank; each query's results are the ones it gets
 // searched alone with its settings. Results are nq x kmax (host), query i's
-// first qs[i].k valid and the rest padded with -1 / +inf.
+// first qs[i].k valid and the rest padded with -1 / +inf. With a second
+// stream st2, a batch holding both classes of k' (up to 256 and above) runs
+// the larger class on st2 from a second host thread, at the same time.
 void search_mixed(IndexObj& idx, const float* q, size_t nq, const MixedQuery* qs, size_t kmax, int64_t* out_ids,
-                  float* out_d, cudaStream_t st);
+                  float* out_d, cudaStream_t st, cudaStream_t st2 = nullptr);
 
 // add()'s argument checks alone, so they fail before any CUDA work.
 void validate_add(const IndexObj& idx, size_t n, const int64_t* ids);

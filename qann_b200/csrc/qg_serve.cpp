@@ -225,10 +225,11 @@ private:
 
     // lane 0: every request but the narrow-filter ones; lane 1: those (see submit)
     void worker(int lane) {
-        cudaStream_t st = nullptr;
+        cudaStream_t st = nullptr, st2 = nullptr;   // st2: a mixed batch's larger k' class, at the same time
         if (cudaSetDevice(idx_->device) != cudaSuccess ||
             cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
             st = nullptr;
+        if (st && cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking) != cudaSuccess) st2 = nullptr;
         keep_pool_memory();
         const size_t d = dim();
         std::vector<ServeRequest*> b;
@@ -275,7 +276,7 @@ private:
                 std::shared_lock<std::shared_mutex> lk(idx_->mu);
                 std::shared_lock<std::shared_mutex> lb;
                 if (idx_->kind == Kind::Refine) lb = std::shared_lock<std::shared_mutex>(static_cast<RefineObj&>(*idx_).base->mu);
-                search_mixed(*idx_, q.data(), nb, mq.data(), kmax, ids.data(), dist.data(), st);
+                search_mixed(*idx_, q.data(), nb, mq.data(), kmax, ids.data(), dist.data(), st, st2);
             } catch (const Error& e) {
                 status = e.status;
                 err = e.what();
@@ -302,6 +303,7 @@ private:
             cv_out_.notify_all();
             for (auto& cv : cv_in_) cv.notify_all();
         }
+        if (st2) cudaStreamDestroy(st2);
         if (st) cudaStreamDestroy(st);
     }
 

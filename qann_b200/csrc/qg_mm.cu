@@ -417,6 +417,52 @@ __global__ void __launch_bounds__(256) k_mm_merge(const float* __restrict__ q, i
         }
         keys[i] = key;
     }
+    if (n <= 512 && blockDim.x == 256) {
+        // (block-uniform) the k smallest without a sort network: each of the
+        // 8 warps sorts a run of up to 64 keys in registers, a key's rank is
+        // the number of keys below it in every run (binary searches), and a
+        // key of rank below k goes to its place. Keys are unique but for the
+        // all-ones key of empty running places, which takes no place.
+        __syncthreads();
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int n_w = max(0, min(64, n - 64 * warp));
+        if (n_w > 0) warp_sort_keys_reg<2>(keys + 64 * warp, n_w);
+        __syncthreads();
+        auto below = [&](uint64_t key) {
+            int rank = 0;
+            for (int w = 0; w < 8; ++w) {
+                const int len = max(0, min(64, n - 64 * w));
+                const uint64_t* rw = keys + 64 * w;
+                int pos = 0;
+#pragma unroll
+                for (int step = 64; step > 0; step >>= 1)
+                    if (pos + step <= len && rw[pos + step - 1] < key) pos += step;
+                rank += pos;
+            }
+            return rank;
+        };
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int e = 32 * i + lane;
+            if (e >= n_w) continue;
+            const uint64_t key = keys[64 * warp + e];
+            if (key == ~0ull) continue;
+            const int rank = below(key);
+            if (rank < k) {
+                run_key[static_cast<size_t>(qi) * k + rank] = key;
+                run_slot[static_cast<size_t>(qi) * k + rank] = static_cast<uint32_t>(key);
+            }
+        }
+        if (static_cast<int>(threadIdx.x) < k) {
+            const int valid = below(~0ull);
+            for (int i = threadIdx.x; i < k; i += blockDim.x)
+                if (i >= valid) {
+                    run_key[static_cast<size_t>(qi) * k + i] = ~0ull;
+                    run_slot[static_cast<size_t>(qi) * k + i] = 0xFFFFFFFFu;
+                }
+        }
+        return;
+    }
     bitonic_sort_keys(keys, npow);
     for (int i = threadIdx.x; i < k; i += blockDim.x) {
         run_key[static_cast<size_t>(qi) * k + i] = keys[i];

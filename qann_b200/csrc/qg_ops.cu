@@ -152,10 +152,14 @@ void tensor_coarse_counts(int64_t* queries, int64_t* redone) {
 // 2.5e7 multiply-adds (about 12 queries against 16,384 lists of 128
 // dimensions): there the exact scores and row select of a batch took 66 us
 // at 16 queries and 310 us at 256, the F16 GEMM and recheck 47 and 56 us.
+// Coarse tables of at least 2^21 values (16,384 lists of 128 dimensions)
+// take the tensor cores at every batch size: for a single query there the
+// exact path took 92 us and the F16 GEMM and recheck 66 us.
 bool use_tensor_coarse(size_t nq, int nlist, int dim) {
     const int mode = g_tensor_filter.load();
     return mode > 0 && mm_supported(dim) &&
-           (mode == 2 || static_cast<double>(nq) * nlist * dim >= 2.5e7);
+           (mode == 2 || static_cast<double>(nq) * nlist * dim >= 2.5e7 ||
+            static_cast<double>(nlist) * dim >= 2097152.0);
 }
 
 void flat_candidates(const float* q_dev, size_t nq, const float* rows_dev, size_t n, int dim, bool ip, size_t k,

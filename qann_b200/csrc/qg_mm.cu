@@ -694,11 +694,11 @@ static void mm_topk_block(const float* q, size_t nq, const float* rows, const Mm
 
     // seed: the exact top-k of the first rows, which gives the first filter
     // chunk its threshold. The exact tiles run far below the tensor cores, so
-    // the seed is a small share of the rows: 1/64 of them, at least 256 (and
+    // the seed is a small share of the rows: 1/256 of them, at least 64 (and
     // 4k) and at most 4,096 (and 4k). Nearest-centroid assignment against
     // 4,096 to 16,384 centroids otherwise spends most of its time here.
-    const size_t seed_lo = std::max<size_t>(256, 4 * k), seed_hi = std::max<size_t>(4096, 4 * k);
-    const size_t seed = std::min(n, std::clamp<size_t>(n / 64, seed_lo, seed_hi));
+    const size_t seed_lo = std::max<size_t>(64, 4 * k), seed_hi = std::max<size_t>(4096, 4 * k);
+    const size_t seed = std::min(n, std::clamp<size_t>(n / 256, seed_lo, seed_hi));
     flat_candidates(q, nq, rows, seed, d, ip, k, allow, deny, out_key, out_slot, st, /*allow_mm=*/false);
     if (seed == n) return;
 
